@@ -1,0 +1,1658 @@
+// Host side of the arcos CDR library: context, device storage, work lists,
+// launch sequences and the C ABI of include/arcos_cdr.h.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/arcos_cdr.h"
+#include "device_common.cuh"
+#include "stage_kernel.cuh"
+#include "aux_kernels.cuh"
+
+using namespace arcos;
+
+namespace {
+
+thread_local std::string g_err;
+
+int
+fail (int code, const std::string &msg)
+{
+  g_err = msg;
+  return code;
+}
+
+#define CK(x)                                                                    \
+  do {                                                                           \
+    cudaError_t e_ = (x);                                                        \
+    if (e_ != cudaSuccess)                                                       \
+      return fail (ARCOS_ERR_CUDA, std::string (#x) + ": " + cudaGetErrorString (e_)); \
+  } while (0)
+
+#define CKL()                                                                    \
+  do {                                                                           \
+    cudaError_t e_ = cudaGetLastError ();                                        \
+    if (e_ != cudaSuccess)                                                       \
+      return fail (ARCOS_ERR_CUDA, std::string ("kernel launch: ") + cudaGetErrorString (e_)); \
+  } while (0)
+
+constexpr int N_TILE_CFG_MAX = 3;
+
+struct GridH {
+  int r0, z0, r1, z1, ntheta, level, ext_bound, parent, fam;
+  std::vector<int> kids;    // visit order (reverse creation)
+};
+
+struct Ctx {
+  arcos_params p{};
+  Model M{};
+  std::vector<double> table_values;  // flat, for re-building nodes
+  std::vector<TableNode> nodes_h;
+  TableNode *nodes_d = nullptr;
+  std::vector<GridH> g;
+  std::vector<PatchDesc> pd_h;
+  PatchDesc *pd_d = nullptr;
+  std::vector<double> dr, dz;
+  double *pool = nullptr;
+  size_t pool_doubles = 0;
+  int nfam = 0;
+  std::vector<int> fam_root;
+  DevState *st_d = nullptr;
+  double *dtlog_d = nullptr;
+  int dt_cap = 0;
+  int *etz_d = nullptr;
+  unsigned *done_d = nullptr;
+  cudaStream_t stream = 0;
+  cudaStream_t own_stream = 0;        // created by arcos_create, destroyed with the context
+  bool committed = false;
+  int num_sms = 148;
+  // work lists
+  WorkItem *items_d = nullptr;
+  int n_items = 0;
+  std::vector<int> item_off, item_cnt;
+  int tile_cfg = 1;                   // index into TILE_WY / TILE_RPW
+  int occ[4][N_TILE_CFG_MAX] = {};
+  int *plist_d = nullptr;             // 0..npatch-1
+  std::vector<int> level_off, level_cnt;   // children lists per level inside kids_d
+  int *kids_d = nullptr;
+  StripDesc *strips_d = nullptr;
+  std::vector<int> strip_off, strip_cnt;   // per level
+  std::vector<int> strip_patch;            // per strip: child patch (for per-patch mode)
+  long long *match_src_d[2] = {nullptr, nullptr}, *match_dst_d[2] = {nullptr, nullptr};
+  double *match_tmp_d = nullptr;
+  int n_match = 0;
+  double *ext_d = nullptr;            // [ext_r (nfam*MAXPLANES) | ext_t | ext_z (nfam)]
+  std::vector<double> famE;           // 3 per family
+  arcos_field_fn fn = nullptr;
+  void *user = nullptr;
+  bool field_set[2] = {false, false};
+  bool per_patch = false;             // launch every kernel once per patch
+  int max_level = 0;
+  bool fused_ok = false;              // every family is one root grid with all sides external
+  cudaGraphExec_t graph2 = nullptr;   // two fused steps
+  int graph_items = -1;
+};
+
+// ---- reaction-table thresholds ----------------------------------------------
+// The reference's classification of |E| (reaction.c:127-136):
+// -1 underflow, +1 overflow, 0 inside with *pos.
+int
+ref_class (double x, double e_min, double e_step, int steps, int *pos)
+{
+  const double log_e = log10 (x);
+  if (log_e < e_min) return -1;
+  if (log_e > e_min + e_step * steps) return 1;
+  *pos = (int) floor ((log_e - e_min) / e_step);
+  return 0;
+}
+
+double
+bits2d (unsigned long long b)
+{
+  double d;
+  memcpy (&d, &b, 8);
+  return d;
+}
+
+// Smallest non-negative double x (+inf included) with pred(x); pred monotone.
+template <class F>
+double
+smallest_true (F pred)
+{
+  unsigned long long lo = 0, hi = 0x7FF0000000000000ULL;   // +0 .. +inf
+  if (pred (bits2d (lo))) return 0.0;
+  if (!pred (bits2d (hi))) return INFINITY;
+  while (hi - lo > 1) {
+    const unsigned long long mid = lo + (hi - lo) / 2;
+    if (pred (bits2d (mid))) hi = mid;
+    else lo = mid;
+  }
+  return bits2d (hi);
+}
+
+void
+build_nodes (double e_min, double e_step, int steps, const double *values,
+             std::vector<TableNode> &out)
+{
+  const size_t base = out.size ();
+  out.resize (base + steps + 2);
+  for (int k = 0; k <= steps + 1; k++) {
+    TableNode n{};
+    if (k <= steps) {
+      n.thr = smallest_true ([&] (double x) {
+        int pos = 0;
+        const int c = ref_class (x, e_min, e_step, steps, &pos);
+        return c > 0 || (c == 0 && pos >= k);
+      });
+      const double v1 = values[k];
+      const double v2 = (k + 1 <= steps) ? values[k + 1] : values[steps];
+      const double e1 = pow (10, e_min + e_step * (double) k);       // reaction.c:139
+      const double e2 = e1 * pow (10, e_step);                        // reaction.c:140
+      n.val = v1;
+      n.e1 = e1;
+      n.slope = (v2 - v1) / (e2 - e1);                                // reaction.c:142
+    } else {
+      n.thr = smallest_true ([&] (double x) {
+        int pos = 0;
+        return ref_class (x, e_min, e_step, steps, &pos) > 0;
+      });
+    }
+    out[base + k] = n;
+  }
+}
+
+// ---- helpers -------------------------------------------------------------------
+inline int
+grid_blocks (long long work, int threads, int cap = 4096)
+{
+  long long b = (work + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (int) b;
+}
+
+constexpr int NODES_SMEM_MAX = 24 * 1024 / (int) sizeof (TableNode);
+
+// Tile shapes the autotuner chooses from: (warps per block, rows per thread);
+// tiles are 32 columns wide and WY * RPW rows high.
+constexpr int N_TILE_CFG = 3;
+constexpr int TILE_WY[N_TILE_CFG] = {4, 4, 8};
+constexpr int TILE_RPW[N_TILE_CFG] = {4, 8, 4};
+
+template <int NS, int MODE, int WY, int RPW>
+size_t
+stage_smem_t (int n_nodes)
+{
+  size_t b = sizeof (double) * (size_t) TileLayout<NS, MODE, WY, RPW>::DOUBLES;
+  if (n_nodes > 0 && n_nodes <= NODES_SMEM_MAX) b += sizeof (TableNode) * (size_t) n_nodes;
+  return b;
+}
+
+template <int NS, int MODE, int WY, int RPW>
+cudaError_t
+launch_stage_t (const Model &M, const StageArgs &A, int blocks, cudaStream_t s, int *occ)
+{
+  const size_t sm = stage_smem_t<NS, MODE, WY, RPW> (A.n_nodes);
+  cudaFuncSetAttribute (k_stage<NS, MODE, WY, RPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+  if (occ) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor (occ, k_stage<NS, MODE, WY, RPW>, 32 * WY, sm);
+    return cudaGetLastError ();
+  }
+  k_stage<NS, MODE, WY, RPW><<<blocks, 32 * WY, sm, s>>> (M, A);
+  return cudaGetLastError ();
+}
+
+template <int NS, int MODE>
+cudaError_t
+launch_stage_c (int cfg, const Model &M, const StageArgs &A, int blocks, cudaStream_t s, int *occ)
+{
+  switch (cfg) {
+  case 0: return launch_stage_t<NS, MODE, 4, 4> (M, A, blocks, s, occ);
+  case 1: return launch_stage_t<NS, MODE, 4, 8> (M, A, blocks, s, occ);
+  default: return launch_stage_t<NS, MODE, 8, 4> (M, A, blocks, s, occ);
+  }
+}
+
+template <int MODE>
+cudaError_t
+launch_stage_m (int ns, int cfg, const Model &M, const StageArgs &A, int blocks, cudaStream_t s, int *occ)
+{
+  switch (ns) {
+  case 1: return launch_stage_c<1, MODE> (cfg, M, A, blocks, s, occ);
+  case 2: return launch_stage_c<2, MODE> (cfg, M, A, blocks, s, occ);
+  case 3: return launch_stage_c<3, MODE> (cfg, M, A, blocks, s, occ);
+  case 4: return launch_stage_c<4, MODE> (cfg, M, A, blocks, s, occ);
+  case 5: return launch_stage_c<5, MODE> (cfg, M, A, blocks, s, occ);
+  case 6: return launch_stage_c<6, MODE> (cfg, M, A, blocks, s, occ);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t
+launch_stage (int mode, int ns, int cfg, const Model &M, const StageArgs &A, int blocks,
+              cudaStream_t s, int *occ = nullptr)
+{
+  switch (mode) {
+  case M_DERIV: return launch_stage_m<M_DERIV> (ns, cfg, M, A, blocks, s, occ);
+  case M_S1: return launch_stage_m<M_S1> (ns, cfg, M, A, blocks, s, occ);
+  case M_S2: return launch_stage_m<M_S2> (ns, cfg, M, A, blocks, s, occ);
+  case M_AMR2: return launch_stage_m<M_AMR2> (ns, cfg, M, A, blocks, s, occ);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+int
+stage_blocks (Ctx *c, int mode, int n_items)
+{
+  int &o = c->occ[mode][c->tile_cfg];
+  if (o == 0) {
+    StageArgs A{};
+    A.n_nodes = (int) c->nodes_h.size ();
+    int b = 0;
+    launch_stage (mode, c->M.ns, c->tile_cfg, c->M, A, 0, 0, &b);
+    o = b > 0 ? b : 1;
+  }
+  const int cap = c->num_sms * o;
+  return n_items < cap ? n_items : cap;
+}
+
+StageArgs
+base_args (Ctx *c)
+{
+  StageArgs A{};
+  A.patches = c->pd_d;
+  A.items = c->items_d;
+  A.n_items = c->n_items;
+  A.nodes = c->nodes_d;
+  A.st = c->st_d;
+  A.nfam = c->nfam;
+  A.etz = c->etz_d;
+  A.done = c->done_d;
+  A.n_nodes = (int) c->nodes_h.size ();
+  A.nodes_smem = A.n_nodes > 0 && A.n_nodes <= NODES_SMEM_MAX;
+  return A;
+}
+
+// Runs a stage-kernel mode over all patches (one persistent launch) or once per
+// patch in per-patch mode.
+int
+run_stage (Ctx *c, StageArgs A, int mode)
+{
+  if (!c->per_patch) {
+    const int blocks = stage_blocks (c, mode, A.n_items);
+    if (blocks <= 0) return ARCOS_OK;
+    cudaError_t e = launch_stage (mode, c->M.ns, c->tile_cfg, c->M, A, blocks, c->stream);
+    if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("stage launch: ") + cudaGetErrorString (e));
+    return ARCOS_OK;
+  }
+  for (size_t p = 0; p < c->pd_h.size (); p++) {
+    StageArgs B = A;
+    B.items = c->items_d + c->item_off[p];
+    B.n_items = c->item_cnt[p];
+    if (B.n_items == 0) continue;
+    const int blocks = stage_blocks (c, mode, B.n_items);
+    cudaError_t e = launch_stage (mode, c->M.ns, c->tile_cfg, c->M, B, blocks, c->stream);
+    if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("stage launch: ") + cudaGetErrorString (e));
+  }
+  return ARCOS_OK;
+}
+
+// Launch a per-patch streaming kernel over all patches (gridDim.y) or one by one.
+template <class L>
+int
+for_patches (Ctx *c, long long work_per_patch, L launch)
+{
+  const int np = (int) c->pd_h.size ();
+  if (!c->per_patch) {
+    dim3 grid (grid_blocks (work_per_patch, 256, 1024), np);
+    launch (grid, c->plist_d);
+  } else {
+    for (int p = 0; p < np; p++) {
+      const long long w = c->pd_h[p].asz * c->pd_h[p].ns;
+      dim3 grid (grid_blocks (w, 256, 1024), 1);
+      launch (grid, c->plist_d + p);
+    }
+  }
+  CKL ();
+  return ARCOS_OK;
+}
+
+long long
+max_patch_work (Ctx *c)
+{
+  long long m = 0;
+  for (auto &P : c->pd_h) m = std::max (m, P.asz * P.ns);
+  return m;
+}
+
+int
+chk_committed (Ctx *c)
+{
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  if (!c->committed) return fail (ARCOS_ERR_STATE, "arcos_commit has not been called");
+  return ARCOS_OK;
+}
+
+// ---- ghost phases -----------------------------------------------------------
+int
+do_nonneg (Ctx *c, int set)
+{
+  return for_patches (c, max_patch_work (c), [&] (dim3 g, const int *pl) {
+    k_nonneg<<<g, 256, 0, c->stream>>> (c->pd_d, pl, set);
+  });
+}
+
+int
+do_ext_bnd (Ctx *c, int set)
+{
+  const int np = (int) c->pd_h.size ();
+  if (!c->per_patch) k_ext_bnd<<<np, 256, 0, c->stream>>> (c->M, c->pd_d, c->plist_d, set);
+  else
+    for (int p = 0; p < np; p++) k_ext_bnd<<<1, 256, 0, c->stream>>> (c->M, c->pd_d, c->plist_d + p, set);
+  CKL ();
+  return ARCOS_OK;
+}
+
+int
+do_periodic (Ctx *c, int set, int what)
+{
+  bool any3d = false;
+  for (auto &P : c->pd_h) any3d |= P.ntheta > 1;
+  if (!any3d) return ARCOS_OK;
+  long long w = 0;
+  for (auto &P : c->pd_h) w = std::max (w, (long long) (2 * P.ns + 3) * 4 * P.plane_stride);
+  const int np = (int) c->pd_h.size ();
+  if (!c->per_patch) k_periodic<<<dim3 (grid_blocks (w, 256, 2048), np), 256, 0, c->stream>>> (c->pd_d, c->plist_d, set, what);
+  else
+    for (int p = 0; p < np; p++)
+      k_periodic<<<dim3 (grid_blocks (w, 256, 2048), 1), 256, 0, c->stream>>> (c->pd_d, c->plist_d + p, set, what);
+  CKL ();
+  return ARCOS_OK;
+}
+
+int
+do_restrict (Ctx *c, int set)
+{
+  for (int l = c->max_level; l >= 1; l--) {
+    const int n = c->level_cnt[l];
+    if (n == 0) continue;
+    if (!c->per_patch)
+      k_restrict<<<dim3 (64, n), 256, 0, c->stream>>> (c->pd_d, c->kids_d + c->level_off[l], set);
+    else
+      for (int i = 0; i < n; i++)
+        k_restrict<<<dim3 (64, 1), 256, 0, c->stream>>> (c->pd_d, c->kids_d + c->level_off[l] + i, set);
+    CKL ();
+  }
+  return ARCOS_OK;
+}
+
+int
+do_set_bnd (Ctx *c, int set)
+{
+  for (int l = 1; l <= c->max_level; l++) {
+    const int n = c->strip_cnt[l];
+    if (n == 0) continue;
+    if (!c->per_patch)
+      k_interp<<<dim3 (8, n), 256, 0, c->stream>>> (c->pd_d, c->strips_d + c->strip_off[l], set);
+    else
+      for (int i = 0; i < n; i++)
+        k_interp<<<dim3 (8, 1), 256, 0, c->stream>>> (c->pd_d, c->strips_d + c->strip_off[l] + i, set);
+    CKL ();
+  }
+  return ARCOS_OK;
+}
+
+int
+do_match (Ctx *c, int set)
+{
+  if (c->n_match == 0) return ARCOS_OK;
+  const int b = grid_blocks (c->n_match, 256, 1024);
+  k_match_gather<<<b, 256, 0, c->stream>>> (c->pool, c->match_src_d[set], c->n_match, c->match_tmp_d);
+  k_match_scatter<<<b, 256, 0, c->stream>>> (c->pool, c->match_dst_d[set], c->n_match, c->match_tmp_d);
+  CKL ();
+  return ARCOS_OK;
+}
+
+int
+do_prepare (Ctx *c, int set)
+{
+  int r;
+  if ((r = do_restrict (c, set))) return r;
+  if ((r = do_ext_bnd (c, set))) return r;
+  if ((r = do_set_bnd (c, set))) return r;
+  if ((r = do_match (c, set))) return r;
+  return do_periodic (c, set, 1);
+}
+
+int
+do_charge (Ctx *c, int set)
+{
+  long long w = 0;
+  for (auto &P : c->pd_h) w = std::max (w, P.asz);
+  return for_patches (c, w, [&] (dim3 g, const int *pl) {
+    k_charge<<<g, 256, 0, c->stream>>> (c->M, c->pd_d, pl, set);
+  });
+}
+
+// The on-device part of cdr_calc_field_r after the field solve: external
+// field, |E| (+ the root's field maxima) and theta periodicity.
+int
+do_field_post (Ctx *c, int set)
+{
+  const int np = (int) c->pd_h.size ();
+  // reset the per-set counters and maxima
+  {
+    std::vector<int> h (np * 2);
+    CK (cudaMemcpyAsync (h.data (), c->etz_d, sizeof (int) * np * 2, cudaMemcpyDeviceToHost, c->stream));
+    CK (cudaStreamSynchronize (c->stream));
+    for (int p = 0; p < np; p++) h[p * 2 + set] = 0;
+    CK (cudaMemcpyAsync (c->etz_d, h.data (), sizeof (int) * np * 2, cudaMemcpyHostToDevice, c->stream));
+    std::vector<DevState> st (c->nfam);
+    CK (cudaMemcpyAsync (st.data (), c->st_d, sizeof (DevState) * c->nfam, cudaMemcpyDeviceToHost, c->stream));
+    CK (cudaStreamSynchronize (c->stream));
+    for (auto &s : st)
+      for (int k = 0; k < 3; k++) s.emax_key[set][k] = dkey (-1.0);
+    CK (cudaMemcpyAsync (c->st_d, st.data (), sizeof (DevState) * c->nfam, cudaMemcpyHostToDevice, c->stream));
+    CK (cudaStreamSynchronize (c->stream));
+  }
+  long long w = 0;
+  for (auto &P : c->pd_h) w = std::max (w, P.asz);
+  const double *er = c->ext_d, *et = c->ext_d + c->nfam * ARCOS_MAXPLANES,
+               *ez = c->ext_d + 2 * c->nfam * ARCOS_MAXPLANES;
+  int r = for_patches (c, w, [&] (dim3 g, const int *pl) {
+    k_add_ext<<<g, 256, 0, c->stream>>> (c->pd_d, pl, set, er, et, ez, c->etz_d);
+  });
+  if (r) return r;
+  r = for_patches (c, w, [&] (dim3 g, const int *pl) {
+    k_eabs<<<g, 256, 0, c->stream>>> (c->pd_d, pl, set, c->st_d);
+  });
+  if (r) return r;
+  return do_periodic (c, set, 2);
+}
+
+int
+upload_field (Ctx *c, int gid, int set, const double *er, const double *ez, const double *et)
+{
+  const PatchDesc &P = c->pd_h[gid];
+  const size_t w = sizeof (double) * (P.nr + 4);
+  const size_t hgt = (size_t) (P.nz + 4) * P.planes;
+  const double *src[3] = {er, ez, et};
+  const int kinds[3] = {K_ER, K_EZ, K_ETHETA};
+  for (int k = 0; k < 3; k++) {
+    double *dst = P.arr (set, kinds[k]);
+    if (src[k])
+      CK (cudaMemcpy2DAsync (dst, sizeof (double) * P.pitch, src[k], w, w, hgt, cudaMemcpyHostToDevice, c->stream));
+    else
+      CK (cudaMemsetAsync (dst, 0, sizeof (double) * P.asz, c->stream));
+  }
+  return ARCOS_OK;
+}
+
+int
+read_states (Ctx *c, std::vector<DevState> &st)
+{
+  st.resize (c->nfam);
+  CK (cudaMemcpyAsync (st.data (), c->st_d, sizeof (DevState) * c->nfam, cudaMemcpyDeviceToHost, c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
+int
+check_state_errors (Ctx *c)
+{
+  std::vector<DevState> st;
+  int r = read_states (c, st);
+  if (r) return r;
+  for (int f = 0; f < c->nfam; f++) {
+    if (st[f].error & (1 << ARCOS_ERR_NAN))
+      return fail (ARCOS_ERR_NAN, "CFL maxima invalid (the assertion of cdr_courant, cdr.c:1023), family " + std::to_string (f));
+    if (st[f].error & (1 << ARCOS_ERR_SMALL_DT))
+      return fail (ARCOS_ERR_SMALL_DT, "too many steps below warn_min_timestep (cdr.c:1296-1302), family " + std::to_string (f));
+  }
+  return ARCOS_OK;
+}
+
+// field callback for the root of family 0 (the reference solves the field on the tree root)
+int
+field_from_callback (Ctx *c, int stage, int set)
+{
+  const PatchDesc &P = c->pd_h[0];
+  const size_t n = (size_t) (P.nr + 4) * (P.nz + 4) * P.planes;
+  std::vector<double> ch (n), er (n, 0.0), ez (n, 0.0), et (n, 0.0);
+  const size_t w = sizeof (double) * (P.nr + 4);
+  CK (cudaMemcpy2DAsync (ch.data (), w, P.arr (set, K_CHARGE), sizeof (double) * P.pitch, w,
+                         (size_t) (P.nz + 4) * P.planes, cudaMemcpyDeviceToHost, c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  if (c->fn (c->user, stage, ch.data (), er.data (), ez.data (), et.data ()))
+    return fail (ARCOS_ERR_ARG, "field callback returned an error");
+  int r = upload_field (c, 0, set, er.data (), ez.data (), et.data ());
+  if (r) return r;
+  return do_field_post (c, set);
+}
+
+int
+set_h_attempt (Ctx *c, double h)
+{
+  std::vector<DevState> st;
+  int r = read_states (c, st);
+  if (r) return r;
+  for (auto &s : st) s.h_attempt = h;
+  CK (cudaMemcpyAsync (c->st_d, st.data (), sizeof (DevState) * c->nfam, cudaMemcpyHostToDevice, c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
+int
+reset_dmax (Ctx *c, int slot_rel)
+{
+  std::vector<DevState> st;
+  int r = read_states (c, st);
+  if (r) return r;
+  for (auto &s : st) s.dmax_key[(s.step + slot_rel) & 1] = dkey (-1.0);
+  CK (cudaMemcpyAsync (c->st_d, st.data (), sizeof (DevState) * c->nfam, cudaMemcpyHostToDevice, c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
+int
+do_dmax (Ctx *c, int set, int slot_rel)
+{
+  long long w = 0;
+  for (auto &P : c->pd_h) w = std::max (w, (long long) P.nr * P.nz * P.ntheta);
+  return for_patches (c, w, [&] (dim3 g, const int *pl) {
+    k_dmax<<<g, 256, 0, c->stream>>> (c->M, c->pd_d, pl, set, c->st_d, slot_rel);
+  });
+}
+
+// One cdr_rk2 step on materialised arrays (any tree), state in set 0.
+int
+rk2_general (Ctx *c)
+{
+  int r;
+  StageArgs A = base_args (c);
+  if ((r = reset_dmax (c, 0))) return r;
+  if ((r = do_nonneg (c, 0))) return r;                 // cdr.c:1276
+  if ((r = do_prepare (c, 0))) return r;                // cdr.c:1279
+  if (c->fn && (r = field_from_callback (c, 0, 0))) return r;   // cdr.c:1283
+  A.nset = 0; A.dset = 0;
+  if ((r = run_stage (c, A, M_DERIV))) return r;        // cdr.c:1288
+  if ((r = do_dmax (c, 0, 0))) return r;                // cdr.c:1293
+  k_cfl<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->M, c->st_d, c->nfam, 0);
+  CKL ();
+  if ((r = for_patches (c, max_patch_work (c), [&] (dim3 g, const int *pl) {
+         k_update<<<g, 256, 0, c->stream>>> (c->pd_d, pl, 0, 1, c->st_d, 0.0, 1);
+       }))) return r;                                   // cdr.c:1308
+  if ((r = do_charge (c, 1))) return r;
+  if ((r = do_prepare (c, 1))) return r;                // cdr.c:1311
+  if (c->fn && (r = field_from_callback (c, 1, 1))) return r;   // cdr.c:1313
+  if ((r = run_stage (c, A, M_AMR2))) return r;         // cdr.c:1314-1317
+  if ((r = do_charge (c, 0))) return r;
+  if ((r = do_prepare (c, 0))) return r;                // cdr.c:1322
+  k_step_end<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->st_d, c->nfam);
+  CKL ();
+  return ARCOS_OK;
+}
+
+// The fused single-grid step: two launches, ghosts from the boundary
+// conditions, state moves from dens[src] to dens[1 - src].
+int
+rk2_fused_launches (Ctx *c, int src, int fold)
+{
+  StageArgs A = base_args (c);
+  A.src = src;
+  A.dst = 1 - src;
+  int r = run_stage (c, A, M_S1);
+  if (r) return r;
+  A.fam_state = 1;
+  A.cfl_fold = fold;
+  A.want_charge = c->fn ? 1 : 0;
+  return run_stage (c, A, M_S2);
+}
+
+}  // namespace
+
+// =============================== C ABI ==========================================
+extern "C" {
+
+const char *
+arcos_last_error (void)
+{
+  return g_err.c_str ();
+}
+
+int
+arcos_create (const arcos_params *p, void **out)
+{
+  if (!p || !out) return fail (ARCOS_ERR_ARG, "null argument");
+  if (p->no_species < 1 || p->no_species > 6)
+    return fail (ARCOS_ERR_ARG, "no_species must be 1..6 for the device kernels");
+  if (p->max_ntheta < 1 || p->max_ntheta > 64) return fail (ARCOS_ERR_ARG, "max_ntheta must be 1..64");
+  Ctx *c = new Ctx ();
+  c->p = *p;
+  Model &M = c->M;
+  M.ns = p->no_species;
+  for (int s = 0; s < M.ns; s++) {
+    M.charge[s] = p->charge[s];
+    M.mass[s] = p->mass[s];
+    M.mobile[s] = p->mass[s] > 0;
+  }
+  M.diffusion_coeff = p->diffusion_coeff;
+  M.nu_a = p->nu_a; M.nu_d = p->nu_d; M.nu_rt = p->nu_rt;
+  M.warn_min_timestep = p->warn_min_timestep;
+  M.z_cutoff = p->z_cutoff;
+  M.dtheta = 6.283185307179586477 / p->max_ntheta;   // cstream.c:38,305
+  M.bnd_sign[1] = p->cdr_bnd_right;
+  M.bnd_sign[2] = p->cdr_bnd_bottom;
+  M.bnd_sign[3] = p->cdr_bnd_top;
+  M.per_plane = p->per_plane;
+  // dr[], dz[] of init_gridsizes_a (cstream.c:276-306)
+  const int n = p->max_levels + p->extra_pois_levels + 1;
+  std::vector<double> drs (n), dzs (n);
+  drs[0] = (p->L_r / p->gridpoints_r) * (1 << p->extra_pois_levels);
+  dzs[0] = (p->L_z / p->gridpoints_z) * (1 << p->extra_pois_levels);
+  for (int i = 1; i < n; i++) { drs[i] = drs[i - 1] / 2.0; dzs[i] = dzs[i - 1] / 2.0; }
+  c->dr.assign (drs.begin () + p->extra_pois_levels, drs.end ());
+  c->dz.assign (dzs.begin () + p->extra_pois_levels, dzs.end ());
+  int dev = 0;
+  cudaGetDevice (&dev);
+  if (cudaStreamCreateWithFlags (&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail (ARCOS_ERR_CUDA, "cudaStreamCreateWithFlags failed");
+  }
+  c->own_stream = c->stream;
+  cudaDeviceGetAttribute (&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (c->num_sms <= 0) c->num_sms = 148;
+  *out = c;
+  return ARCOS_OK;
+}
+
+int
+arcos_destroy (void *ctx)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return ARCOS_OK;
+  if (c->graph2) cudaGraphExecDestroy (c->graph2);
+  cudaFree (c->pool); cudaFree (c->pd_d); cudaFree (c->nodes_d); cudaFree (c->st_d);
+  cudaFree (c->dtlog_d); cudaFree (c->etz_d); cudaFree (c->done_d); cudaFree (c->items_d);
+  cudaFree (c->plist_d); cudaFree (c->kids_d); cudaFree (c->strips_d); cudaFree (c->ext_d);
+  for (int s = 0; s < 2; s++) { cudaFree (c->match_src_d[s]); cudaFree (c->match_dst_d[s]); }
+  cudaFree (c->match_tmp_d);
+  if (c->own_stream) cudaStreamDestroy (c->own_stream);
+  delete c;
+  return ARCOS_OK;
+}
+
+int
+arcos_set_stream (void *ctx, void *stream)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  c->stream = stream ? (cudaStream_t) stream : c->own_stream;
+  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  return ARCOS_OK;
+}
+
+int
+arcos_add_reaction (void *ctx, int nin, const int *inputs, int nout, const int *outputs,
+                    double e_min, double e_step, int steps, double underflow,
+                    double overflow, const double *values)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  if (c->committed) return fail (ARCOS_ERR_STATE, "reactions must be added before arcos_commit");
+  Model &M = c->M;
+  if (M.nreact >= ARCOS_MAXR) return fail (ARCOS_ERR_ARG, "too many reactions");
+  if (nin < 0 || nin > ARCOS_MAXIN || nout < 0 || nout > ARCOS_MAXOUT)
+    return fail (ARCOS_ERR_ARG, "nin/nout out of range (reaction.h:10-11)");
+  if (steps < 1 || !values || !(e_step > 0)) return fail (ARCOS_ERR_ARG, "bad reaction table");
+  for (int i = 0; i < nin; i++)
+    if (inputs[i] < 0 || inputs[i] >= M.ns) return fail (ARCOS_ERR_ARG, "reaction input species out of range");
+  for (int i = 0; i < nout; i++)
+    if (outputs[i] < 0 || outputs[i] >= M.ns) return fail (ARCOS_ERR_ARG, "reaction output species out of range");
+  const int r = M.nreact++;
+  M.r_nin[r] = nin; M.r_nout[r] = nout;
+  for (int i = 0; i < nin; i++) M.r_in[r][i] = inputs[i];
+  for (int i = 0; i < nout; i++) M.r_out[r][i] = outputs[i];
+  M.r_steps[r] = steps;
+  M.r_e_min[r] = e_min; M.r_e_step[r] = e_step;
+  M.r_under[r] = underflow; M.r_over[r] = overflow;
+  M.r_node_off[r] = (int) c->nodes_h.size ();
+  // react_apply's updates in order (reaction.c:147-155): inputs (-rate) then
+  // outputs (+rate), only for charged species
+  int nop = 0;
+  for (int i = 0; i < nin + nout; i++) {
+    const int sp = i < nin ? inputs[i] : outputs[i - nin];
+    if (M.charge[sp] != 0.0) {
+      M.r_op_sp[r][nop] = (signed char) sp;
+      M.r_op_neg[r][nop] = (signed char) (i < nin);
+      nop++;
+    }
+  }
+  M.r_nops[r] = nop;
+  build_nodes (e_min, e_step, steps, values, c->nodes_h);
+  return ARCOS_OK;
+}
+
+int
+arcos_grid_new (void *ctx, int r0, int z0, int r1, int z1, int ntheta, int level,
+                int ext_bound, int parent, int *id)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  if (c->committed) return fail (ARCOS_ERR_STATE, "grids must be added before arcos_commit");
+  if (r1 - r0 < 2 || z1 - z0 < 2) return fail (ARCOS_ERR_ARG, "a grid needs at least 2x2 cells");
+  if (ntheta != c->p.max_ntheta) return fail (ARCOS_ERR_ARG, "ntheta must equal max_ntheta");
+  if (level < 0 || level > c->p.max_levels) return fail (ARCOS_ERR_ARG, "level out of range");
+  if (parent >= (int) c->g.size ()) return fail (ARCOS_ERR_ARG, "parent id out of range");
+  GridH g{r0, z0, r1, z1, ntheta, level, ext_bound, parent, 0, {}};
+  if (parent < 0) {
+    if (ext_bound & 1 && r0 != 0) return fail (ARCOS_ERR_ARG, "the axis boundary needs r0 == 0 (cdr.c:807)");
+    g.fam = c->nfam++;
+    c->fam_root.push_back ((int) c->g.size ());
+  } else {
+    const GridH &pg = c->g[parent];
+    if (level != pg.level + 1) return fail (ARCOS_ERR_ARG, "a child is one level below its parent");
+    g.fam = pg.fam;
+    if (r0 < 2 * pg.r0 - 2 || r1 > 2 * pg.r1 + 2 || z0 < 2 * pg.z0 - 2 || z1 > 2 * pg.z1 + 2)
+      return fail (ARCOS_ERR_ARG, "child outside its parent");
+    if (!(ext_bound & 1) && r0 < 2) return fail (ARCOS_ERR_ARG, "an inner left side needs r0 >= 2");
+    if ((r0 | z0 | r1 | z1) & 1)
+      return fail (ARCOS_ERR_ARG, "child corners must be even (ratio-2 refinement of parent cells)");
+  }
+  *id = (int) c->g.size ();
+  c->g.push_back (g);
+  if (parent >= 0) {
+    auto &k = c->g[parent].kids;
+    k.insert (k.begin (), *id);   // add_child prepends (tree.h:58-62)
+  }
+  return ARCOS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Resolves the sibling matching of cdr_match_r (cdr.c:1763-1800) into a gather.
+// The reference's copies run in a fixed order and a later copy may read a ghost
+// cell an earlier copy wrote; replaying the order symbolically gives, for every
+// written ghost cell, the cell whose pre-matching value it ends up with.
+struct MatchBuilder {
+  Ctx *c;
+  std::vector<std::pair<long long, long long>> ops;   // (dst key, src key) in order
+  long long k (int gid, int ir, int iz, int it, int s) {
+    const PatchDesc &P = c->pd_h[gid];
+    // encode as (gid, s, plane index, row, col) with generous strides
+    return (((long long) gid * 64 + s) * 128 + (it - P.theta0)) * 1048576LL * 4096
+           + (long long) (iz + 2) * 4096 + (ir + 2);
+  }
+  void copy_bnd (int fro, int to, int fr, int fz, int tr, int tz, int dim0, int inout, int dim1, int n1) {
+    // rz_copy_bnd with sign 1, inout_from == inout_to == inout (match_grids)
+    const PatchDesc &F = c->pd_h[fro];
+    for (int s = 0; s < F.ns; s++)
+      for (int i = 0; i < n1; i++)
+        for (int it = 0; it < F.ntheta; it++) {
+          int a_fr = fr, a_fz = fz, a_tr = tr, a_tz = tz;
+          if (dim1 == 1) { a_fz += i; a_tz += i; } else { a_fr += i; a_tr += i; }
+          for (int d = 1; d <= 2; d++) {
+            const int src_off = (d == 1) ? 0 : inout;     // from: p, p + inout
+            int sr = a_fr, sz = a_fz, dr_ = a_tr, dz_ = a_tz;
+            if (dim0 == 0) { sr += src_off; dr_ += d * inout; }
+            else { sz += src_off; dz_ += d * inout; }
+            ops.push_back ({k (to, dr_ - c->pd_h[to].r0, dz_ - c->pd_h[to].z0, it, s),
+                            k (fro, sr - F.r0, sz - F.z0, it, s)});
+          }
+        }
+  }
+  bool match_grids (int fro, int to) {
+    const GridH &f = c->g[fro], &t = c->g[to];
+    int x0, x1;
+    if (t.r1 == f.r0) {
+      x0 = std::max (t.z0 - 2, f.z0 - 2); x1 = std::min (t.z1 + 2, f.z1 + 2);
+      if (x1 <= x0) return false;
+      copy_bnd (fro, to, f.r0, x0, t.r1 - 1, x0, 0, +1, 1, x1 - x0);
+      return true;
+    }
+    if (t.r0 == f.r1) {
+      x0 = std::max (t.z0 - 2, f.z0 - 2); x1 = std::min (t.z1 + 2, f.z1 + 2);
+      if (x1 <= x0) return false;
+      copy_bnd (fro, to, f.r1 - 1, x0, t.r0, x0, 0, -1, 1, x1 - x0);
+      return true;
+    }
+    if (t.z1 == f.z0) {
+      x0 = std::max (t.r0 - 2, f.r0 - 2); x1 = std::min (t.r1 + 2, f.r1 + 2);
+      if (x1 <= x0) return false;
+      copy_bnd (fro, to, x0, f.z0, x0, t.z1 - 1, 1, +1, 0, x1 - x0);
+      return true;
+    }
+    if (t.z0 == f.z1) {
+      x0 = std::max (t.r0 - 2, f.r0 - 2); x1 = std::min (t.r1 + 2, f.r1 + 2);
+      if (x1 <= x0) return false;
+      copy_bnd (fro, to, x0, f.z1 - 1, x0, t.z0, 1, -1, 0, x1 - x0);
+      return true;
+    }
+    return false;
+  }
+  void match_r (int g1, int g2) {
+    bool m = true;
+    if (g2 >= 0) m = match_grids (g1, g2);
+    if (!m) return;
+    for (int c1 : c->g[g1].kids) {
+      for (int c2 : c->g[g1].kids) match_r (c1, c1 != c2 ? c2 : -1);
+      if (g2 < 0) continue;
+      for (int c2 : c->g[g2].kids) match_r (c1, c2);
+    }
+  }
+};
+
+long long
+elem_offset (Ctx *c, long long key, int set)
+{
+  const long long col = key % 4096;
+  const long long row = (key / 4096) % 1048576;
+  const long long rest = key / 4096 / 1048576;
+  const int plane = (int) (rest % 128);
+  const int s = (int) ((rest / 128) % 64);
+  const int gid = (int) (rest / 128 / 64);
+  if (gid < 0 || gid >= (int) c->pd_h.size ()) return -1;
+  const PatchDesc &P = c->pd_h[gid];
+  if (col >= P.nr + 4 || row >= P.nz + 4 || plane >= P.planes || s >= P.ns) return -1;
+  return (P.arr (set, K_DENS, s) - c->pool) + col + row * P.pitch + plane * P.plane_stride;
+}
+
+// Work list of the tile kernel: per patch, per real plane, tiles of 32 columns
+// by TY rows (TY from the tile shape).
+int
+build_items (Ctx *c)
+{
+  const int np = (int) c->pd_h.size ();
+  const int ty = TILE_WY[c->tile_cfg] * TILE_RPW[c->tile_cfg];
+  std::vector<WorkItem> items;
+  c->item_off.assign (np, 0);
+  c->item_cnt.assign (np, 0);
+  for (int i = 0; i < np; i++) {
+    const PatchDesc &P = c->pd_h[i];
+    c->item_off[i] = (int) items.size ();
+    for (int zb = 0; zb < P.nz; zb += ty)
+      for (int pl = 0; pl < P.ntheta; pl++)
+        for (int c0 = 0; c0 < P.nr; c0 += TX)
+          items.push_back ({i, pl, c0, std::min (TX, P.nr - c0), zb, std::min (ty, P.nz - zb)});
+    c->item_cnt[i] = (int) items.size () - c->item_off[i];
+  }
+  c->n_items = (int) items.size ();
+  cudaFree (c->items_d);
+  c->items_d = nullptr;
+  CK (cudaMalloc (&c->items_d, sizeof (WorkItem) * items.size ()));
+  CK (cudaMemcpy (c->items_d, items.data (), sizeof (WorkItem) * items.size (), cudaMemcpyHostToDevice));
+  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  return ARCOS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int
+arcos_commit (void *ctx)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r_ = 0;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  if (c->committed) return fail (ARCOS_ERR_STATE, "already committed");
+  if (c->g.empty ()) return fail (ARCOS_ERR_ARG, "no grids");
+  const int np = (int) c->g.size ();
+  const int ns = c->M.ns;
+  // patch descriptors and the storage pool
+  size_t total = 0;
+  c->pd_h.resize (np);
+  for (int i = 0; i < np; i++) {
+    const GridH &g = c->g[i];
+    PatchDesc &P = c->pd_h[i];
+    P.nr = g.r1 - g.r0; P.nz = g.z1 - g.z0; P.ntheta = g.ntheta;
+    P.planes = g.ntheta == 1 ? 1 : g.ntheta + 4;
+    P.theta0 = g.ntheta == 1 ? 0 : -2;
+    P.r0 = g.r0; P.z0 = g.z0; P.level = g.level; P.ext_bound = g.ext_bound;
+    P.pitch = ((P.nr + 6) + 3) / 4 * 4;    // 16-byte staging chunks may touch column nr+2
+    P.ns = ns; P.parent = g.parent; P.fam = g.fam;
+    P.plane_stride = (long long) P.pitch * (P.nz + 4);
+    P.asz = (P.plane_stride * P.planes + 31) / 32 * 32;
+    P.dr = c->dr[g.level]; P.dz = c->dz[g.level];
+    c->max_level = std::max (c->max_level, g.level);
+    total += (size_t) P.asz * 2 * (2 * ns + 5);
+  }
+  CK (cudaMalloc (&c->pool, total * sizeof (double)));
+  CK (cudaMemsetAsync (c->pool, 0, total * sizeof (double), c->stream));
+  c->pool_doubles = total;
+  size_t off = 0;
+  for (int i = 0; i < np; i++) {
+    c->pd_h[i].base = c->pool + off;
+    off += (size_t) c->pd_h[i].asz * 2 * (2 * ns + 5);
+  }
+  CK (cudaMalloc (&c->pd_d, sizeof (PatchDesc) * np));
+  CK (cudaMemcpyAsync (c->pd_d, c->pd_h.data (), sizeof (PatchDesc) * np, cudaMemcpyHostToDevice, c->stream));
+  // tables
+  if (!c->nodes_h.empty ()) {
+    CK (cudaMalloc (&c->nodes_d, sizeof (TableNode) * c->nodes_h.size ()));
+    CK (cudaMemcpyAsync (c->nodes_d, c->nodes_h.data (), sizeof (TableNode) * c->nodes_h.size (), cudaMemcpyHostToDevice, c->stream));
+  }
+  if ((r_ = build_items (c))) return r_;
+  std::vector<int> pl (np);
+  for (int i = 0; i < np; i++) pl[i] = i;
+  CK (cudaMalloc (&c->plist_d, sizeof (int) * np));
+  CK (cudaMemcpyAsync (c->plist_d, pl.data (), sizeof (int) * np, cudaMemcpyHostToDevice, c->stream));
+  // children per level (restriction) and ghost strips per level (interpolation)
+  std::vector<int> kids;
+  std::vector<StripDesc> strips;
+  c->level_off.assign (c->max_level + 1, 0);
+  c->level_cnt.assign (c->max_level + 1, 0);
+  c->strip_off.assign (c->max_level + 1, 0);
+  c->strip_cnt.assign (c->max_level + 1, 0);
+  for (int l = 1; l <= c->max_level; l++) {
+    c->level_off[l] = (int) kids.size ();
+    c->strip_off[l] = (int) strips.size ();
+    for (int i = 0; i < np; i++) {
+      const GridH &g = c->g[i];
+      if (g.level != l || g.parent < 0) continue;
+      kids.push_back (i);
+      // cdr_set_bnd (cdr.c:1911-1938): top, bottom, left, right guest strips
+      if (!(g.ext_bound & 8)) strips.push_back ({i, g.r0 - 2, g.z1, g.r1 + 2, g.z1 + 2});
+      if (!(g.ext_bound & 4)) strips.push_back ({i, g.r0 - 2, g.z0 - 2, g.r1 + 2, g.z0});
+      if (!(g.ext_bound & 1)) strips.push_back ({i, g.r0 - 2, g.z0, g.r0, g.z1});
+      if (!(g.ext_bound & 2)) strips.push_back ({i, g.r1, g.z0, g.r1 + 2, g.z1});
+    }
+    c->level_cnt[l] = (int) kids.size () - c->level_off[l];
+    c->strip_cnt[l] = (int) strips.size () - c->strip_off[l];
+  }
+  if (!kids.empty ()) {
+    CK (cudaMalloc (&c->kids_d, sizeof (int) * kids.size ()));
+    CK (cudaMemcpyAsync (c->kids_d, kids.data (), sizeof (int) * kids.size (), cudaMemcpyHostToDevice, c->stream));
+  }
+  if (!strips.empty ()) {
+    CK (cudaMalloc (&c->strips_d, sizeof (StripDesc) * strips.size ()));
+    CK (cudaMemcpyAsync (c->strips_d, strips.data (), sizeof (StripDesc) * strips.size (), cudaMemcpyHostToDevice, c->stream));
+  }
+  // sibling matching, resolved
+  {
+    MatchBuilder mb{c, {}};
+    for (int f = 0; f < c->nfam; f++) mb.match_r (c->fam_root[f], -1);
+    // replay: current[key] = source key of the value now held
+    std::vector<std::pair<long long, long long>> &ops = mb.ops;
+    std::vector<long long> dst_keys;
+    std::vector<long long> src_keys;
+    {
+      // map from key to resolved source key, kept as a sorted vector rebuilt lazily
+      std::vector<std::pair<long long, long long>> cur;   // (key, resolved src)
+      auto find = [&] (long long k) -> long long {
+        for (auto it = cur.rbegin (); it != cur.rend (); ++it)
+          if (it->first == k) return it->second;
+        return k;
+      };
+      // the op list is usually short (2 layers x face length x species); a linear
+      // scan from the back keeps the last write semantics
+      for (auto &op : ops) cur.push_back ({op.first, find (op.second)});
+      // last write per destination
+      std::vector<std::pair<long long, long long>> last;
+      for (auto it = cur.rbegin (); it != cur.rend (); ++it) {
+        bool seen = false;
+        for (auto &l : last) if (l.first == it->first) { seen = true; break; }
+        if (!seen) last.push_back (*it);
+      }
+      for (auto &l : last) { dst_keys.push_back (l.first); src_keys.push_back (l.second); }
+    }
+    c->n_match = (int) dst_keys.size ();
+    if (c->n_match) {
+      for (int s = 0; s < 2; s++) {
+        std::vector<long long> so (c->n_match), dof (c->n_match);
+        for (int i = 0; i < c->n_match; i++) {
+          so[i] = elem_offset (c, src_keys[i], s);
+          dof[i] = elem_offset (c, dst_keys[i], s);
+          if (so[i] < 0 || dof[i] < 0)
+            return fail (ARCOS_ERR_ARG, "sibling matching reaches outside a grid's ghost extent");
+        }
+        CK (cudaMalloc (&c->match_src_d[s], sizeof (long long) * c->n_match));
+        CK (cudaMalloc (&c->match_dst_d[s], sizeof (long long) * c->n_match));
+        CK (cudaMemcpy (c->match_src_d[s], so.data (), sizeof (long long) * c->n_match, cudaMemcpyHostToDevice));
+        CK (cudaMemcpy (c->match_dst_d[s], dof.data (), sizeof (long long) * c->n_match, cudaMemcpyHostToDevice));
+      }
+      CK (cudaMalloc (&c->match_tmp_d, sizeof (double) * c->n_match));
+    }
+  }
+  // families: device state, CFL constants (cdr.c:981-986, grid.c:15-44)
+  std::vector<DevState> st (c->nfam);
+  c->dt_cap = 1 << 16;
+  CK (cudaMalloc (&c->dtlog_d, sizeof (double) * c->dt_cap * c->nfam));
+  for (int f = 0; f < c->nfam; f++) {
+    DevState &s = st[f];
+    memset (&s, 0, sizeof (s));
+    s.h_attempt = 1e300;
+    s.dmax_key[0] = s.dmax_key[1] = dkey (-1.0);
+    for (int a = 0; a < 2; a++) for (int k = 0; k < 3; k++) s.emax_key[a][k] = dkey (-1.0);
+    int depth = 0;
+    double rmin = 1e300;
+    bool first = true;
+    for (int i = 0; i < np; i++) {
+      if (c->g[i].fam != f) continue;
+      depth = std::max (depth, c->g[i].level);
+      const double r = ((double) c->g[i].r0 + 0.5) * c->dr[c->g[i].level];
+      if (first || r < rmin) rmin = r;
+      first = false;
+    }
+    // grid_rmin_r: root first, then children recursively with (minr > cminr) ? cminr : minr
+    s.courant_const[0] = c->dr[depth];
+    s.courant_const[1] = c->dz[depth];
+    s.courant_const[2] = (6.283185307179586477 / c->p.max_ntheta) * rmin;
+    s.courant_const[3] = (c->p.max_ntheta == 1) ? 0.0 : 1.0;
+    s.dt_cap = c->dt_cap;
+    s.dt_log = c->dtlog_d + (size_t) f * c->dt_cap;
+  }
+  CK (cudaMalloc (&c->st_d, sizeof (DevState) * c->nfam));
+  CK (cudaMemcpyAsync (c->st_d, st.data (), sizeof (DevState) * c->nfam, cudaMemcpyHostToDevice, c->stream));
+  CK (cudaMalloc (&c->etz_d, sizeof (int) * np * 2));
+  CK (cudaMemsetAsync (c->etz_d, 0, sizeof (int) * np * 2, c->stream));
+  CK (cudaMalloc (&c->done_d, sizeof (unsigned)));
+  CK (cudaMemsetAsync (c->done_d, 0, sizeof (unsigned), c->stream));
+  // applied field per family and plane (e0_r / e0_z / e0_theta, cstream.c:435-455)
+  c->famE.assign (3 * c->nfam, 0.0);
+  for (int f = 0; f < c->nfam; f++) {
+    c->famE[3 * f] = c->p.E_x; c->famE[3 * f + 1] = c->p.E_y; c->famE[3 * f + 2] = c->p.E_z;
+  }
+  CK (cudaMalloc (&c->ext_d, sizeof (double) * (2 * c->nfam * ARCOS_MAXPLANES + c->nfam)));
+  c->committed = true;
+  // write the ext table
+  std::vector<double> ext (2 * c->nfam * ARCOS_MAXPLANES + c->nfam, 0.0);
+  const double dth = 6.283185307179586477 / c->p.max_ntheta;
+  const int nplanes = c->p.max_ntheta == 1 ? 1 : c->p.max_ntheta + 4;
+  const int th0 = c->p.max_ntheta == 1 ? 0 : -2;
+  for (int f = 0; f < c->nfam; f++) {
+    const double Ex = c->famE[3 * f], Ey = c->famE[3 * f + 1], Ez = c->famE[3 * f + 2];
+    for (int pl = 0; pl < nplanes; pl++) {
+      const int it = pl + th0;
+      const double th = (double) it * dth, tht = ((double) it + 0.5) * dth;
+      ext[f * ARCOS_MAXPLANES + pl] = Ex * cos (th) + Ey * sin (th);
+      ext[c->nfam * ARCOS_MAXPLANES + f * ARCOS_MAXPLANES + pl] = -Ex * cos (tht) + Ey * sin (tht);
+    }
+    ext[2 * c->nfam * ARCOS_MAXPLANES + f] = Ez;
+  }
+  CK (cudaMemcpy (c->ext_d, ext.data (), sizeof (double) * ext.size (), cudaMemcpyHostToDevice));
+  // the fused path needs single-grid families with every side external
+  c->fused_ok = true;
+  for (int i = 0; i < np; i++)
+    if (c->g[i].parent >= 0 || c->g[i].ext_bound != 15 || c->g[i].r0 != 0) c->fused_ok = false;
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
+int
+arcos_device_bytes (void *ctx, size_t *bytes)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  *bytes = c->pool_doubles * sizeof (double);
+  return ARCOS_OK;
+}
+
+// Sets the applied field of one family (per-instance E0, e.g. a batch of runs).
+int
+arcos_set_family_field (void *ctx, int fam, double Ex, double Ey, double Ez)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (fam < 0 || fam >= c->nfam) return fail (ARCOS_ERR_ARG, "family out of range");
+  const double dth = 6.283185307179586477 / c->p.max_ntheta;
+  const int nplanes = c->p.max_ntheta == 1 ? 1 : c->p.max_ntheta + 4;
+  const int th0 = c->p.max_ntheta == 1 ? 0 : -2;
+  std::vector<double> er (ARCOS_MAXPLANES, 0.0), et (ARCOS_MAXPLANES, 0.0);
+  for (int pl = 0; pl < nplanes; pl++) {
+    const int it = pl + th0;
+    const double th = (double) it * dth, tht = ((double) it + 0.5) * dth;
+    er[pl] = Ex * cos (th) + Ey * sin (th);
+    et[pl] = -Ex * cos (tht) + Ey * sin (tht);
+  }
+  c->famE[3 * fam] = Ex; c->famE[3 * fam + 1] = Ey; c->famE[3 * fam + 2] = Ez;
+  CK (cudaMemcpy (c->ext_d + fam * ARCOS_MAXPLANES, er.data (), sizeof (double) * ARCOS_MAXPLANES, cudaMemcpyHostToDevice));
+  CK (cudaMemcpy (c->ext_d + c->nfam * ARCOS_MAXPLANES + fam * ARCOS_MAXPLANES, et.data (), sizeof (double) * ARCOS_MAXPLANES, cudaMemcpyHostToDevice));
+  CK (cudaMemcpy (c->ext_d + 2 * c->nfam * ARCOS_MAXPLANES + fam, &Ez, sizeof (double), cudaMemcpyHostToDevice));
+  return ARCOS_OK;
+}
+
+static int
+kind_ok (int kind, int species, int ns)
+{
+  if (kind < ARCOS_DENS || kind > ARCOS_CHARGE) return 0;
+  if ((kind == ARCOS_DENS || kind == ARCOS_D_DENS) && (species < 0 || species >= ns)) return 0;
+  return 1;
+}
+
+int
+arcos_upload (void *ctx, int grid, int set, int kind, int species, const double *host)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (grid < 0 || grid >= (int) c->pd_h.size () || set < 0 || set > 1 || !host || !kind_ok (kind, species, c->M.ns))
+    return fail (ARCOS_ERR_ARG, "arcos_upload: bad argument");
+  const PatchDesc &P = c->pd_h[grid];
+  const size_t w = sizeof (double) * (P.nr + 4);
+  CK (cudaMemcpy2DAsync (P.arr (set, kind, species), sizeof (double) * P.pitch, host, w, w,
+                         (size_t) (P.nz + 4) * P.planes, cudaMemcpyHostToDevice, c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
+int
+arcos_download (void *ctx, int grid, int set, int kind, int species, double *host)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (grid < 0 || grid >= (int) c->pd_h.size () || set < 0 || set > 1 || !host || !kind_ok (kind, species, c->M.ns))
+    return fail (ARCOS_ERR_ARG, "arcos_download: bad argument");
+  const PatchDesc &P = c->pd_h[grid];
+  const size_t w = sizeof (double) * (P.nr + 4);
+  CK (cudaMemcpy2DAsync (host, w, P.arr (set, kind, species), sizeof (double) * P.pitch, w,
+                         (size_t) (P.nz + 4) * P.planes, cudaMemcpyDeviceToHost, c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
+int
+arcos_sync (void *ctx)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
+int
+arcos_set_field (void *ctx, int grid, int set, const double *er, const double *ez,
+                 const double *etheta)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (grid < 0 || grid >= (int) c->pd_h.size () || set < 0 || set > 1)
+    return fail (ARCOS_ERR_ARG, "arcos_set_field: bad grid or set");
+  if ((r = upload_field (c, grid, set, er, ez, etheta))) return r;
+  c->field_set[set] = true;
+  return ARCOS_OK;
+}
+
+// Applies the external field, |E| and periodicity to set `set` after all
+// grids' fields were uploaded (the rest of cdr_calc_field_r).
+int
+arcos_field_post (void *ctx, int set)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if ((r = do_field_post (c, set))) return r;
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
+int
+arcos_set_field_fn (void *ctx, arcos_field_fn fn, void *user)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  c->fn = fn;
+  c->user = user;
+  return ARCOS_OK;
+}
+
+int
+arcos_set_per_patch (void *ctx, int on)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  c->per_patch = on != 0;
+  return ARCOS_OK;
+}
+
+#define SET_OK(set_) if ((set_) < 0 || (set_) > 1) return fail (ARCOS_ERR_ARG, "set must be 0 or 1")
+
+int arcos_cdr_nonegative_r (void *ctx, int set)
+{ Ctx *c = (Ctx *) ctx; int r = chk_committed (c); if (r) return r; SET_OK (set); return do_nonneg (c, set); }
+int arcos_cdr_set_ext_bnd_r (void *ctx, int set)
+{ Ctx *c = (Ctx *) ctx; int r = chk_committed (c); if (r) return r; SET_OK (set); return do_ext_bnd (c, set); }
+int arcos_cdr_set_periodic_r (void *ctx, int set)
+{ Ctx *c = (Ctx *) ctx; int r = chk_committed (c); if (r) return r; SET_OK (set); return do_periodic (c, set, 3); }
+int arcos_cdr_restrict_r (void *ctx, int set)
+{ Ctx *c = (Ctx *) ctx; int r = chk_committed (c); if (r) return r; SET_OK (set); return do_restrict (c, set); }
+int arcos_cdr_set_bnd_r (void *ctx, int set)
+{ Ctx *c = (Ctx *) ctx; int r = chk_committed (c); if (r) return r; SET_OK (set); return do_set_bnd (c, set); }
+int arcos_cdr_match_r (void *ctx, int set)
+{ Ctx *c = (Ctx *) ctx; int r = chk_committed (c); if (r) return r; SET_OK (set); return do_match (c, set); }
+int arcos_prepare_grid (void *ctx, int set)
+{ Ctx *c = (Ctx *) ctx; int r = chk_committed (c); if (r) return r; SET_OK (set); return do_prepare (c, set); }
+int arcos_cdr_calc_charge_r (void *ctx, int set)
+{ Ctx *c = (Ctx *) ctx; int r = chk_committed (c); if (r) return r; SET_OK (set); return do_charge (c, set); }
+
+int
+arcos_cdr_add_ext_field_r (void *ctx, int set)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  SET_OK (set);
+  long long w = 0;
+  for (auto &P : c->pd_h) w = std::max (w, P.asz);
+  const double *er = c->ext_d, *et = c->ext_d + c->nfam * ARCOS_MAXPLANES,
+               *ez = c->ext_d + 2 * c->nfam * ARCOS_MAXPLANES;
+  return for_patches (c, w, [&] (dim3 g, const int *pl) {
+    k_add_ext<<<g, 256, 0, c->stream>>> (c->pd_d, pl, set, er, et, ez, c->etz_d);
+  });
+}
+
+int
+arcos_cdr_calc_eabs_r (void *ctx, int set)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  SET_OK (set);
+  long long w = 0;
+  for (auto &P : c->pd_h) w = std::max (w, P.asz);
+  return for_patches (c, w, [&] (dim3 g, const int *pl) {
+    k_eabs<<<g, 256, 0, c->stream>>> (c->pd_d, pl, set, c->st_d);
+  });
+}
+
+// react_apply_all alone: d_dens = reactions (interior), no drift/diffusion.
+int
+arcos_react_apply_all (void *ctx, int set)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  SET_OK (set);
+  // the derivative kernel with every species treated as immobile
+  Model M = c->M;
+  for (int s = 0; s < M.ns; s++) M.mobile[s] = 0;
+  Model keep = c->M;
+  c->M = M;
+  StageArgs A = base_args (c);
+  A.nset = set; A.dset = set;
+  r = run_stage (c, A, M_DERIV);
+  c->M = keep;
+  return r;
+}
+
+// cdr_advect_diffu_r alone: d_dens += drift/diffusion divergence.
+int
+arcos_cdr_advect_diffu_r (void *ctx, int set)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  SET_OK (set);
+  StageArgs A = base_args (c);
+  A.nset = set; A.dset = set; A.accumulate = 1;
+  return run_stage (c, A, M_DERIV);
+}
+
+int
+arcos_cdr_calc_d_dens (void *ctx, int set)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  SET_OK (set);
+  StageArgs A = base_args (c);
+  A.nset = set; A.dset = set;
+  return run_stage (c, A, M_DERIV);
+}
+
+int
+arcos_cdr_courant (void *ctx, int set, double *h)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  SET_OK (set);
+  if ((r = set_h_attempt (c, 1e300))) return r;
+  if ((r = reset_dmax (c, 0))) return r;
+  if ((r = do_dmax (c, set, 0))) return r;
+  // cfl_step logs and counts; run it on a copy of the state
+  std::vector<DevState> keep;
+  if ((r = read_states (c, keep))) return r;
+  k_cfl<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->M, c->st_d, c->nfam, set);
+  CKL ();
+  std::vector<DevState> st;
+  if ((r = read_states (c, st))) return r;
+  *h = st[0].h;
+  const int err = st[0].error & (1 << ARCOS_ERR_NAN);
+  CK (cudaMemcpy (c->st_d, keep.data (), sizeof (DevState) * c->nfam, cudaMemcpyHostToDevice));
+  if (err) return fail (ARCOS_ERR_NAN, "CFL maxima invalid (cdr.c:1023)");
+  return ARCOS_OK;
+}
+
+int
+arcos_cdr_update (void *ctx, double h)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if ((r = for_patches (c, max_patch_work (c), [&] (dim3 g, const int *pl) {
+         k_update<<<g, 256, 0, c->stream>>> (c->pd_d, pl, 0, 1, c->st_d, h, 0);
+       }))) return r;
+  return do_charge (c, 1);
+}
+
+int
+arcos_cdr_rk2_update (void *ctx, double h)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if ((r = for_patches (c, max_patch_work (c), [&] (dim3 g, const int *pl) {
+         k_rk2_update<<<g, 256, 0, c->stream>>> (c->pd_d, pl, c->st_d, h, 0);
+       }))) return r;
+  return do_charge (c, 0);
+}
+
+int
+arcos_cdr_rk2 (void *ctx, double h, double t, double *h_used)
+{
+  Ctx *c = (Ctx *) ctx;
+  (void) t;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (!c->fn && !(c->field_set[0] && c->field_set[1]))
+    return fail (ARCOS_ERR_STATE, "no field: call arcos_set_field (+ arcos_field_post) for both sets, or arcos_set_field_fn");
+  if ((r = set_h_attempt (c, h))) return r;
+  if ((r = rk2_general (c))) return r;
+  CK (cudaStreamSynchronize (c->stream));
+  std::vector<DevState> st;
+  if ((r = read_states (c, st))) return r;
+  if (h_used) *h_used = st[0].h;
+  return check_state_errors (c);
+}
+
+// nsteps fused steps (single-grid families, fixed field or callback).
+int
+arcos_run (void *ctx, int nsteps, double h, double *dt_out)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (nsteps < 0) return fail (ARCOS_ERR_ARG, "nsteps < 0");
+  if (!c->fn && !(c->field_set[0] && c->field_set[1]))
+    return fail (ARCOS_ERR_STATE, "no field: call arcos_set_field (+ arcos_field_post) for both sets, or arcos_set_field_fn");
+  std::vector<DevState> st0;
+  if ((r = read_states (c, st0))) return r;
+  const int step0 = st0[0].step;
+  if ((r = set_h_attempt (c, h))) return r;
+  if (!c->fused_ok) {
+    for (int k = 0; k < nsteps; k++)
+      if ((r = rk2_general (c))) return r;
+  } else if (c->fn) {
+    // field in the loop: the host solve sits between the stages
+    for (int k = 0; k < nsteps; k++) {
+      if ((r = field_from_callback (c, 0, 0))) return r;
+      if ((r = reset_dmax (c, 0))) return r;
+      if ((r = do_dmax (c, 0, 0))) return r;
+      k_cfl<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->M, c->st_d, c->nfam, 0);
+      CKL ();
+      StageArgs A = base_args (c);
+      A.src = 0;
+      if ((r = run_stage (c, A, M_S1))) return r;
+      long long w = 0;
+      for (auto &P : c->pd_h) w = std::max (w, P.asz);
+      if ((r = for_patches (c, w, [&] (dim3 g, const int *pl) {
+             k_charge_star<<<g, 256, 0, c->stream>>> (c->M, c->pd_d, pl, 0, c->st_d);
+           }))) return r;
+      if ((r = field_from_callback (c, 1, 1))) return r;
+      A.dst = 1; A.fam_state = 0; A.want_charge = 1;
+      if ((r = run_stage (c, A, M_S2))) return r;
+      // move the state back to set 0 (the callback path keeps it there)
+      for (auto &P : c->pd_h) {
+        CK (cudaMemcpyAsync (P.arr (0, K_DENS, 0), P.arr (1, K_DENS, 0), sizeof (double) * P.asz * P.ns, cudaMemcpyDeviceToDevice, c->stream));
+        CK (cudaMemcpyAsync (P.arr (0, K_CHARGE), P.arr (1, K_CHARGE), sizeof (double) * P.asz, cudaMemcpyDeviceToDevice, c->stream));
+      }
+      k_step_end<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->st_d, c->nfam);
+      CKL ();
+    }
+    // ghosts of the final state as prepare_grid leaves them (cdr.c:1322)
+    if ((r = do_ext_bnd (c, 0))) return r;
+    if ((r = do_periodic (c, 0, 1))) return r;
+  } else {
+    // fixed field: h of the first step from the current state, then pairs of
+    // steps replayed from a CUDA graph (state 0 -> 1 -> 0)
+    if ((r = reset_dmax (c, 0))) return r;
+    if ((r = do_dmax (c, 0, 0))) return r;
+    k_cfl<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->M, c->st_d, c->nfam, 0);
+    CKL ();
+    const int pairs = nsteps / 2;
+    if (pairs > 0) {
+      if (!c->graph2) {
+        cudaGraph_t gr;
+        CK (cudaStreamBeginCapture (c->stream, cudaStreamCaptureModeThreadLocal));
+        int e1 = rk2_fused_launches (c, 0, 1);
+        int e2 = e1 ? e1 : rk2_fused_launches (c, 1, 1);
+        cudaError_t ee = cudaStreamEndCapture (c->stream, &gr);
+        if (e2) return e2;
+        if (ee != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("graph capture: ") + cudaGetErrorString (ee));
+        CK (cudaGraphInstantiate (&c->graph2, gr, 0));
+        cudaGraphDestroy (gr);
+      }
+      for (int k = 0; k < pairs; k++) CK (cudaGraphLaunch (c->graph2, c->stream));
+    }
+    if (nsteps & 1) {
+      if ((r = rk2_fused_launches (c, 0, 1))) return r;
+      for (auto &P : c->pd_h)
+        CK (cudaMemcpyAsync (P.arr (0, K_DENS, 0), P.arr (1, K_DENS, 0), sizeof (double) * P.asz * P.ns, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    // ghosts of the final state as prepare_grid leaves them (cdr.c:1322)
+    if ((r = do_ext_bnd (c, 0))) return r;
+    if ((r = do_periodic (c, 0, 1))) return r;
+  }
+  CK (cudaStreamSynchronize (c->stream));
+  if (dt_out && nsteps > 0) {
+    for (int f = 0; f < c->nfam; f++) {
+      const int n = std::min (nsteps, std::max (0, c->dt_cap - step0));
+      CK (cudaMemcpy (dt_out + (size_t) f * nsteps, c->dtlog_d + (size_t) f * c->dt_cap + step0,
+                      sizeof (double) * n, cudaMemcpyDeviceToHost));
+    }
+  }
+  return check_state_errors (c);
+}
+
+// Enqueues nsteps fused steps without synchronising or error checks (for
+// timing inside a caller's CUDA-event bracket).  Requires an even nsteps,
+// a fixed field and single-grid families; the first step's h must have been
+// prepared by arcos_run_prepare.
+int
+arcos_run_prepare (void *ctx, double h)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (!c->fused_ok) return fail (ARCOS_ERR_STATE, "fused path needs single-grid families");
+  if ((r = set_h_attempt (c, h))) return r;
+  if ((r = reset_dmax (c, 0))) return r;
+  if ((r = do_dmax (c, 0, 0))) return r;
+  k_cfl<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->M, c->st_d, c->nfam, 0);
+  CKL ();
+  if (!c->graph2) {
+    cudaGraph_t gr;
+    CK (cudaStreamBeginCapture (c->stream, cudaStreamCaptureModeThreadLocal));
+    int e1 = rk2_fused_launches (c, 0, 1);
+    int e2 = e1 ? e1 : rk2_fused_launches (c, 1, 1);
+    cudaError_t ee = cudaStreamEndCapture (c->stream, &gr);
+    if (e2) return e2;
+    if (ee != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("graph capture: ") + cudaGetErrorString (ee));
+    CK (cudaGraphInstantiate (&c->graph2, gr, 0));
+    cudaGraphDestroy (gr);
+  }
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
+int
+arcos_run_enqueue (void *ctx, int nsteps)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (!c->graph2 || (nsteps & 1)) return fail (ARCOS_ERR_STATE, "call arcos_run_prepare; nsteps must be even");
+  for (int k = 0; k < nsteps / 2; k++) CK (cudaGraphLaunch (c->graph2, c->stream));
+  return ARCOS_OK;
+}
+
+// Enqueues one stage kernel (for timing a single kernel): mode 1 = stage 1,
+// 2 = stage 2 (with the CFL fold).
+int
+arcos_enqueue_stage (void *ctx, int mode, int src)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  StageArgs A = base_args (c);
+  A.src = src; A.dst = 1 - src;
+  if (mode == 2) { A.fam_state = 1; A.cfl_fold = 1; }
+  return run_stage (c, A, mode == 1 ? M_S1 : M_S2);
+}
+
+// Per-family steps taken so far and the error bits.
+int
+arcos_family_state (void *ctx, int fam, int *steps, double *h, int *error_bits)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (fam < 0 || fam >= c->nfam) return fail (ARCOS_ERR_ARG, "family out of range");
+  std::vector<DevState> st;
+  if ((r = read_states (c, st))) return r;
+  if (steps) *steps = st[fam].step;
+  if (h) *h = st[fam].h;
+  if (error_bits) *error_bits = st[fam].error;
+  return ARCOS_OK;
+}
+
+int
+arcos_num_items (void *ctx)
+{
+  Ctx *c = (Ctx *) ctx;
+  return c ? c->n_items : -1;
+}
+
+// Tile shape of the stencil kernel (0: 32x16 cells, 128 threads; 1: 32x32,
+// 128 threads; 2: 32x32, 256 threads).  May be changed after arcos_commit.
+int
+arcos_set_tile (void *ctx, int cfg)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  if (cfg < 0 || cfg >= N_TILE_CFG) return fail (ARCOS_ERR_ARG, "tile shape out of range");
+  c->tile_cfg = cfg;
+  if (c->committed) return build_items (c);
+  return ARCOS_OK;
+}
+
+int
+arcos_get_tile (void *ctx)
+{
+  Ctx *c = (Ctx *) ctx;
+  return c ? c->tile_cfg : -1;
+}
+
+// ---- narrow seam: arcos_cdr_advect_vec ------------------------------------------
+// One species, one 2-D slab, no reactions: the derivative kernel in
+// accumulate mode on a one-grid context whose ghosts are read from memory.
+// The context is cached and rebuilt when the slab shape changes.
+static Ctx *seam_ctx = nullptr;
+static double seam_key[6];
+
+static int
+seam_prepare (double mass, double charge, double diffusion_coeff, double dr, double dz,
+              int r0, int r1, int z0, int z1)
+{
+  const double key[6] = {mass, charge, diffusion_coeff, dr, dz, (double) r0};
+  Ctx *c = seam_ctx;
+  if (c && c->pd_h[0].nr == r1 - r0 && c->pd_h[0].nz == z1 - z0 && memcmp (key, seam_key, sizeof key) == 0)
+    return ARCOS_OK;
+  if (c) { arcos_destroy (c); seam_ctx = nullptr; }
+  arcos_params p{};
+  p.no_species = 1; p.charge[0] = charge; p.mass[0] = mass;
+  p.diffusion_coeff = diffusion_coeff;
+  p.L_r = dr; p.L_z = dz; p.gridpoints_r = 1; p.gridpoints_z = 1;
+  p.max_ntheta = 1; p.max_levels = 0; p.extra_pois_levels = 0; p.per_plane = 1;
+  p.z_cutoff = 1e7; p.nu_a = p.nu_d = p.nu_rt = 1; p.cdr_bnd_bottom = p.cdr_bnd_top = p.cdr_bnd_right = 1;
+  void *vc = nullptr;
+  int r = arcos_create (&p, &vc);
+  if (r) return r;
+  c = (Ctx *) vc;
+  c->g.push_back (GridH{r0, z0, r1, z1, 1, 0, 0, -1, 0, {}});
+  c->nfam = 1;
+  c->fam_root.push_back (0);
+  if ((r = arcos_commit (c))) { arcos_destroy (c); return r; }
+  c->pd_h[0].dr = dr;                    // the slab's own spacing (cdr.c:947)
+  c->pd_h[0].dz = dz;
+  CK (cudaMemcpy (c->pd_d, c->pd_h.data (), sizeof (PatchDesc), cudaMemcpyHostToDevice));
+  seam_ctx = c;
+  memcpy (seam_key, key, sizeof key);
+  return ARCOS_OK;
+}
+
+static int
+seam_run (const double *dens, double *d_dens, const double *er, const double *ez,
+          cudaMemcpyKind in_kind, cudaStream_t stream)
+{
+  Ctx *c = seam_ctx;
+  c->stream = stream;
+  const PatchDesc &P = c->pd_h[0];
+  const size_t w = sizeof (double) * (P.nr + 4), hgt = (size_t) (P.nz + 4);
+  const size_t dp = sizeof (double) * P.pitch;
+  CK (cudaMemcpy2DAsync (P.arr (0, K_DENS, 0), dp, dens, w, w, hgt, in_kind, stream));
+  CK (cudaMemcpy2DAsync (P.arr (0, K_DDENS, 0), dp, d_dens, w, w, hgt, in_kind, stream));
+  CK (cudaMemcpy2DAsync (P.arr (0, K_ER), dp, er, w, w, hgt, in_kind, stream));
+  CK (cudaMemcpy2DAsync (P.arr (0, K_EZ), dp, ez, w, w, hgt, in_kind, stream));
+  StageArgs A = base_args (c);
+  A.nset = 0; A.dset = 0; A.accumulate = 1;
+  int r = run_stage (c, A, M_DERIV);
+  if (r) return r;
+  const cudaMemcpyKind out_kind = in_kind == cudaMemcpyHostToDevice ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  CK (cudaMemcpy2DAsync (d_dens, w, P.arr (0, K_DDENS, 0), dp, w, hgt, out_kind, stream));
+  CK (cudaStreamSynchronize (stream));
+  return ARCOS_OK;
+}
+
+int
+arcos_cdr_advect_vec_dev (double mass, double charge, const double *dens, double *d_dens,
+                          const double *er, const double *ez, double diffusion_coeff,
+                          double dr, double dz, int r0, int r1, int z0, int z1, void *stream)
+{
+  if (mass <= 0) return ARCOS_OK;                    // .f90:82
+  if (r1 - r0 < 2 || z1 - z0 < 2 || !dens || !d_dens || !er || !ez)
+    return fail (ARCOS_ERR_ARG, "arcos_cdr_advect_vec_dev: bad slab");
+  int r = seam_prepare (mass, charge, diffusion_coeff, dr, dz, r0, r1, z0, z1);
+  if (r) return r;
+  return seam_run (dens, d_dens, er, ez, cudaMemcpyDeviceToDevice, (cudaStream_t) stream);
+}
+
+void
+arcos_cdr_advect_vec (double mass, double charge, double *dens_array, double *d_dens_array,
+                      double *er_array, int er_len, double *ez_array, int ez_len,
+                      double diffusion_coeff, double dr, double dz, int sprite_module,
+                      int r0, int r1, int z0, int z1)
+{
+  const int len = (r1 - r0 + 4) * (z1 - z0 + 4);
+  int r = ARCOS_OK;
+  if (mass <= 0) return;                             // .f90:82
+  if (sprite_module) r = fail (ARCOS_ERR_ARG, "sprite_module is not supported on the device path");
+  else if (er_len < len || ez_len < len) r = fail (ARCOS_ERR_ARG, "er/ez shorter than the slab");
+  else if ((r = seam_prepare (mass, charge, diffusion_coeff, dr, dz, r0, r1, z0, z1)) == ARCOS_OK)
+    r = seam_run (dens_array, d_dens_array, er_array, ez_array, cudaMemcpyHostToDevice, 0);
+  if (r != ARCOS_OK) {
+    fprintf (stderr, "arcos_cdr_advect_vec: Fatal error: %s\n", g_err.c_str ());
+    exit (-1);                                       // fatal(), cstream.h:47-51
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,500 @@
+// The CDR derivative / RK2 stage kernel (drift flux + diffusion flux +
+// reaction source, fused with the stage update), one persistent launch over a
+// work list of tiles from any number of patches.
+//
+// Arithmetic follows the reference operation by operation so results are
+// bit-identical to the CPU code (the library is compiled with -fmad=false):
+//   * reactions: react_apply (src/reaction.c:110-156), in list order, into a
+//     zeroed accumulator (zero_fill, reaction.c:180-189);
+//   * radial face flux: mat_efield_r / mat_cdr_f_ad_r
+//     (arcos_f90/src/cdr_advect_diffu_vec.f90:134-181, 233-308);
+//   * axial face flux: mat_efield_z / mat_cdr_f_ad_z (.f90:183-231, 310-386);
+//   * divergence: d += er_min*F(i-1/2) - er*F(i+1/2) (.f90:113-117), then
+//     d += (1/dz)(F(j-1/2) - F(j+1/2)) (.f90:128-130);
+//   * stage updates: cdr_update (cdr.c:1091-1097) and cdr_rk2_update
+//     (cdr.c:1125-1132).
+//
+// Tiling: see the comment above k_stage.
+#pragma once
+#include "device_common.cuh"
+
+namespace arcos {
+
+#define VERYSMALL_F90 ((double) 1.0e-20f)   // .f90:240,317 (REAL literal)
+#define POINT4_F90 ((double) 0.4f)          // .f90:282,356 (REAL literal)
+
+enum StageMode {
+  M_DERIV = 0,  // d[dset] = F(n[nset]); ghosts read from memory
+  M_S1 = 1,     // d0 = F(max(0, n0)); ghosts from the boundary conditions
+  M_S2 = 2,     // n1 = n0 + h/2 d0 + h/2 F(n0 + h d0); ghosts from the conditions
+  M_AMR2 = 3    // n[0] = n[0] + h/2 d[0] + h/2 F(n[1]); ghosts read from memory
+};
+
+struct StageArgs {
+  const PatchDesc *patches;
+  const WorkItem *items;
+  int n_items;
+  int nset, dset;       // M_DERIV: read dens of nset, write d_dens of dset
+  int src, dst;         // M_S1/M_S2: state in dens[src]; M_S2 writes n1 to dens[dst]
+  int want_charge;      // M_S2: write charge(n1) into charge[dst]
+  int fam_state;        // M_S2: reduce max density into the next dmax slot
+  const TableNode *nodes;
+  DevState *st;         // one per family
+  int nfam;
+  const int *etz;       // [patch][set]: number of non-zero etheta values (0: |E| from er, ez)
+  unsigned int *done;   // M_S2 with cfl_fold: blocks finished (last block computes the next step)
+  int cfl_fold;         // M_S2: the last block computes the next step's h for every family
+  int accumulate;       // M_DERIV: add the drift/diffusion divergence to the existing d_dens
+                        // (no reactions), as the Fortran kernel does (.f90:113-130)
+  int n_nodes;          // reaction-table nodes
+  int nodes_smem;       // copy the nodes to shared memory
+};
+
+__device__ __forceinline__ double clamp0 (double x) { return 0 > x ? 0 : x; }   // MYMAX(0, x)
+__device__ __forceinline__ double mymin (double x, double y) { return x < y ? x : y; }  // MYMIN
+
+// Radial face flux (mat_cdr_f_ad_r, .f90:259-306).
+__device__ __forceinline__ double
+face_r (double nLL, double nL, double nR, double nRR, double v, double dd)
+{
+  double dC = nR - nL, psi, aux;
+  if (fabs (dC) > VERYSMALL_F90) {
+    double p = 0.0;
+    if (v >= 0.0) p = (nL - nLL) / dC;
+    else if (v < 0.0) p = (nRR - nR) / dC;
+    if (p <= 0.0) psi = 0.0;
+    else if (p >= 4.0) psi = 1.0;
+    else if (p >= POINT4_F90) psi = (1.0 + 0.5 * p) / 3.0;
+    else psi = p;
+  } else {
+    psi = -1.0;
+  }
+  aux = psi * dC;
+  aux = (v >= 0.0) ? nL + aux : nR - aux;
+  return aux * v - dd * dC;
+}
+
+// Axial face flux (mat_cdr_f_ad_z, .f90:335-384).
+__device__ __forceinline__ double
+face_z (double nLL, double nL, double nR, double nRR, double v, double dd)
+{
+  double dC = nR - nL, pij, aux;
+  if (fabs (dC) > VERYSMALL_F90) {
+    double p = (v > 0.0) ? (nL - nLL) / dC : (nRR - nR) / dC;
+    pij = p;
+    if ((p > POINT4_F90) && (p < 4.0)) pij = (1.0 + 0.5 * p) / 3.0;
+    else if (p >= 4.0) pij = 1.0;
+    else if (p <= 0.0) pij = 0.0;
+  } else {
+    pij = 1.0;
+  }
+  aux = pij * dC;
+  aux = (v >= 0.0) ? nL + aux : nR - aux;
+  return aux * v - dd * dC;
+}
+
+// Reaction rate k(|E|) exactly as react_apply computes it (reaction.c:127-142):
+// the table position the reference derives from log10/floor is recovered by
+// comparing |E| with exact per-node thresholds (precomputed on the host with
+// the same log10), starting from a single-precision estimate.
+__device__ __forceinline__ double
+table_rate (const Model &M, const TableNode *__restrict__ nodes, int r, double eabs)
+{
+  const TableNode *nd = nodes + M.r_node_off[r];
+  const int steps = M.r_steps[r];
+  if (!(eabs >= nd[0].thr)) return M.r_under[r];        // log_e < e_min (or NaN)
+  if (eabs >= nd[steps + 1].thr) return M.r_over[r];     // log_e > e_min + e_step*steps
+  float lf = __log10f ((float) eabs);
+  float pf = (lf - (float) M.r_e_min[r]) / (float) M.r_e_step[r];
+  int k = (pf > 0.f) ? (int) pf : 0;
+  if (!(pf < (float) steps)) k = steps;
+  while (k > 0 && eabs < nd[k].thr) k--;
+  while (k < steps && eabs >= nd[k + 1].thr) k++;
+  const TableNode n = nd[k];
+  return n.val + n.slope * (eabs - n.e1);
+}
+
+// CFL time step of cdr_courant (cdr.c:971-1061) and the step limit of cdr_rk2
+// (cdr.c:1287-1302) for one family, from the reduced maxima.  `idx` is the
+// step being started (its h goes to the dt log).
+__device__ inline void
+cfl_step (DevState *st, const Model &M, int slot, int eset, int idx)
+{
+  const double dmax = dkey_inv (st->dmax_key[slot]);
+  const double emr = dkey_inv (st->emax_key[eset][0]);
+  const double emz = dkey_inv (st->emax_key[eset][1]);
+  const double emt = dkey_inv (st->emax_key[eset][2]);
+  const double dr_min = st->courant_const[0], dz_min = st->courant_const[1];
+  const double rdt = st->courant_const[2], is_3d = st->courant_const[3];
+  const bool ok = emr >= 0 && emz >= 0 && emt >= 0 && dmax >= 0;          // cdr.c:1023
+  const double tau_a = M.nu_a / (emr / dr_min + emz / dz_min + is_3d * emt / rdt);
+  const double max_diff = 0.1;                                            // cdr.c:1041
+  const double tau_d = M.nu_d / (max_diff / dr_min / dr_min + max_diff / dz_min / dz_min
+                                 + is_3d * max_diff / rdt / rdt);
+  const double tau_f = tau_d;                                             // cdr.c:1055
+  const double tau_rt = M.nu_rt / dmax;
+  const double cour = mymin (tau_a, mymin (tau_d, mymin (tau_f, tau_rt)));
+  const double h = mymin (st->h_attempt, cour);                          // cdr.c:1288
+  st->h = h;
+  if (!ok) st->error |= 1 << 3;
+  if (h < M.warn_min_timestep) {                                          // cdr.c:1290-1302
+    st->small_dt_count++;
+    if (st->small_dt_count >= 6) st->error |= 1 << 4;
+  }
+  if (idx >= 0 && idx < st->dt_cap) st->dt_log[idx] = h;
+}
+
+// Tile kernel.  A block of WY warps owns a tile of TX = 32 columns (one warp
+// wide, lane = column) by TY = WY * RPW rows of one theta plane; warp w owns
+// rows w*RPW .. w*RPW + RPW - 1 of the tile, so every thread computes RPW
+// independent cells.  The tile plus a two-cell halo of every input array is
+// staged in shared memory with 16-byte cp.async copies; ghost cells of the
+// fused forms are then filled in shared memory from the mirrored interior
+// cells (the boundary conditions of cdr_set_ext_bnd), radial face fluxes pass
+// between neighbouring lanes by warp shuffle, axial face fluxes stay in
+// registers.  Each face flux is evaluated once (one extra radial face per
+// warp and one extra axial face per thread).
+#define TX 32
+#define TXP (TX + 4)
+
+template <int NS, int MODE, int WY, int RPW>
+struct TileLayout {
+  static constexpr int TY = WY * RPW;
+  static constexpr int ROWS = TY + 4;
+  static constexpr int PLANE = ROWS * TXP;                 // doubles per staged array
+  // staged arrays: stencil densities, (M_S2) d0, fields er, ez, eabs
+  static constexpr int NA = NS * (MODE == M_S2 ? 2 : 1) + 3;
+  static constexpr int A_D = NS;
+  static constexpr int A_F = NA - 3;
+  // 3-D axis: the two columns nearest the axis of the opposite plane (n0, and d0 for M_S2)
+  static constexpr int NOPP = NS * (MODE == M_S2 ? 2 : 1);
+  static constexpr int OPP = NOPP * ROWS * 2;
+  static constexpr int DOUBLES = NA * PLANE + OPP;
+};
+
+__device__ __forceinline__ void
+cp_async16 (void *smem_dst, const void *gsrc)
+{
+  const unsigned d = (unsigned) __cvta_generic_to_shared (smem_dst);
+  asm volatile ("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit () { asm volatile ("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all () { asm volatile ("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <int NS, int MODE, int WY, int RPW>
+__global__ void __launch_bounds__ (32 * WY)
+k_stage (const __grid_constant__ Model M, const StageArgs A)
+{
+  using LY = TileLayout<NS, MODE, WY, RPW>;
+  constexpr int TY = LY::TY, ROWS = LY::ROWS, PL = LY::PLANE, NA = LY::NA;
+  constexpr int A_D = LY::A_D, A_F = LY::A_F;
+  constexpr bool OTF = (MODE == M_S1 || MODE == M_S2);
+  constexpr int NT = 32 * WY;
+  extern __shared__ double smem[];
+  double *opp = smem + NA * PL;
+  const TableNode *nodes = A.nodes;
+  __shared__ unsigned long long red_key[WY];
+  const int t = threadIdx.x, lane = t & 31, wq = t >> 5;
+
+  if (A.nodes_smem) {
+    TableNode *sn = reinterpret_cast<TableNode *> (smem + LY::DOUBLES);
+    for (int i = t; i < A.n_nodes; i += NT) sn[i] = A.nodes[i];
+    nodes = sn;
+    __syncthreads ();
+  }
+  // staged element (row, col) of array a; row, col relative to the tile corner (zb-2, c0-2)
+#define SA(a_, row_, col_) smem[(a_) * PL + (row_) * TXP + (col_)]
+
+  double dmax_local = -1.0;
+  bool seen = false;
+
+  for (int item = blockIdx.x; item < A.n_items; item += gridDim.x) {
+    const WorkItem w = A.items[item];
+    const PatchDesc P = A.patches[w.patch];
+    const int nr = P.nr, nz = P.nz, nt = P.ntheta;
+    const int plane = w.plane;
+    const int fset = (MODE == M_DERIV) ? A.nset : (MODE == M_S1 ? 0 : 1);
+    double h = 0.0;
+    if (MODE == M_S2 || MODE == M_AMR2) h = A.st[P.fam].h;
+    const bool do_flux = (nt == 1) || M.per_plane;
+    const bool etz = A.etz[w.patch * 2 + fset] == 0;
+    const int zb = w.zb, c0 = w.c0;
+    const int nrow = w.zlen + 4;                  // staged rows zb-2 .. zb+zlen+1
+    const int ncol = w.width + 4;                 // staged columns c0-2 .. c0+width+1
+    const int nchunk = (ncol + 1) >> 1;           // 16-byte chunks per staged row
+    const int nset = (MODE == M_DERIV) ? A.nset : (MODE == M_AMR2 ? 1 : A.src);
+    const long long pbase = P.off (c0 - 2, zb - 2, plane);   // tile corner in this plane
+
+    // ---- stage the tile ----
+    {
+      const int total = nrow * nchunk;
+      for (int i = t; i < total; i += NT) {
+        const int row = i / nchunk, ch = i - row * nchunk;
+        const long long go = pbase + (long long) row * P.pitch + 2 * ch;
+        const int so = row * TXP + 2 * ch;
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+          cp_async16 (smem + s * PL + so, P.arr (nset, K_DENS, s) + go);
+          if (MODE == M_S2) cp_async16 (smem + (A_D + s) * PL + so, P.arr (0, K_DDENS, s) + go);
+        }
+        cp_async16 (smem + (A_F + 0) * PL + so, P.arr (fset, K_ER) + go);
+        cp_async16 (smem + (A_F + 1) * PL + so, P.arr (fset, K_EZ) + go);
+        if (!etz) cp_async16 (smem + (A_F + 2) * PL + so, P.arr (fset, K_EABS) + go);
+      }
+      if (OTF && nt > 1 && c0 == 0) {
+        // axis ghosts of a 3-D grid come from the opposite plane (cdr.c:798-824)
+        const int pl2 = (plane + nt / 2) % nt;
+        const long long ob = P.off (0, zb - 2, pl2);
+        for (int row = t; row < nrow; row += NT) {
+#pragma unroll
+          for (int s = 0; s < NS; s++) {
+            cp_async16 (opp + (s * ROWS + row) * 2, P.arr (nset, K_DENS, s) + ob + (long long) row * P.pitch);
+            if (MODE == M_S2)
+              cp_async16 (opp + ((NS + s) * ROWS + row) * 2, P.arr (0, K_DDENS, s) + ob + (long long) row * P.pitch);
+          }
+        }
+      }
+      cp_async_commit ();
+      cp_async_wait_all ();
+      __syncthreads ();
+    }
+
+    // ---- stencil values: clamp (cdr_nonegative) and the RK2 intermediate
+    // state on the interior, then the ghost cells from the boundary
+    // conditions (prepare_grid on the fused forms) ----
+    if (OTF) {
+      const int total = nrow * ncol;
+      for (int i = t; i < total; i += NT) {
+        const int row = i / ncol, col = i - row * ncol;
+        const int gr = zb - 2 + row, gc = c0 - 2 + col;
+        if (gr < 0 || gr >= nz || gc < 0 || gc >= nr) continue;
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+          double v = clamp0 (SA (s, row, col));
+          if (MODE == M_S2) v = v + h * SA (A_D + s, row, col);
+          SA (s, row, col) = v;
+        }
+      }
+      __syncthreads ();
+      for (int i = t; i < total; i += NT) {
+        const int row = i / ncol, col = i - row * ncol;
+        const int gr = zb - 2 + row, gc = c0 - 2 + col;
+        const bool gin = gr >= 0 && gr < nz, cin = gc >= 0 && gc < nr;
+        if (gin == cin) continue;                 // interior, or a corner (never read)
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+          double v;
+          if (gc < 0) {                           // axis
+            if (nt == 1) {
+              v = SA (s, row, col + 2 * (-1 - gc) + 1);      // column -1-gc
+            } else {
+              const int oc = -1 - gc;             // 0 or 1
+              v = clamp0 (opp[(s * ROWS + row) * 2 + oc]);
+              if (MODE == M_S2) v = v + h * opp[((NS + s) * ROWS + row) * 2 + oc];
+            }
+          } else if (gc >= nr) {                  // r = L_r
+            v = (double) M.bnd_sign[1] * SA (s, row, col - 2 * (gc - nr) - 1);
+          } else if (gr < 0) {                    // z = 0
+            v = (double) M.bnd_sign[2] * SA (s, row + 2 * (-1 - gr) + 1, col);
+          } else {                                // z = L_z
+            v = (double) M.bnd_sign[3] * SA (s, row - 2 * (gr - nz) - 1, col);
+          }
+          SA (s, row, col) = v;
+        }
+      }
+      __syncthreads ();
+    }
+
+    // ---- per-species and per-column constants ----
+    double cm[NS], ddr[NS], ddz[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      const double mass = M.mass[s];
+      if (mass > 0) {
+        const double d_iso0 = M.diffusion_coeff / mass;     // .f90:85
+        cm[s] = M.charge[s] / mass;                        // .f90:90
+        ddr[s] = d_iso0 / P.dr;                            // .f90:174
+        ddz[s] = d_iso0 / P.dz;                            // .f90:224
+      } else {
+        cm[s] = 0; ddr[s] = 0; ddz[s] = 0;
+      }
+    }
+    const double gdz = 1.0 / P.dz;                          // .f90:88
+    const bool active = lane < w.width;
+    const int c = c0 + lane;
+    const int ir_abs = P.r0 + c;
+    const double r_inv = 1.0 / (((double) ir_abs + 0.5) * P.dr);   // .f90:409
+    const double erm = (double) ir_abs * r_inv;                     // .f90:410
+    const double erp = (double) (ir_abs + 1) * r_inv;               // .f90:411
+    const int sc = lane + 2;                      // this column in the staged rows
+    const int r_first = wq * RPW;                 // tile rows of this thread
+    const bool last_lane = lane == w.width - 1 || lane == 31;
+
+    // ---- fluxes, reactions and the update of this thread's RPW cells ----
+    double acc[RPW][NS];
+#pragma unroll
+    for (int k = 0; k < RPW; k++)
+#pragma unroll
+      for (int s = 0; s < NS; s++) acc[k][s] = 0.0;
+    if (MODE == M_DERIV && A.accumulate) {
+      // the Fortran kernel adds to the d_dens it is given (.f90:113-130)
+#pragma unroll
+      for (int k = 0; k < RPW; k++) {
+        const int tr = r_first + k;
+        if (!active || tr >= w.zlen) continue;
+        const long long o = P.off (c, zb + tr, plane);
+#pragma unroll
+        for (int s = 0; s < NS; s++) acc[k][s] = P.arr (A.dset, K_DDENS, s)[o];
+      }
+    }
+
+    // reactions (react_apply, reaction.c:110-156), in list order
+    if (M.nreact > 0 && !(MODE == M_DERIV && A.accumulate)) {
+#pragma unroll
+      for (int k = 0; k < RPW; k++) {
+        const int tr = r_first + k;               // tile row (0-based, interior)
+        const int sr = tr + 2;
+        if (tr >= w.zlen) continue;
+        const double zc = ((double) (P.z0 + zb + tr) + 0.5) * P.dz;
+        if (!(zc < M.z_cutoff)) continue;
+        double eabs;
+        if (etz) {
+          const double e_r = 0.5 * (SA (A_F + 0, sr, sc) + SA (A_F + 0, sr, sc - 1));  // cdr.c:681-682
+          const double e_z = 0.5 * (SA (A_F + 1, sr, sc) + SA (A_F + 1, sr - 1, sc));  // cdr.c:683-684
+          eabs = sqrt (e_r * e_r + e_z * e_z + 0.0 * 0.0);                           // cdr.c:691-692
+        } else {
+          eabs = SA (A_F + 2, sr, sc);
+        }
+        eabs = fabs (eabs);
+        double cen[NS];
+#pragma unroll
+        for (int s = 0; s < NS; s++) cen[s] = SA (s, sr, sc);
+        for (int r = 0; r < M.nreact; r++) {
+          double rate = table_rate (M, nodes, r, eabs);
+          const int nin = M.r_nin[r];
+          for (int i = 0; i < nin; i++) {
+            const int sp = M.r_in[r][i];
+            double inv = 0.0;
+#pragma unroll
+            for (int s = 0; s < NS; s++) if (s == sp) inv = fabs (cen[s]);
+            rate *= (0 > inv ? 0 : inv);
+          }
+          const int nop = M.r_nops[r];
+          for (int i = 0; i < nop; i++) {
+            const int sp = M.r_op_sp[r][i];
+            const double rm = M.r_op_neg[r][i] ? -rate : rate;
+#pragma unroll
+            for (int s = 0; s < NS; s++) if (s == sp) acc[k][s] += rm;
+          }
+        }
+      }
+    }
+
+    if (do_flux) {
+#pragma unroll
+      for (int s = 0; s < NS; s++) {
+        if (!M.mobile[s]) continue;
+        // axial faces below each row and above the last (.f90:310-386)
+        double fz[RPW + 1];
+#pragma unroll
+        for (int k = 0; k <= RPW; k++) {
+          const int sr = r_first + k + 2;         // face below staged row sr
+          fz[k] = face_z (SA (s, sr - 2, sc), SA (s, sr - 1, sc), SA (s, sr, sc), SA (s, sr + 1, sc),
+                          cm[s] * SA (A_F + 1, sr - 1, sc), ddz[s]);
+        }
+#pragma unroll
+        for (int k = 0; k < RPW; k++) {
+          const int sr = r_first + k + 2;
+          // radial face at the left of this column (.f90:233-308)
+          const double fl = face_r (SA (s, sr, sc - 2), SA (s, sr, sc - 1), SA (s, sr, sc),
+                                    SA (s, sr, sc + 1), cm[s] * SA (A_F + 0, sr, sc - 1), ddr[s]);
+          double fr = __shfl_down_sync (0xffffffffu, fl, 1);
+          if (last_lane)
+            fr = face_r (SA (s, sr, sc - 1), SA (s, sr, sc), SA (s, sr, sc + 1), SA (s, sr, sc + 2),
+                         cm[s] * SA (A_F + 0, sr, sc), ddr[s]);
+          double dv = acc[k][s];
+          dv = dv + erm * fl - erp * fr;                         // .f90:113-117
+          dv = dv + gdz * (fz[k] - fz[k + 1]);                   // .f90:128-130
+          acc[k][s] = dv;
+        }
+      }
+    }
+
+    // ---- write ----
+#pragma unroll
+    for (int k = 0; k < RPW; k++) {
+      const int tr = r_first + k;
+      if (!active || tr >= w.zlen) continue;
+      const int iz = zb + tr;
+      const long long o = P.off (c, iz, plane);
+      if (MODE == M_DERIV) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) P.arr (A.dset, K_DDENS, s)[o] = acc[k][s];
+      } else if (MODE == M_S1) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) P.arr (0, K_DDENS, s)[o] = acc[k][s];
+      } else {
+        double chg = 0.0;
+        const double hh = 0.5 * h;
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+          const double n0c = (MODE == M_S2) ? clamp0 (P.arr (A.src, K_DENS, s)[o]) : P.arr (0, K_DENS, s)[o];
+          const double d0 = (MODE == M_S2) ? SA (A_D + s, tr + 2, sc) : P.arr (0, K_DDENS, s)[o];
+          const double n1 = n0c + hh * d0 + hh * acc[k][s];                // cdr.c:1128-1131
+          P.arr (MODE == M_S2 ? A.dst : 0, K_DENS, s)[o] = n1;
+          if (MODE == M_S2) {
+            chg += (n1 * M.charge[s]) / nt;                                // cdr.c:380-381
+            if (M.mobile[s] && P.level == 0) {
+              const double v = clamp0 (n1);
+              if (v == v) { if (!seen || v > dmax_local) dmax_local = v; seen = true; }
+            }
+          }
+        }
+        if (MODE == M_S2 && A.want_charge) P.arr (A.dst, K_CHARGE)[o] = chg;
+      }
+    }
+    // ---- block max of the mobile densities -> next step's CFL (M_S2) ----
+    if (MODE == M_S2 && A.fam_state && P.level == 0) {
+      unsigned long long key = seen ? dkey (dmax_local) : 0ULL;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long other = __shfl_xor_sync (0xffffffffu, key, o);
+        key = other > key ? other : key;
+      }
+      if (lane == 0) red_key[wq] = key;
+      __syncthreads ();
+      if (t == 0) {
+        unsigned long long kk = red_key[0];
+        for (int i = 1; i < WY; i++) kk = red_key[i] > kk ? red_key[i] : kk;
+        DevState *st = A.st + P.fam;
+        if (kk) atomicMax (&st->dmax_key[(st->step + 1) & 1], kk);
+      }
+      dmax_local = -1.0;
+      seen = false;
+    }
+    __syncthreads ();                              // the next tile reuses the staging area
+  }
+#undef SA
+
+  // ---- the last block to finish starts the next step of every family ----
+  if (MODE == M_S2 && A.cfl_fold) {
+    __shared__ int is_last;
+    __threadfence ();
+    __syncthreads ();
+    if (t == 0) is_last = (atomicAdd (A.done, 1u) == gridDim.x - 1);
+    __syncthreads ();
+    if (is_last) {
+      __threadfence ();
+      for (int f = t; f < A.nfam; f += NT) {
+        DevState *st = A.st + f;
+        const int k = st->step + 1;
+        st->dmax_key[(k + 1) & 1] = dkey (-1.0);
+        st->step = k;
+        cfl_step (st, M, k & 1, 0, k);
+      }
+      if (t == 0) *A.done = 0u;
+    }
+  }
+}
+
+}  // namespace arcos

@@ -1,0 +1,235 @@
+"""Seeded synthetic workloads with the shapes of the five benchmark
+configurations (no datasets are involved; every input is generated here).
+
+* single grid (``plain``): the minimal model on an r-z grid, electrons = ions =
+  1e-4 + a Gaussian seed of amplitude 0.1, radius 0.1, on the axis at
+  z = 0.9 L_z; in 3-D the seed is modulated by 1 + 0.05 cos(theta) +
+  0.02 cos(2 theta) and a 1e-6 U[0,1) background is added;
+* ``amr``: a refinement tree nested around a seeded streamer-head location;
+* ``kinetic``: six charged species, nine tabulated reactions, a batch of
+  uneven single-grid instances with their own applied fields.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from .grids import GridSpec, inherit_ext_bound
+from .model import KineticModel, Params, Reaction, Species, minimal_model
+from .react_table import ReactTable, log_uniform_table
+
+
+@dataclass
+class Problem:
+    params: Params
+    model: KineticModel
+    specs: List[GridSpec]
+    dens: List[List[np.ndarray]]                     # [grid][species] rz arrays
+    fields: List[Tuple[np.ndarray, np.ndarray, Optional[np.ndarray]]] = field(default_factory=list)
+    family_E: List[Tuple[float, float, float]] = field(default_factory=list)
+
+    @property
+    def cells(self) -> int:
+        return sum(s.nr * s.nz * s.ntheta for s in self.specs)
+
+    @property
+    def updated_species(self) -> int:
+        """Species a step updates: those with a charge (reaction.c:152) — in
+        these models every species."""
+        return self.model.no_species
+
+
+def seed_dens(spec: GridSpec, params: Params, rng: np.random.Generator, amp: float = 0.1,
+              sigma: float = 0.1, z_frac: float = 0.9, bg: float = 1e-4,
+              noise: float = 0.0, theta_mod: bool = False, center_r: float = 0.0,
+              center_z: Optional[float] = None) -> np.ndarray:
+    """Density on every cell of ``spec`` (ghosts included) in rz layout."""
+    dr, dz = params.dr(spec.level), params.dz(spec.level)
+    ir = np.arange(spec.r0 - 2, spec.r1 + 2)
+    iz = np.arange(spec.z0 - 2, spec.z1 + 2)
+    r = (ir + 0.5) * dr
+    z = (iz + 0.5) * dz
+    zc = z_frac * params.L_z if center_z is None else center_z
+    R, Z = np.meshgrid(r, z)
+    g = amp * np.exp(-((R - center_r) ** 2 + (Z - zc) ** 2) / sigma ** 2)
+    a = spec.zeros()
+    for p in range(spec.planes):
+        it = p + spec.theta0
+        th = it * params.dtheta
+        mod = (1.0 + 0.05 * math.cos(th) + 0.02 * math.cos(2 * th)) if theta_mod else 1.0
+        a[p] = bg + g * mod
+        if noise > 0:
+            a[p] += noise * rng.random(R.shape)
+    return a
+
+
+def uniform_field(spec: GridSpec):
+    """The field solve's part of a uniform applied field: zero (the applied
+    E0 is added on the device, as cdr_add_ext_field does)."""
+    return (spec.zeros(), spec.zeros(), None)
+
+
+def plain(nr: int = 128, nz: int = 256, ntheta: int = 1, L_r: float = 2.0, L_z: float = 4.0,
+          ion_mass: float = 1.0, seed: int = 0, noise: float = 0.0, table_points: int = 256,
+          nu: float = 0.5, attempt_dt: float = 50.0) -> Problem:
+    """Single uniform grid with the minimal model and a uniform Ez = -1."""
+    params = Params(L_r=L_r, L_z=L_z, gridpoints_r=nr, gridpoints_z=nz, max_ntheta=ntheta,
+                    E0_z=-1.0, nu_a=nu, nu_d=nu, nu_rt=nu, diffusion_coeff=0.1,
+                    warn_min_timestep=1e-12, max_levels=4)
+    model = minimal_model(ion_mass=ion_mass, points=table_points)
+    spec = GridSpec(0, 0, nr, nz, ntheta=ntheta, level=0, ext_bound=15, parent=-1)
+    rng = np.random.default_rng(seed)
+    dens = [[seed_dens(spec, params, rng, noise=noise, theta_mod=ntheta > 1)
+             for _ in range(model.no_species)]]
+    return Problem(params, model, [spec], dens, [uniform_field(spec)])
+
+
+def amr(n_patches: int = 320, levels: int = 4, root_nr: int = 256, root_nz: int = 512,
+        side_lo: int = 16, side_hi: int = 256, seed: int = 0, ion_mass: float = 1.0,
+        ntheta: int = 1) -> Problem:
+    """A refinement tree of ``n_patches`` patches on ``levels`` levels (ratio
+    2) nested around a seeded head point: each level-l patch lies inside one
+    level-(l-1) patch (one cell of margin), siblings do not overlap, sides are
+    drawn from U{side_lo..side_hi} (clipped to what fits), all even so
+    children stay aligned with parent cells."""
+    rng = np.random.default_rng(seed)
+    params = Params(L_r=2.0, L_z=4.0, gridpoints_r=root_nr, gridpoints_z=root_nz,
+                    max_ntheta=ntheta, E0_z=-1.0, nu_a=0.5, nu_d=0.5, nu_rt=0.5,
+                    diffusion_coeff=0.1, warn_min_timestep=1e-14, max_levels=levels + 1)
+    model = minimal_model(ion_mass=ion_mass)
+    specs = [GridSpec(0, 0, root_nr, root_nz, ntheta, 0, 15, -1)]
+    head_r = 0.0
+    head_z = float(rng.uniform(0.55, 0.85)) * params.L_z
+    occupied = {0: []}
+
+    def fits(rect, lst):
+        r0, z0, r1, z1 = rect
+        for (a0, b0, a1, b1) in lst:
+            if r0 < a1 + 2 and a0 < r1 + 2 and z0 < b1 + 2 and b0 < z1 + 2:
+                return False
+        return True
+
+    target = n_patches - 1
+    per_level = []
+    rem = target
+    weights = [2 ** l for l in range(1, levels)]
+    for i, w in enumerate(weights):
+        k = rem if i == len(weights) - 1 else int(round(target * w / sum(weights)))
+        per_level.append(k)
+        rem -= k
+    attempts = 0
+    for l, want in zip(range(1, levels), per_level):
+        parents = [i for i, s in enumerate(specs) if s.level == l - 1]
+        made = 0
+        while made < want and attempts < 200000:
+            attempts += 1
+            # prefer parents near the head
+            pi = parents[int(rng.integers(len(parents)))]
+            P = specs[pi]
+            pr0, pz0, pr1, pz1 = 2 * P.r0, 2 * P.z0, 2 * P.r1, 2 * P.z1
+            wr = int(rng.integers(side_lo, side_hi + 1)) // 2 * 2
+            wz = int(rng.integers(side_lo, side_hi + 1)) // 2 * 2
+            wr = min(wr, (pr1 - pr0 - 4) // 2 * 2)
+            wz = min(wz, (pz1 - pz0 - 4) // 2 * 2)
+            if wr < side_lo or wz < side_lo:
+                continue
+            dr_l = params.dr(l)
+            dz_l = params.dz(l)
+            cr = int(head_r / dr_l) + int(rng.normal(0, 3 * wr))
+            cz = int(head_z / dz_l) + int(rng.normal(0, 3 * wz))
+            r0 = min(max(cr - wr // 2, pr0 + 2), pr1 - 2 - wr) // 2 * 2
+            z0 = min(max(cz - wz // 2, pz0 + 2), pz1 - 2 - wz) // 2 * 2
+            if P.r0 == 0 and rng.random() < 0.3:
+                r0 = 0
+            r0, z0 = max(r0, pr0 if P.r0 == 0 else pr0 + 2), max(z0, pz0 + 2)
+            r1, z1 = r0 + wr, z0 + wz
+            if r1 > pr1 - (0 if (P.ext_bound & 2) else 2) or z1 > pz1 - 2:
+                continue
+            if r0 != 0 and r0 < 2:
+                continue
+            rect = (r0, z0, r1, z1)
+            lst = occupied.setdefault(l, [])
+            if not fits(rect, lst):
+                continue
+            child = GridSpec(r0, z0, r1, z1, ntheta, l, 0, pi)
+            child.ext_bound = inherit_ext_bound(P, child)
+            specs.append(child)
+            lst.append(rect)
+            made += 1
+    dens = []
+    for sp in specs:
+        per = []
+        for s in range(model.no_species):
+            per.append(seed_dens(sp, params, rng, noise=1e-6, theta_mod=ntheta > 1,
+                                 center_r=head_r, center_z=head_z))
+        dens.append(per)
+    return Problem(params, model, specs, dens, [uniform_field(s) for s in specs])
+
+
+def kinetic_model(points: int = 1000, seed: int = 0) -> KineticModel:
+    """Six charged species (e, N2+, O2+, O2-, O-, cluster+) and nine reactions
+    with seeded smooth monotone rate curves tabulated on ``points``
+    log-uniform nodes of [0.01, 50]: impact ionisation of N2 and O2,
+    two- and three-body attachment, detachment, two recombinations and ion
+    conversion.  Electrons have mass 1, ions mass 100 (mobility 0.01)."""
+    rng = np.random.default_rng(seed)
+    sp = [Species("e", -1.0, 1.0), Species("N2+", 1.0, 100.0), Species("O2+", 1.0, 100.0),
+          Species("O2-", -1.0, 100.0), Species("O-", -1.0, 100.0), Species("X+", 1.0, 100.0)]
+    e, n2p, o2p, o2m, om, xp = range(6)
+
+    def curve(kind):
+        a = float(rng.uniform(0.5, 2.0))
+        b = float(rng.uniform(0.5, 3.0))
+        c = float(rng.uniform(0.05, 0.5))
+        if kind == "ion":
+            return lambda E: a * E * math.exp(-b / E)
+        if kind == "att":
+            return lambda E: c * a * math.exp(-E / (b * 10.0)) + 1e-3
+        return lambda E: c * (1.0 + a * E / (E + b))
+
+    def tab(kind):
+        return log_uniform_table(curve(kind), 0.01, 50.0, points)
+
+    reactions = [
+        Reaction([e], [e, e, n2p], tab("ion")),       # e + N2 -> 2e + N2+
+        Reaction([e], [e, e, o2p], tab("ion")),       # e + O2 -> 2e + O2+
+        Reaction([e], [o2m], tab("att")),             # e + O2 + M -> O2- + M
+        Reaction([e], [om], tab("att")),              # e + O2 -> O- + O
+        Reaction([o2m], [e], tab("det")),             # O2- -> e + O2
+        Reaction([e, n2p], [], tab("det")),           # e + N2+ -> N2
+        Reaction([o2m, o2p], [], tab("det")),         # O2- + O2+ -> 2 O2
+        Reaction([o2p], [xp], tab("det")),            # O2+ + M -> X+
+        Reaction([om, xp], [], tab("det")),           # O- + X+ -> neutrals
+    ]
+    return KineticModel(species=sp, reactions=reactions)
+
+
+def kinetic_batch(n_inst: int = 32, seed: int = 0, points: int = 1000,
+                  sizes_r: Sequence[int] = (64, 128, 256),
+                  sizes_z: Sequence[int] = (128, 256, 512)) -> Problem:
+    """A batch of independent single-grid instances of uneven sizes, each its
+    own family with its own applied field Ez ~ U[-2, -0.5]."""
+    rng = np.random.default_rng(seed)
+    model = kinetic_model(points=points, seed=seed + 1)
+    params = Params(L_r=2.0, L_z=4.0, gridpoints_r=128, gridpoints_z=256, E0_z=-1.0,
+                    nu_a=0.5, nu_d=0.5, nu_rt=0.5, diffusion_coeff=0.1,
+                    warn_min_timestep=1e-14, max_levels=4)
+    specs, dens, fields, famE = [], [], [], []
+    for i in range(n_inst):
+        nr = int(rng.choice(sizes_r))
+        nz = int(rng.choice(sizes_z))
+        sp = GridSpec(0, 0, nr, nz, 1, 0, 15, -1)
+        specs.append(sp)
+        # every instance uses the level-0 spacing of the shared params
+        per = []
+        for s in range(model.no_species):
+            amp = 0.1 if s in (0, 1, 2) else 0.01
+            per.append(seed_dens(sp, params, rng, amp=amp, noise=1e-6,
+                                 center_z=0.9 * nz * params.dz(0)))
+        dens.append(per)
+        fields.append(uniform_field(sp))
+        famE.append((0.0, 0.0, float(rng.uniform(-2.0, -0.5))))
+    return Problem(params, model, specs, dens, fields, famE)

@@ -1,0 +1,368 @@
+"""Benchmark of the CDR density update (one RK2 step = one "step").
+
+Default workload: the plain 3-D configuration, one grid of 512 x 1024 cells
+with 16 theta planes, two species (electrons, positive ions, both mobility 1,
+diffusion 0.1), impact-ionisation table of 256 nodes, fixed field (uniform
+applied Ez = -1; no field solve in the loop), drift/diffusion on every theta
+plane.  Inputs are synthetic (seeded).  One step reads and writes about
+940 MB, far above the 126 MB L2, so no flush is needed between steps.
+
+Metric: FP64 cell-species updates per second (interior cells x updated
+species x RK2 steps / time), whole job.  With --gpus N every rank advances its
+own replica (independent runs; the path has no exchange step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference's own CPU implementation of the same
+step (the reference C sources with the restated Fortran kernel, built under
+oracle/_ref, OpenMP build on all host cores) on a bounded slab of the same
+grid per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 cell-species updates/s & %HBM roofline; batched/plain; adjoint/forward"
+UNIT = "cell-species updates/s"
+NR, NZ, NTHETA, NS = 512, 1024, 16, 2
+SAMPLE_NZ = 64                     # CPU sample: a 512 x 64 x 16 slab of the grid
+
+
+def workload_config(extra=None):
+    cfg = {"workload": f"plain 3-D CDR RK2 step, {NR}x{NZ} r-z cells x {NTHETA} theta planes, "
+                       f"{NS} species (both mobile), 1 reaction table (256 nodes), fixed field",
+           "nr": NR, "nz": NZ, "ntheta": NTHETA, "species": NS,
+           "cells_per_replica": NR * NZ * NTHETA,
+           "l2": "inputs larger than L2 (about 940 MB moved per step vs 126 MB L2); no flush",
+           "parallelism": "replicas (one independent grid per GPU)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------- clocks ----
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.lines = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "50", "-i", str(device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 10:
+            time.sleep(0.02)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self, t0: float, t1: float):
+        rows = [l for (ts, l) in self.lines if t0 - 0.06 <= ts <= t1 + 0.06]
+        if not rows and self.lines:
+            rows = [min(self.lines, key=lambda x: abs(x[0] - (t0 + t1) / 2))[1]]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            f = [x.strip() for x in r.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU baseline ----
+def cpu_baseline_sample(omp: bool, seconds: float = 12.0, max_steps: int = 10**9):
+    """Reference CPU implementation (oracle/_ref) on a 512 x 64 x 16 slab of
+    the workload; returns (cell-species updates/s, threads, kind, steps)."""
+    from arcos_b200 import workloads
+    from oracle import bind
+    if not bind.ref_available(omp):
+        omp = False
+    kind = "reference" if bind.ref_available(False) else "port"
+    pb = workloads.plain(nr=NR, nz=SAMPLE_NZ, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=0)
+    threads = (os.cpu_count() or 1) if omp else 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    if kind == "reference":
+        t = bind.RefTree(pb.params, pb.model, pb.specs, field_mode=bind.FIELD_FIXED, omp=omp)
+        for s in range(NS):
+            t.dens(0, s)[...] = pb.dens[0][s]
+        er, ez, _ = pb.fields[0]
+        t.set_fixed_field(0, er, ez, pb.specs[0].zeros())
+        step = lambda: t.rk2_sw(50.0, per_plane=True, zero_all=False)  # noqa: E731
+    else:
+        t = bind.PortTree(pb.params, pb.model, pb.specs, field_mode=bind.FIELD_FIXED)
+        for s in range(NS):
+            t.dens(0, s)[...] = pb.dens[0][s]
+        er, ez, _ = pb.fields[0]
+        t.set_fixed_field(0, er, ez, pb.specs[0].zeros())
+        step = lambda: t.rk2(50.0)  # noqa: E731
+        threads = 1
+    step()
+    n, t0 = 0, time.perf_counter()
+    while n < max_steps and (time.perf_counter() - t0 < seconds or n == 0):
+        step()
+        n += 1
+    el = time.perf_counter() - t0
+    return NR * SAMPLE_NZ * NTHETA * NS * n / el, threads, kind, n, el
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import bind
+    omp = bind.ref_available(True)
+    # each "step" is one RK2 step of the 512 x 64 x 16 slab
+    from arcos_b200 import workloads
+    pb = workloads.plain(nr=NR, nz=SAMPLE_NZ, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=0)
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    if bind.ref_available(omp):
+        t = bind.RefTree(pb.params, pb.model, pb.specs, field_mode=bind.FIELD_FIXED, omp=omp)
+        kind = "reference"
+        step = lambda: t.rk2_sw(50.0, per_plane=True, zero_all=False)  # noqa: E731
+    else:
+        t = bind.PortTree(pb.params, pb.model, pb.specs, field_mode=bind.FIELD_FIXED)
+        kind, threads = "port", 1
+        step = lambda: t.rk2(50.0)  # noqa: E731
+    for s in range(NS):
+        t.dens(0, s)[...] = pb.dens[0][s]
+    er, ez, _ = pb.fields[0]
+    t.set_fixed_field(0, er, ez, pb.specs[0].zeros())
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    el = time.perf_counter() - t0
+    value = NR * SAMPLE_NZ * NTHETA * NS * args.steps / el
+    sample = (f"each step: one RK2 step of a {NR}x{SAMPLE_NZ}x{NTHETA} slab of the grid "
+              f"({'OpenMP build' if omp else 'serial build'})")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": workload_config({"reference_sample": sample}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- device ----
+def run_device(args):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from arcos_b200 import workloads
+    from arcos_b200._lib import check
+    from arcos_b200.cdr import CdrTree
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev_id = torch.cuda.current_device()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allmax(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    pb = workloads.plain(nr=NR, nz=NZ, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=rank)
+    stream = torch.cuda.Stream()
+    tree = CdrTree(pb.params, pb.model, pb.specs, stream=stream.cuda_stream)
+    for s in range(NS):
+        tree.upload(0, "dens", pb.dens[0][s], s)
+    tree.set_fixed_field(pb.fields)
+    L, h = tree.L, tree.h
+    warm = max(4, args.warmup + (args.warmup & 1))
+    steps = args.steps + (args.steps & 1)
+    check(L.arcos_run_prepare(h, 50.0))
+    check(L.arcos_run_enqueue(h, warm))
+    torch.cuda.synchronize()
+
+    clk = ClockSampler(dev_id) if rank == 0 else None
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    w0 = time.time()
+    e0.record(stream)
+    check(L.arcos_run_enqueue(h, steps))
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    w1 = time.time()
+    barrier()
+    ms = e0.elapsed_time(e1) / steps
+    ms = allmax(ms)
+    clocks = clk.summary(w0, w1) if clk else None
+    if clk:
+        clk.stop()
+    st, hlast, err = tree.family_state(0)
+    if err:
+        raise RuntimeError(f"device error bits {err}")
+
+    cells = NR * NZ * NTHETA
+    value = world * cells * NS / (ms / 1e3)
+
+    # per-kernel durations (same work, stage kernels launched one by one)
+    nk = 20
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    s1 = s2 = 0.0
+    for k in range(nk):
+        src = k & 1
+        ev[0].record(stream)
+        check(L.arcos_enqueue_stage(h, 1, src))
+        ev[1].record(stream)
+        check(L.arcos_enqueue_stage(h, 2, src))
+        ev[2].record(stream)
+        ev[2].synchronize()
+        s1 += ev[0].elapsed_time(ev[1])
+        s2 += ev[1].elapsed_time(ev[2])
+    s1 /= nk
+    s2 /= nk
+    bytes_s1 = 8 * (2 * NS + 2) * cells          # reads n0[S], er, ez; writes d0[S]
+    bytes_s2 = 8 * (3 * NS + 2) * cells          # reads n0[S], d0[S], er, ez; writes n1[S]
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fp:
+            peaks = json.load(fp)
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    dom_ms, dom_bytes, dom_name = (s2, bytes_s2, "stage-2 kernel") if s2 >= s1 else (s1, bytes_s1, "stage-1 kernel")
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "stage_kernels_plain3d.json")
+    if os.path.exists(prof):
+        try:
+            with open(prof) as fp:
+                traffic = json.load(fp).get("dram_bytes_per_launch", {}).get(
+                    "stage2" if dom_name.startswith("stage-2") else "stage1")
+        except Exception:
+            traffic = None
+    step_bytes = 8 * (5 * NS + 4) * cells
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+                "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
+                "kernel_ms": dom_ms, "step_achieved_gbs": step_bytes / (ms / 1e3) / 1e9,
+                "step_frac": step_bytes / (ms / 1e3) / 1e9 / peak}
+
+    # end to end through the C ABI with host buffers: H2D of the densities,
+    # one cdr_rk2 step (arcos_run), D2H of the densities, every step
+    e2e_steps = max(3, min(10, args.steps))
+    sp = pb.specs[0]
+    host = [torch.empty(sp.shape, dtype=torch.float64, pin_memory=True) for _ in range(NS)]
+    for s in range(NS):
+        host[s].numpy()[...] = tree.download(0, "dens", s)
+    DPp = C.POINTER(C.c_double)
+    ptrs = [C.cast(C.c_void_p(x.data_ptr()), DPp) for x in host]
+    dts = np.zeros(1)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for s in range(NS):
+            check(L.arcos_upload(h, 0, 0, 0, s, ptrs[s]))
+        check(L.arcos_run(h, 1, 50.0, dts.ctypes.data_as(DPp)))
+        for s in range(NS):
+            check(L.arcos_download(h, 0, 0, 0, s, ptrs[s]))
+    torch.cuda.synchronize()
+    e2e_s = allmax(time.perf_counter() - t0)
+    barrier()
+    arr_bytes = int(np.prod(sp.shape)) * 8
+    e2e = {"value": world * cells * NS * e2e_steps / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": NS * arr_bytes, "d2h_bytes_per_step": NS * arr_bytes,
+           "steps": e2e_steps, "api": "arcos_upload + arcos_run(1 step) + arcos_download"}
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            v, thr, kind, n, el = cpu_baseline_sample(omp=False)
+            cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": kind,
+                   "sample": f"{n} RK2 steps of a {NR}x{SAMPLE_NZ}x{NTHETA} slab of the grid "
+                             f"({el:.1f} s, serial build as shipped)"}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded)",
+                "config": workload_config({"replicas": world}),
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": 2 * steps, "clocks": clocks,
+                "stage_kernel_ms": {"stage1": s1, "stage2": s2},
+                "dt_last": hlast}
+        print(json.dumps(line), flush=True)
+    tree.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_device(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,204 @@
+/* arcos_cdr.h — C ABI of the B200 (sm_100a) arcos CDR density update.
+ *
+ * Plain C types only (pointers, sizes, ints, doubles).  Every call returns an
+ * int status (ARCOS_OK = 0); arcos_last_error() holds a message for the last
+ * failure of the calling thread.  The reference reports failures with fatal()
+ * -> exit(-1) and assert (include/cstream.h:47-51); this library returns
+ * instead, and the legacy adapter of INTEGRATION.md turns a non-zero status
+ * back into fatal().
+ *
+ * Host arrays use the reference rz_array layout (include/rz_array.h:11-22,
+ * src/rz_array.c:23-96): r fastest, two ghost cells on each side, row stride
+ * nr+4, plane stride (nr+4)(nz+4); one plane for ntheta == 1, else ntheta+4
+ * planes starting at theta = -2.
+ *
+ * A context holds one kinetic model and one grid family (a root and its
+ * refinement patches: the tree of tree.h).  Each grid has two storage sets,
+ * ARCOS_SET_GRID and ARCOS_SET_INTER, for the two RK2 stages (the reference's
+ * `grid` and `inter` trees, src/cdr.c:1262-1327).
+ */
+#ifndef ARCOS_CDR_H
+#define ARCOS_CDR_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ARCOS_OK            0
+#define ARCOS_ERR_ARG       1   /* bad argument or size */
+#define ARCOS_ERR_CUDA      2   /* CUDA runtime error */
+#define ARCOS_ERR_NAN       3   /* CFL maxima invalid: the assert of cdr.c:1023 */
+#define ARCOS_ERR_SMALL_DT  4   /* more than 5 steps below warn_min_timestep (cdr.c:1296-1302) */
+#define ARCOS_ERR_TIMEOUT   5   /* a bounded device wait gave up */
+#define ARCOS_ERR_NOMEM     6
+#define ARCOS_ERR_STATE     7   /* call out of order (e.g. before arcos_commit) */
+
+#define ARCOS_MAX_SPECIES   16  /* rt.c:14 MAX_SPECIES is 15 */
+#define ARCOS_MAX_REACTIONS 32  /* rt.c:15 MAX_REACTIONS is 30 */
+#define ARCOS_MAX_IN        4   /* reaction.h:10 REACTION_MAX_IN */
+#define ARCOS_MAX_OUT       6   /* reaction.h:11 REACTION_MAX_OUT */
+
+/* array kinds for upload/download */
+#define ARCOS_DENS    0
+#define ARCOS_D_DENS  1
+#define ARCOS_ER      2
+#define ARCOS_EZ      3
+#define ARCOS_ETHETA  4
+#define ARCOS_EABS    5
+#define ARCOS_CHARGE  6
+
+#define ARCOS_SET_GRID  0
+#define ARCOS_SET_INTER 1
+
+/* boundary masks of include/grid.h:22-31 */
+#define ARCOS_BND_MASK_LEFT   1
+#define ARCOS_BND_MASK_RIGHT  2
+#define ARCOS_BND_MASK_BOTTOM 4
+#define ARCOS_BND_MASK_TOP    8
+
+/* Snapshot of the reference globals the update reads
+ * (include/parameters.h:24-61, include/species.h:12-20). */
+typedef struct {
+  int no_species;
+  double charge[ARCOS_MAX_SPECIES];
+  double mass[ARCOS_MAX_SPECIES];          /* mobility = 1/mass; <= 0 immobile */
+  double diffusion_coeff;
+  double nu_a, nu_d, nu_rt;
+  double warn_min_timestep;
+  int cdr_bnd_bottom, cdr_bnd_top, cdr_bnd_right;   /* +1 Neumann, -1 Dirichlet */
+  double E_x, E_y, E_z;                    /* applied field (cstream.c:400-455) */
+  double z_cutoff;                         /* cdr.c:37 (1e7) */
+  double L_r, L_z;
+  int gridpoints_r, gridpoints_z;
+  int max_ntheta;
+  int max_levels, extra_pois_levels;       /* dr[]/dz[] as init_gridsizes_a, cstream.c:276-306 */
+  int per_plane;                           /* 1: drift/diffusion on every theta plane;
+                                              0: the reference's literal behaviour, where the
+                                              Fortran sees only the theta = -2 plane
+                                              (cdr.c:945-949 with rz_array.c:42-58) */
+} arcos_params;
+
+/* ---- context ---------------------------------------------------------- */
+int arcos_create (const arcos_params *p, void **ctx_out);
+int arcos_destroy (void *ctx);
+const char *arcos_last_error (void);
+/* cudaStream_t as void*; 0 = the legacy default stream. */
+int arcos_set_stream (void *ctx, void *stream);
+
+/* Replaces react_add + react_table_read (reaction.c:48-66, react_table.c:73-111):
+ * reactions are applied in the order they are added (react_apply_all,
+ * reaction.c:203-210).  values holds steps+1 entries. */
+int arcos_add_reaction (void *ctx, int nin, const int *inputs, int nout,
+                        const int *outputs, double e_min, double e_step,
+                        int steps, double underflow, double overflow,
+                        const double *values);
+
+/* Adds a grid; parent = -1 for the root, otherwise the id of the parent
+ * (children are visited in reverse order of creation, as tree.h add_child
+ * prepends).  Returns the grid id (>= 0) in *id. */
+int arcos_grid_new (void *ctx, int r0, int z0, int r1, int z1, int ntheta,
+                    int level, int ext_bound, int parent, int *id);
+/* Allocates device storage (zeroed, as rz_new_3d_a's calloc) and builds the
+ * patch work lists.  No grid may be added afterwards. */
+int arcos_commit (void *ctx);
+/* Device bytes held by the context. */
+int arcos_device_bytes (void *ctx, size_t *bytes);
+
+int arcos_upload (void *ctx, int grid, int set, int kind, int species,
+                  const double *host);
+int arcos_download (void *ctx, int grid, int set, int kind, int species,
+                    double *host);
+int arcos_sync (void *ctx);
+
+/* ---- the field seam ----------------------------------------------------
+ * Replaces what pois_solve_a (src/poisson.c:763) writes into the CDR grids:
+ * the host field solve's er/ez/etheta for one grid and set.  The library then
+ * performs the rest of cdr_calc_field_r (cdr.c:532-580) on the device:
+ * cdr_add_ext_field, cdr_calc_eabs and (3-D) cdr_set_periodic. */
+int arcos_set_field (void *ctx, int grid, int set, const double *er,
+                     const double *ez, const double *etheta);
+/* Field callback for runs with the field solve in the loop: called once per
+ * RK2 stage with the root grid's charge (rz layout) and must fill er, ez,
+ * etheta (rz layout).  Return non-zero to abort the step. */
+typedef int (*arcos_field_fn) (void *user, int stage, const double *charge,
+                               double *er, double *ez, double *etheta);
+int arcos_set_field_fn (void *ctx, arcos_field_fn fn, void *user);
+
+/* ---- reference entry points (src/cdr.c, src/reaction.c) -----------------
+ * Each acts on the whole grid family of the given storage set, with the
+ * recursion of the reference's *_r variant. */
+int arcos_cdr_nonegative_r (void *ctx, int set);            /* cdr.c:703-721 */
+int arcos_cdr_set_ext_bnd_r (void *ctx, int set);           /* cdr.c:726-824 */
+int arcos_cdr_set_periodic_r (void *ctx, int set);          /* cdr.c:288-310 */
+int arcos_cdr_restrict_r (void *ctx, int set);              /* cdr.c:2050-2097 */
+int arcos_cdr_set_bnd_r (void *ctx, int set);               /* cdr.c:1888-1948 */
+int arcos_cdr_match_r (void *ctx, int set);                 /* cdr.c:1763-1882 */
+int arcos_prepare_grid (void *ctx, int set);                /* cdr.c:1334-1351 */
+int arcos_cdr_add_ext_field_r (void *ctx, int set);         /* cdr.c:595-625 */
+int arcos_cdr_calc_eabs_r (void *ctx, int set);             /* cdr.c:668-695 */
+int arcos_cdr_calc_charge_r (void *ctx, int set);           /* cdr.c:361-389 */
+int arcos_react_apply_all (void *ctx, int set);             /* reaction.c:192-211 */
+int arcos_cdr_advect_diffu_r (void *ctx, int set);          /* cdr.c:900-955 */
+int arcos_cdr_calc_d_dens (void *ctx, int set);             /* cdr.c:830-835 */
+int arcos_cdr_courant (void *ctx, int set, double *h);      /* cdr.c:971-1061 */
+/* inter.dens = grid.dens + h grid.d_dens, then charge (cdr.c:1075-1100,1184-1208) */
+int arcos_cdr_update (void *ctx, double h);
+/* grid.dens = grid.dens + h/2 grid.d_dens + h/2 inter.d_dens, then charge (cdr.c:1107-1162) */
+int arcos_cdr_rk2_update (void *ctx, double h);
+/* One full step, cdr_rk2 (cdr.c:1262-1327).  h is the attempted step; the
+ * step taken is returned in *h_used.  Uses the field set with
+ * arcos_set_field (fixed) or the callback of arcos_set_field_fn. */
+int arcos_cdr_rk2 (void *ctx, double h, double t, double *h_used);
+
+/* nsteps steps of cdr_rk2 with a fixed field, replayed from a CUDA graph.
+ * dt_out (may be NULL) receives the nsteps steps taken. */
+int arcos_run (void *ctx, int nsteps, double h, double *dt_out);
+
+/* ---- batching, timing and inspection (no single reference counterpart) ---- */
+/* Applied field E0 of one family (an independent grid tree of the context);
+ * the reference has one global E0 (cstream.c:400-431), a batch of runs has one
+ * per instance. */
+int arcos_set_family_field (void *ctx, int fam, double Ex, double Ey, double Ez);
+/* The device half of cdr_calc_field_r after arcos_set_field was called for
+ * every grid of the set: external field, |E|, theta periodicity. */
+int arcos_field_post (void *ctx, int set);
+/* 1: launch every kernel once per patch (the plain form the batched
+ * persistent launch is compared with); 0: batched (default). */
+int arcos_set_per_patch (void *ctx, int on);
+/* Tile shape of the stencil kernel: 0 = 32x16 cells (128 threads),
+ * 1 = 32x32 (128 threads), 2 = 32x32 (256 threads).  Any time. */
+int arcos_set_tile (void *ctx, int cfg);
+int arcos_get_tile (void *ctx);
+int arcos_num_items (void *ctx);
+/* Device-timed runs: arcos_run_prepare sets the attempted step, computes the
+ * first step's h and instantiates the two-step CUDA graph; arcos_run_enqueue
+ * enqueues nsteps (even) steps on the context stream without synchronising. */
+int arcos_run_prepare (void *ctx, double h);
+int arcos_run_enqueue (void *ctx, int nsteps);
+/* Enqueue one fused stage kernel (1: stage 1, 2: stage 2) reading dens[src]. */
+int arcos_enqueue_stage (void *ctx, int mode, int src);
+int arcos_family_state (void *ctx, int fam, int *steps, double *h, int *error_bits);
+
+/* ---- narrow seam (arcos_f90/src/cdr_advect_diffu_wrap.c:25-41) ----------
+ * Same signature and argument meaning as the reference wrapper around the
+ * Fortran cdr_advect_vec: adds the drift/diffusion divergence of one species
+ * to d_dens on one 2-D (r0-2:r1+1, z0-2:z1+1) slab.  Host pointers; the
+ * arrays are copied to the device and d_dens back.  sprite_module must be 0.
+ * On failure prints the error and exits, like the reference's fatal(). */
+void arcos_cdr_advect_vec (double mass, double charge, double *dens_array,
+                           double *d_dens_array, double *er_array, int er_len,
+                           double *ez_array, int ez_len, double diffusion_coeff,
+                           double dr, double dz, int sprite_module, int r0,
+                           int r1, int z0, int z1);
+/* The same on device pointers (cudaStream_t as void*), returning a status. */
+int arcos_cdr_advect_vec_dev (double mass, double charge, const double *dens,
+                              double *d_dens, const double *er, const double *ez,
+                              double diffusion_coeff, double dr, double dz,
+                              int r0, int r1, int z0, int z1, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
