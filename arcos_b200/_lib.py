@@ -69,7 +69,7 @@ def lib():
                  "arcos_prepare_grid", "arcos_cdr_add_ext_field_r", "arcos_cdr_calc_eabs_r",
                  "arcos_cdr_calc_charge_r", "arcos_react_apply_all", "arcos_cdr_advect_diffu_r",
                  "arcos_cdr_calc_d_dens", "arcos_field_post", "arcos_set_per_patch",
-                 "arcos_set_tile", "arcos_run_enqueue"):
+                 "arcos_set_tile", "arcos_set_exact", "arcos_set_tma", "arcos_run_enqueue"):
         getattr(L, name).argtypes = [VP, C.c_int]
     L.arcos_get_tile.argtypes = [VP]
     L.arcos_cdr_courant.argtypes = [VP, C.c_int, DP]

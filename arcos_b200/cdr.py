@@ -76,7 +76,8 @@ class CdrTree:
     """One or more grid families resident on the current CUDA device."""
 
     def __init__(self, params: Params, model: KineticModel, specs: Sequence[GridSpec],
-                 per_patch: bool = False, tile: int = 1, stream: Optional[int] = None):
+                 per_patch: bool = False, tile: int = 0, stream: Optional[int] = None,
+                 exact: bool = False):
         self.L = lib()
         self.params, self.model, self.specs = params, model, list(specs)
         self._p = make_params(params, model)
@@ -101,6 +102,7 @@ class CdrTree:
                                         sp.ext_bound, parent, C.byref(gid)))
             self.ids.append(gid.value)
         check(self.L.arcos_set_tile(self.h, tile))
+        check(self.L.arcos_set_exact(self.h, 1 if exact else 0))
         check(self.L.arcos_set_per_patch(self.h, 1 if per_patch else 0))
         check(self.L.arcos_commit(self.h))
         self._field_cb = None
@@ -216,6 +218,12 @@ class CdrTree:
         st, h, e = C.c_int(0), C.c_double(0), C.c_int(0)
         check(self.L.arcos_family_state(self.h, fam, C.byref(st), C.byref(h), C.byref(e)))
         return st.value, h.value, e.value
+
+    def set_tma(self, on: bool):
+        check(self.L.arcos_set_tma(self.h, 1 if on else 0))
+
+    def set_exact(self, on: bool):
+        check(self.L.arcos_set_exact(self.h, 1 if on else 0))
 
     def set_tile(self, cfg: int):
         check(self.L.arcos_set_tile(self.h, cfg))

@@ -7,6 +7,9 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "../../include/arcos_cdr.h"
 #include "device_common.cuh"
 #include "stage_kernel.cuh"
@@ -39,7 +42,7 @@ fail (int code, const std::string &msg)
       return fail (ARCOS_ERR_CUDA, std::string ("kernel launch: ") + cudaGetErrorString (e_)); \
   } while (0)
 
-constexpr int N_TILE_CFG_MAX = 3;
+constexpr int N_TILE_CFG_MAX = 2;
 
 struct GridH {
   int r0, z0, r1, z1, ntheta, level, ext_bound, parent, fam;
@@ -74,7 +77,11 @@ struct Ctx {
   int n_items = 0;
   std::vector<int> item_off, item_cnt;
   int tile_cfg = 1;                   // index into TILE_WY / TILE_RPW
-  int occ[4][N_TILE_CFG_MAX] = {};
+  int occ[2][4][N_TILE_CFG_MAX] = {};
+  int exact = 0;                      // 1: bit-exact flux limiter, 0: division-free form
+  int use_tma = 1;                    // stage tiles with bulk tensor copies (else cp.async)
+  CUtensorMap *maps_d = nullptr;      // [patch][set][array]
+  int maps_per_patch = 0;
   int *plist_d = nullptr;             // 0..npatch-1
   std::vector<int> level_off, level_cnt;   // children lists per level inside kids_d
   int *kids_d = nullptr;
@@ -178,9 +185,9 @@ constexpr int NODES_SMEM_MAX = 24 * 1024 / (int) sizeof (TableNode);
 
 // Tile shapes the autotuner chooses from: (warps per block, rows per thread);
 // tiles are 32 columns wide and WY * RPW rows high.
-constexpr int N_TILE_CFG = 3;
-constexpr int TILE_WY[N_TILE_CFG] = {4, 4, 8};
-constexpr int TILE_RPW[N_TILE_CFG] = {4, 8, 4};
+constexpr int N_TILE_CFG = 2;
+constexpr int TILE_WY[N_TILE_CFG] = {4, 8};
+constexpr int TILE_RPW[N_TILE_CFG] = {4, 4};
 
 template <int NS, int MODE, int WY, int RPW>
 size_t
@@ -191,17 +198,17 @@ stage_smem_t (int n_nodes)
   return b;
 }
 
-template <int NS, int MODE, int WY, int RPW>
+template <int NS, int MODE, int WY, int RPW, bool FAST>
 cudaError_t
 launch_stage_t (const Model &M, const StageArgs &A, int blocks, cudaStream_t s, int *occ)
 {
   const size_t sm = stage_smem_t<NS, MODE, WY, RPW> (A.n_nodes);
-  cudaFuncSetAttribute (k_stage<NS, MODE, WY, RPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+  cudaFuncSetAttribute (k_stage<NS, MODE, WY, RPW, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
   if (occ) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor (occ, k_stage<NS, MODE, WY, RPW>, 32 * WY, sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor (occ, k_stage<NS, MODE, WY, RPW, FAST>, 32 * WY, sm);
     return cudaGetLastError ();
   }
-  k_stage<NS, MODE, WY, RPW><<<blocks, 32 * WY, sm, s>>> (M, A);
+  k_stage<NS, MODE, WY, RPW, FAST><<<blocks, 32 * WY, sm, s>>> (M, A);
   return cudaGetLastError ();
 }
 
@@ -209,10 +216,12 @@ template <int NS, int MODE>
 cudaError_t
 launch_stage_c (int cfg, const Model &M, const StageArgs &A, int blocks, cudaStream_t s, int *occ)
 {
+  const bool fast = !A.exact;
   switch (cfg) {
-  case 0: return launch_stage_t<NS, MODE, 4, 4> (M, A, blocks, s, occ);
-  case 1: return launch_stage_t<NS, MODE, 4, 8> (M, A, blocks, s, occ);
-  default: return launch_stage_t<NS, MODE, 8, 4> (M, A, blocks, s, occ);
+  case 0: return fast ? launch_stage_t<NS, MODE, 4, 4, true> (M, A, blocks, s, occ)
+                      : launch_stage_t<NS, MODE, 4, 4, false> (M, A, blocks, s, occ);
+  default: return fast ? launch_stage_t<NS, MODE, 8, 4, true> (M, A, blocks, s, occ)
+                       : launch_stage_t<NS, MODE, 8, 4, false> (M, A, blocks, s, occ);
   }
 }
 
@@ -247,9 +256,10 @@ launch_stage (int mode, int ns, int cfg, const Model &M, const StageArgs &A, int
 int
 stage_blocks (Ctx *c, int mode, int n_items)
 {
-  int &o = c->occ[mode][c->tile_cfg];
+  int &o = c->occ[c->exact][mode][c->tile_cfg];
   if (o == 0) {
     StageArgs A{};
+    A.exact = c->exact;
     A.n_nodes = (int) c->nodes_h.size ();
     int b = 0;
     launch_stage (mode, c->M.ns, c->tile_cfg, c->M, A, 0, 0, &b);
@@ -273,6 +283,9 @@ base_args (Ctx *c)
   A.done = c->done_d;
   A.n_nodes = (int) c->nodes_h.size ();
   A.nodes_smem = A.n_nodes > 0 && A.n_nodes <= NODES_SMEM_MAX;
+  A.exact = c->exact;
+  A.maps = (c->use_tma && c->maps_d) ? c->maps_d : nullptr;
+  A.maps_per_patch = c->maps_per_patch;
   return A;
 }
 
@@ -509,6 +522,8 @@ check_state_errors (Ctx *c)
   for (int f = 0; f < c->nfam; f++) {
     if (st[f].error & (1 << ARCOS_ERR_NAN))
       return fail (ARCOS_ERR_NAN, "CFL maxima invalid (the assertion of cdr_courant, cdr.c:1023), family " + std::to_string (f));
+    if (st[f].error & (1 << ARCOS_ERR_TIMEOUT))
+      return fail (ARCOS_ERR_TIMEOUT, "a bounded wait for a tile copy gave up, family " + std::to_string (f));
     if (st[f].error & (1 << ARCOS_ERR_SMALL_DT))
       return fail (ARCOS_ERR_SMALL_DT, "too many steps below warn_min_timestep (cdr.c:1296-1302), family " + std::to_string (f));
   }
@@ -680,6 +695,7 @@ arcos_destroy (void *ctx)
   cudaFree (c->plist_d); cudaFree (c->kids_d); cudaFree (c->strips_d); cudaFree (c->ext_d);
   for (int s = 0; s < 2; s++) { cudaFree (c->match_src_d[s]); cudaFree (c->match_dst_d[s]); }
   cudaFree (c->match_tmp_d);
+  cudaFree (c->maps_d);
   if (c->own_stream) cudaStreamDestroy (c->own_stream);
   delete c;
   return ARCOS_OK;
@@ -719,6 +735,7 @@ arcos_add_reaction (void *ctx, int nin, const int *inputs, int nout, const int *
   M.r_steps[r] = steps;
   M.r_e_min[r] = e_min; M.r_e_step[r] = e_step;
   M.r_under[r] = underflow; M.r_over[r] = overflow;
+  M.r_inv_step_f[r] = (float) (1.0 / e_step);
   M.r_node_off[r] = (int) c->nodes_h.size ();
   // react_apply's updates in order (reaction.c:147-155): inputs (-rate) then
   // outputs (+rate), only for charged species
@@ -862,6 +879,54 @@ elem_offset (Ctx *c, long long key, int set)
   return (P.arr (set, K_DENS, s) - c->pool) + col + row * P.pitch + plane * P.plane_stride;
 }
 
+// TMA descriptors: one 3-D map (columns incl. padding, rows, planes) per array
+// of every patch and storage set; the box is one staged tile (TX + 4 columns
+// by TY + 4 rows of one plane).  Boxes that run past the last row or column
+// are filled with zeros by the hardware; those cells are never used.
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int
+build_maps (Ctx *c, int ty)
+{
+  cudaFree (c->maps_d);
+  c->maps_d = nullptr;
+  if (!c->use_tma) return ARCOS_OK;
+  if (!g_encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint ("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess
+        || q != cudaDriverEntryPointSuccess || !fn) {
+      c->use_tma = 0;                     // staging falls back to cp.async (same results)
+      return ARCOS_OK;
+    }
+    g_encode = (PFN_cuTensorMapEncodeTiled_v12000) fn;
+  }
+  const int np = (int) c->pd_h.size ();
+  const int per_set = 2 * c->M.ns + 5;
+  c->maps_per_patch = 2 * per_set;
+  std::vector<CUtensorMap> maps ((size_t) np * c->maps_per_patch);
+  for (int p = 0; p < np; p++) {
+    const PatchDesc &P = c->pd_h[p];
+    const cuuint64_t dims[3] = {(cuuint64_t) P.pitch, (cuuint64_t) (P.nz + 4), (cuuint64_t) P.planes};
+    const cuuint64_t strides[2] = {(cuuint64_t) P.pitch * 8, (cuuint64_t) P.plane_stride * 8};
+    const cuuint32_t box[3] = {TXP, (cuuint32_t) (ty + 4), 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    for (int set = 0; set < 2; set++)
+      for (int a = 0; a < per_set; a++) {
+        double *ptr = P.base + (long long) (set * per_set + a) * P.asz;
+        CUresult r = g_encode (&maps[(size_t) p * c->maps_per_patch + set * per_set + a],
+                               CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ptr, dims, strides, box, es,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+          return fail (ARCOS_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string ((int) r) + ")");
+      }
+  }
+  CK (cudaMalloc (&c->maps_d, sizeof (CUtensorMap) * maps.size ()));
+  CK (cudaMemcpy (c->maps_d, maps.data (), sizeof (CUtensorMap) * maps.size (), cudaMemcpyHostToDevice));
+  return ARCOS_OK;
+}
+
 // Work list of the tile kernel: per patch, per real plane, tiles of 32 columns
 // by TY rows (TY from the tile shape).
 int
@@ -887,7 +952,7 @@ build_items (Ctx *c)
   CK (cudaMalloc (&c->items_d, sizeof (WorkItem) * items.size ()));
   CK (cudaMemcpy (c->items_d, items.data (), sizeof (WorkItem) * items.size (), cudaMemcpyHostToDevice));
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
-  return ARCOS_OK;
+  return build_maps (c, ty);
 }
 
 }  // namespace
@@ -1542,8 +1607,20 @@ arcos_num_items (void *ctx)
   return c ? c->n_items : -1;
 }
 
-// Tile shape of the stencil kernel (0: 32x16 cells, 128 threads; 1: 32x32,
-// 128 threads; 2: 32x32, 256 threads).  May be changed after arcos_commit.
+// Flux-limiter arithmetic: 1 = the reference's operations exactly (bit-
+// identical results), 0 = the division-free form (default).
+int
+arcos_set_exact (void *ctx, int on)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  c->exact = on ? 1 : 0;
+  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  return ARCOS_OK;
+}
+
+// Tile shape of the stencil kernel (0: 32x16 cells, 128 threads; 1: 32x16,
+// 256 threads... see TILE_WY/TILE_RPW).  May be changed after arcos_commit.
 int
 arcos_set_tile (void *ctx, int cfg)
 {
@@ -1555,11 +1632,46 @@ arcos_set_tile (void *ctx, int cfg)
   return ARCOS_OK;
 }
 
+// 1: stage tiles with TMA bulk tensor copies (default), 0: with cp.async.
+int
+arcos_set_tma (void *ctx, int on)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  c->use_tma = on ? 1 : 0;
+  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  if (c->committed) return build_maps (c, TILE_WY[c->tile_cfg] * TILE_RPW[c->tile_cfg]);
+  return ARCOS_OK;
+}
+
 int
 arcos_get_tile (void *ctx)
 {
   Ctx *c = (Ctx *) ctx;
   return c ? c->tile_cfg : -1;
+}
+
+// Host evaluation of the device table lookup (thresholds + node), for tests:
+// rates[i] = k(|E| = eabs[i]) exactly as the stage kernel computes it.  No
+// CUDA call is made.
+int
+arcos_table_rates (double e_min, double e_step, int steps, double underflow, double overflow,
+                   const double *values, const double *eabs, int n, double *rates)
+{
+  if (steps < 1 || !values || !eabs || !rates || n < 0 || !(e_step > 0))
+    return fail (ARCOS_ERR_ARG, "arcos_table_rates: bad argument");
+  std::vector<TableNode> nodes;
+  build_nodes (e_min, e_step, steps, values, nodes);
+  for (int i = 0; i < n; i++) {
+    const double e = fabs (eabs[i]);
+    if (!(e >= nodes[0].thr)) { rates[i] = underflow; continue; }
+    if (e >= nodes[steps + 1].thr) { rates[i] = overflow; continue; }
+    int k = 0;
+    while (k < steps && e >= nodes[k + 1].thr) k++;
+    const TableNode &nd = nodes[k];
+    rates[i] = nd.val + nd.slope * (e - nd.e1);
+  }
+  return ARCOS_OK;
 }
 
 // ---- narrow seam: arcos_cdr_advect_vec ------------------------------------------
@@ -1588,6 +1700,7 @@ seam_prepare (double mass, double charge, double diffusion_coeff, double dr, dou
   int r = arcos_create (&p, &vc);
   if (r) return r;
   c = (Ctx *) vc;
+  c->exact = 1;                          // a drop-in for the Fortran kernel: its arithmetic exactly
   c->g.push_back (GridH{r0, z0, r1, z1, 1, 0, 0, -1, 0, {}});
   c->nfam = 1;
   c->fam_root.push_back (0);

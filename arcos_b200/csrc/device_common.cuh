@@ -83,6 +83,7 @@ struct Model {
   int r_node_off[ARCOS_MAXR];     // first node of the reaction in the node array
   double r_e_min[ARCOS_MAXR], r_e_step[ARCOS_MAXR];
   double r_under[ARCOS_MAXR], r_over[ARCOS_MAXR];
+  float r_inv_step_f[ARCOS_MAXR];   // 1/e_step for the single-precision position estimate
   double diffusion_coeff, nu_a, nu_d, nu_rt, warn_min_timestep, z_cutoff, dtheta;
   int bnd_sign[4];                // cdr_ext_bnd_cond[] (cdr.c:79-84), index BND_*
   int per_plane;

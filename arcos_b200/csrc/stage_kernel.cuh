@@ -16,6 +16,7 @@
 //
 // Tiling: see the comment above k_stage.
 #pragma once
+#include <cuda.h>
 #include "device_common.cuh"
 
 namespace arcos {
@@ -48,49 +49,92 @@ struct StageArgs {
                         // (no reactions), as the Fortran kernel does (.f90:113-130)
   int n_nodes;          // reaction-table nodes
   int nodes_smem;       // copy the nodes to shared memory
+  int exact;            // bit-exact flux limiter (host-side dispatch)
+  const CUtensorMap *maps;   // TMA descriptors [patch][set][array], or null (cp.async staging)
+  int maps_per_patch;
 };
 
 __device__ __forceinline__ double clamp0 (double x) { return 0 > x ? 0 : x; }   // MYMAX(0, x)
 __device__ __forceinline__ double mymin (double x, double y) { return x < y ? x : y; }  // MYMIN
 
-// Radial face flux (mat_cdr_f_ad_r, .f90:259-306).
+// Radial face flux (mat_cdr_f_ad_r, .f90:259-306), written with selects so a
+// warp never diverges.  For |dC| <= verysmall psi is -1 (.f90:285-286).
 __device__ __forceinline__ double
 face_r (double nLL, double nL, double nR, double nRR, double v, double dd)
 {
-  double dC = nR - nL, psi, aux;
-  if (fabs (dC) > VERYSMALL_F90) {
-    double p = 0.0;
-    if (v >= 0.0) p = (nL - nLL) / dC;
-    else if (v < 0.0) p = (nRR - nR) / dC;
-    if (p <= 0.0) psi = 0.0;
-    else if (p >= 4.0) psi = 1.0;
-    else if (p >= POINT4_F90) psi = (1.0 + 0.5 * p) / 3.0;
-    else psi = p;
-  } else {
-    psi = -1.0;
-  }
-  aux = psi * dC;
+  const double dC = nR - nL;
+  const bool pos = v >= 0.0;
+  const double num = pos ? (nL - nLL) : (nRR - nR);
+  const double p = num / dC;                               // .f90:269 / :275
+  const double q = (1.0 + 0.5 * p) / 3.0;                  // .f90:283
+  double psi = p;
+  psi = (p >= POINT4_F90) ? q : psi;
+  psi = (p >= 4.0) ? 1.0 : psi;
+  psi = (p <= 0.0) ? 0.0 : psi;
+  psi = (fabs (dC) > VERYSMALL_F90) ? psi : -1.0;
+  double aux = psi * dC;
+  aux = pos ? nL + aux : nR - aux;
+  return aux * v - dd * dC;
+}
+
+// Axial face flux (mat_cdr_f_ad_z, .f90:335-384): the ratio takes v > 0
+// (strict), the upwind value v >= 0, and a masked face uses pij = +1.
+__device__ __forceinline__ double
+face_z (double nLL, double nL, double nR, double nRR, double v, double dd)
+{
+  const double dC = nR - nL;
+  const double num = (v > 0.0) ? (nL - nLL) : (nRR - nR);
+  const double p = num / dC;                               // .f90:346 / :352
+  const double q = (1.0 + 0.5 * p) / 3.0;                  // .f90:357
+  double pij = p;
+  pij = (p <= 0.0) ? 0.0 : pij;
+  pij = (p >= 4.0) ? 1.0 : pij;
+  pij = ((p > POINT4_F90) && (p < 4.0)) ? q : pij;
+  pij = (fabs (dC) > VERYSMALL_F90) ? pij : 1.0;
+  double aux = pij * dC;
   aux = (v >= 0.0) ? nL + aux : nR - aux;
   return aux * v - dd * dC;
 }
 
-// Axial face flux (mat_cdr_f_ad_z, .f90:335-384).
+// The same fluxes without divisions (the default, "fast" form).  psi * dC is
+// what the flux uses, and with p = num / dC:
+//   p <= 0          -> 0
+//   p >= 4          -> dC
+//   0.4 <= p < 4    -> ((1 + p/2) / 3) dC = (dC + num/2) / 3
+//   0 < p < 0.4     -> p dC = num
+// so the ratio never has to be formed.  The limiter is continuous at every
+// switch point, so this differs from the reference's rounding of p only in
+// the last bits of the flux (well inside 1e-12 relative per step).
 __device__ __forceinline__ double
-face_z (double nLL, double nL, double nR, double nRR, double v, double dd)
+psi_dc_fast (double num, double dC, bool strict_lo)
 {
-  double dC = nR - nL, pij, aux;
-  if (fabs (dC) > VERYSMALL_F90) {
-    double p = (v > 0.0) ? (nL - nLL) / dC : (nRR - nR) / dC;
-    pij = p;
-    if ((p > POINT4_F90) && (p < 4.0)) pij = (1.0 + 0.5 * p) / 3.0;
-    else if (p >= 4.0) pij = 1.0;
-    else if (p <= 0.0) pij = 0.0;
-  } else {
-    pij = 1.0;
-  }
-  aux = pij * dC;
+  const double an = fabs (num), ad = fabs (dC);
+  const bool same = (num > 0.0) == (dC > 0.0) && num != 0.0;     // p > 0
+  double r = num;
+  r = (strict_lo ? (an > POINT4_F90 * ad) : (an >= POINT4_F90 * ad)) ? (dC + 0.5 * num) * (1.0 / 3.0) : r;
+  r = (an >= 4.0 * ad) ? dC : r;
+  return same ? r : 0.0;
+}
+
+__device__ __forceinline__ double
+face_r_fast (double nLL, double nL, double nR, double nRR, double v, double dd)
+{
+  const double dC = nR - nL;
+  const bool pos = v >= 0.0;
+  const double num = pos ? (nL - nLL) : (nRR - nR);
+  double aux = (fabs (dC) > VERYSMALL_F90) ? psi_dc_fast (num, dC, false) : -dC;
+  aux = pos ? nL + aux : nR - aux;
+  return __fma_rn (aux, v, -(dd * dC));
+}
+
+__device__ __forceinline__ double
+face_z_fast (double nLL, double nL, double nR, double nRR, double v, double dd)
+{
+  const double dC = nR - nL;
+  const double num = (v > 0.0) ? (nL - nLL) : (nRR - nR);
+  double aux = (fabs (dC) > VERYSMALL_F90) ? psi_dc_fast (num, dC, true) : dC;
   aux = (v >= 0.0) ? nL + aux : nR - aux;
-  return aux * v - dd * dC;
+  return __fma_rn (aux, v, -(dd * dC));
 }
 
 // Reaction rate k(|E|) exactly as react_apply computes it (reaction.c:127-142):
@@ -104,8 +148,8 @@ table_rate (const Model &M, const TableNode *__restrict__ nodes, int r, double e
   const int steps = M.r_steps[r];
   if (!(eabs >= nd[0].thr)) return M.r_under[r];        // log_e < e_min (or NaN)
   if (eabs >= nd[steps + 1].thr) return M.r_over[r];     // log_e > e_min + e_step*steps
-  float lf = __log10f ((float) eabs);
-  float pf = (lf - (float) M.r_e_min[r]) / (float) M.r_e_step[r];
+  const float lf = __log10f ((float) eabs);
+  const float pf = (lf - (float) M.r_e_min[r]) * M.r_inv_step_f[r];
   int k = (pf > 0.f) ? (int) pf : 0;
   if (!(pf < (float) steps)) k = steps;
   while (k > 0 && eabs < nd[k].thr) k--;
@@ -181,7 +225,52 @@ cp_async16 (void *smem_dst, const void *gsrc)
 __device__ __forceinline__ void cp_async_commit () { asm volatile ("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all () { asm volatile ("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <int NS, int MODE, int WY, int RPW>
+// ---- TMA (cp.async.bulk.tensor) staging with an mbarrier ----
+__device__ __forceinline__ unsigned smem_u32 (const void *p) { return (unsigned) __cvta_generic_to_shared (p); }
+
+__device__ __forceinline__ void
+mbar_init (unsigned long long *bar, unsigned count)
+{
+  asm volatile ("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32 (bar)), "r"(count) : "memory");
+  asm volatile ("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void
+mbar_expect_tx (unsigned long long *bar, unsigned bytes)
+{
+  asm volatile ("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32 (bar)), "r"(bytes) : "memory");
+}
+
+// 3-D tile copy global -> shared, completion counted on the mbarrier (no multicast)
+__device__ __forceinline__ void
+tma_load_3d (void *dst, const void *tmap, int x, int y, int z, unsigned long long *bar)
+{
+  asm volatile (
+    "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+    " [%0], [%1, {%2, %3, %4}], [%5];\n"
+    ::"r"(smem_u32 (dst)), "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32 (bar))
+    : "memory");
+}
+
+// Bounded wait for the phase `parity` of the mbarrier: false after `limit`
+// polls (each poll may suspend the thread for a short, hardware-chosen time).
+__device__ __forceinline__ bool
+mbar_wait (unsigned long long *bar, unsigned parity, long long limit)
+{
+  const unsigned a = smem_u32 (bar);
+  for (long long i = 0; i < limit; i++) {
+    unsigned ok;
+    asm volatile ("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                  " selp.u32 %0, 1, 0, p;\n}\n"
+                  : "=r"(ok) : "r"(a), "r"(parity) : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+#define TMA_WAIT_LIMIT (1LL << 22)
+
+template <int NS, int MODE, int WY, int RPW, bool FAST>
 __global__ void __launch_bounds__ (32 * WY)
 k_stage (const __grid_constant__ Model M, const StageArgs A)
 {
@@ -190,18 +279,21 @@ k_stage (const __grid_constant__ Model M, const StageArgs A)
   constexpr int A_D = LY::A_D, A_F = LY::A_F;
   constexpr bool OTF = (MODE == M_S1 || MODE == M_S2);
   constexpr int NT = 32 * WY;
-  extern __shared__ double smem[];
+  extern __shared__ __align__ (128) double smem[];
+  __shared__ __align__ (8) unsigned long long tma_bar;
+  unsigned tma_phase = 0;
   double *opp = smem + NA * PL;
   const TableNode *nodes = A.nodes;
   __shared__ unsigned long long red_key[WY];
   const int t = threadIdx.x, lane = t & 31, wq = t >> 5;
 
+  if (A.maps && t == 0) mbar_init (&tma_bar, 1);
   if (A.nodes_smem) {
     TableNode *sn = reinterpret_cast<TableNode *> (smem + LY::DOUBLES);
     for (int i = t; i < A.n_nodes; i += NT) sn[i] = A.nodes[i];
     nodes = sn;
-    __syncthreads ();
   }
+  __syncthreads ();
   // staged element (row, col) of array a; row, col relative to the tile corner (zb-2, c0-2)
 #define SA(a_, row_, col_) smem[(a_) * PL + (row_) * TXP + (col_)]
 
@@ -225,21 +317,49 @@ k_stage (const __grid_constant__ Model M, const StageArgs A)
     const int nset = (MODE == M_DERIV) ? A.nset : (MODE == M_AMR2 ? 1 : A.src);
     const long long pbase = P.off (c0 - 2, zb - 2, plane);   // tile corner in this plane
 
-    // ---- stage the tile ----
-    {
-      const int total = nrow * nchunk;
-      for (int i = t; i < total; i += NT) {
-        const int row = i / nchunk, ch = i - row * nchunk;
-        const long long go = pbase + (long long) row * P.pitch + 2 * ch;
-        const int so = row * TXP + 2 * ch;
+    // ---- stage the tile: warp-strided rows, one 16-byte chunk per lane ----
+    const double *src_n[NS];
+    const double *src_d[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      src_n[s] = P.arr (nset, K_DENS, s) + pbase;
+      src_d[s] = (MODE == M_S2) ? P.arr (0, K_DDENS, s) + pbase : nullptr;
+    }
+    const double *src_er = P.arr (fset, K_ER) + pbase, *src_ez = P.arr (fset, K_EZ) + pbase;
+    const double *src_ea = P.arr (fset, K_EABS) + pbase;
+    if (A.maps) {
+      // one thread moves the whole tile with bulk tensor copies
+      if (t == 0) {
+        const CUtensorMap *tm = A.maps + (size_t) w.patch * A.maps_per_patch;
+        const int per_set = 2 * P.ns + 5;
+        const int x = c0, y = zb, z = plane - P.theta0;
+        unsigned bytes = (unsigned) (sizeof (double) * PL) * (unsigned) (NA - (etz ? 1 : 0));
+        asm volatile ("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx (&tma_bar, bytes);
 #pragma unroll
         for (int s = 0; s < NS; s++) {
-          cp_async16 (smem + s * PL + so, P.arr (nset, K_DENS, s) + go);
-          if (MODE == M_S2) cp_async16 (smem + (A_D + s) * PL + so, P.arr (0, K_DDENS, s) + go);
+          tma_load_3d (smem + s * PL, tm + nset * per_set + s, x, y, z, &tma_bar);
+          if (MODE == M_S2) tma_load_3d (smem + (A_D + s) * PL, tm + 0 * per_set + P.ns + s, x, y, z, &tma_bar);
         }
-        cp_async16 (smem + (A_F + 0) * PL + so, P.arr (fset, K_ER) + go);
-        cp_async16 (smem + (A_F + 1) * PL + so, P.arr (fset, K_EZ) + go);
-        if (!etz) cp_async16 (smem + (A_F + 2) * PL + so, P.arr (fset, K_EABS) + go);
+        tma_load_3d (smem + (A_F + 0) * PL, tm + fset * per_set + 2 * P.ns + 0, x, y, z, &tma_bar);
+        tma_load_3d (smem + (A_F + 1) * PL, tm + fset * per_set + 2 * P.ns + 1, x, y, z, &tma_bar);
+        if (!etz) tma_load_3d (smem + (A_F + 2) * PL, tm + fset * per_set + 2 * P.ns + 3, x, y, z, &tma_bar);
+      }
+    }
+    {
+      if (!A.maps && lane < nchunk) {
+        for (int row = wq; row < nrow; row += WY) {
+          const long long go = (long long) row * P.pitch + 2 * lane;
+          const int so = row * TXP + 2 * lane;
+#pragma unroll
+          for (int s = 0; s < NS; s++) {
+            cp_async16 (smem + s * PL + so, src_n[s] + go);
+            if (MODE == M_S2) cp_async16 (smem + (A_D + s) * PL + so, src_d[s] + go);
+          }
+          cp_async16 (smem + (A_F + 0) * PL + so, src_er + go);
+          cp_async16 (smem + (A_F + 1) * PL + so, src_ez + go);
+          if (!etz) cp_async16 (smem + (A_F + 2) * PL + so, src_ea + go);
+        }
       }
       if (OTF && nt > 1 && c0 == 0) {
         // axis ghosts of a 3-D grid come from the opposite plane (cdr.c:798-824)
@@ -256,53 +376,73 @@ k_stage (const __grid_constant__ Model M, const StageArgs A)
       }
       cp_async_commit ();
       cp_async_wait_all ();
-      __syncthreads ();
+      if (A.maps) {
+        bool ok = mbar_wait (&tma_bar, tma_phase, TMA_WAIT_LIMIT);
+        if (__syncthreads_or (!ok)) {
+          // give the copies in flight a last bounded chance, report, leave
+          if (!ok) mbar_wait (&tma_bar, tma_phase, TMA_WAIT_LIMIT);
+          if (t == 0) atomicOr (&A.st[P.fam].error, 1 << 5);
+          return;
+        }
+        tma_phase ^= 1u;
+      } else {
+        __syncthreads ();
+      }
     }
 
     // ---- stencil values: clamp (cdr_nonegative) and the RK2 intermediate
     // state on the interior, then the ghost cells from the boundary
     // conditions (prepare_grid on the fused forms) ----
     if (OTF) {
-      const int total = nrow * ncol;
-      for (int i = t; i < total; i += NT) {
-        const int row = i / ncol, col = i - row * ncol;
-        const int gr = zb - 2 + row, gc = c0 - 2 + col;
-        if (gr < 0 || gr >= nz || gc < 0 || gc >= nr) continue;
+      const int gr0 = zb - 2, gc0 = c0 - 2;
+      for (int row = wq; row < nrow; row += WY) {
+        const int gr = gr0 + row;
+        const bool rin = gr >= 0 && gr < nz;
+        for (int col = lane; col < ncol; col += 32) {
+          const int gc = gc0 + col;
+          if (!rin || gc < 0 || gc >= nr) continue;
 #pragma unroll
-        for (int s = 0; s < NS; s++) {
-          double v = clamp0 (SA (s, row, col));
-          if (MODE == M_S2) v = v + h * SA (A_D + s, row, col);
-          SA (s, row, col) = v;
-        }
-      }
-      __syncthreads ();
-      for (int i = t; i < total; i += NT) {
-        const int row = i / ncol, col = i - row * ncol;
-        const int gr = zb - 2 + row, gc = c0 - 2 + col;
-        const bool gin = gr >= 0 && gr < nz, cin = gc >= 0 && gc < nr;
-        if (gin == cin) continue;                 // interior, or a corner (never read)
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-          double v;
-          if (gc < 0) {                           // axis
-            if (nt == 1) {
-              v = SA (s, row, col + 2 * (-1 - gc) + 1);      // column -1-gc
-            } else {
-              const int oc = -1 - gc;             // 0 or 1
-              v = clamp0 (opp[(s * ROWS + row) * 2 + oc]);
-              if (MODE == M_S2) v = v + h * opp[((NS + s) * ROWS + row) * 2 + oc];
-            }
-          } else if (gc >= nr) {                  // r = L_r
-            v = (double) M.bnd_sign[1] * SA (s, row, col - 2 * (gc - nr) - 1);
-          } else if (gr < 0) {                    // z = 0
-            v = (double) M.bnd_sign[2] * SA (s, row + 2 * (-1 - gr) + 1, col);
-          } else {                                // z = L_z
-            v = (double) M.bnd_sign[3] * SA (s, row - 2 * (gr - nz) - 1, col);
+          for (int s = 0; s < NS; s++) {
+            double v = clamp0 (SA (s, row, col));
+            if (MODE == M_S2) v = v + h * SA (A_D + s, row, col);
+            SA (s, row, col) = v;
           }
-          SA (s, row, col) = v;
         }
       }
+      const bool edge = (c0 == 0) || (c0 + w.width + 2 > nr) || (zb == 0) || (zb + w.zlen + 2 > nz);
       __syncthreads ();
+      if (edge) {
+        for (int row = wq; row < nrow; row += WY) {
+          const int gr = gr0 + row;
+          const bool rin = gr >= 0 && gr < nz;
+          for (int col = lane; col < ncol; col += 32) {
+            const int gc = gc0 + col;
+            const bool cin = gc >= 0 && gc < nr;
+            if (rin == cin) continue;             // interior, or a corner (never read)
+#pragma unroll
+            for (int s = 0; s < NS; s++) {
+              double v;
+              if (gc < 0) {                       // axis
+                if (nt == 1) {
+                  v = SA (s, row, col + 2 * (-1 - gc) + 1);      // column -1-gc
+                } else {
+                  const int oc = -1 - gc;         // 0 or 1
+                  v = clamp0 (opp[(s * ROWS + row) * 2 + oc]);
+                  if (MODE == M_S2) v = v + h * opp[((NS + s) * ROWS + row) * 2 + oc];
+                }
+              } else if (gc >= nr) {              // r = L_r
+                v = (double) M.bnd_sign[1] * SA (s, row, col - 2 * (gc - nr) - 1);
+              } else if (gr < 0) {                // z = 0
+                v = (double) M.bnd_sign[2] * SA (s, row + 2 * (-1 - gr) + 1, col);
+              } else {                            // z = L_z
+                v = (double) M.bnd_sign[3] * SA (s, row - 2 * (gr - nz) - 1, col);
+              }
+              SA (s, row, col) = v;
+            }
+          }
+        }
+        __syncthreads ();
+      }
     }
 
     // ---- per-species and per-column constants ----
@@ -344,7 +484,7 @@ k_stage (const __grid_constant__ Model M, const StageArgs A)
         if (!active || tr >= w.zlen) continue;
         const long long o = P.off (c, zb + tr, plane);
 #pragma unroll
-        for (int s = 0; s < NS; s++) acc[k][s] = P.arr (A.dset, K_DDENS, s)[o];
+        for (int s = 0; s < NS; s++) acc[k][s] = P.arr (A.dset, K_DDENS, s)[o];   // rare path (narrow seam)
       }
     }
 
@@ -399,19 +539,23 @@ k_stage (const __grid_constant__ Model M, const StageArgs A)
 #pragma unroll
         for (int k = 0; k <= RPW; k++) {
           const int sr = r_first + k + 2;         // face below staged row sr
-          fz[k] = face_z (SA (s, sr - 2, sc), SA (s, sr - 1, sc), SA (s, sr, sc), SA (s, sr + 1, sc),
-                          cm[s] * SA (A_F + 1, sr - 1, sc), ddz[s]);
+          const double vz = cm[s] * SA (A_F + 1, sr - 1, sc);
+          fz[k] = FAST ? face_z_fast (SA (s, sr - 2, sc), SA (s, sr - 1, sc), SA (s, sr, sc), SA (s, sr + 1, sc), vz, ddz[s])
+                       : face_z (SA (s, sr - 2, sc), SA (s, sr - 1, sc), SA (s, sr, sc), SA (s, sr + 1, sc), vz, ddz[s]);
         }
 #pragma unroll
         for (int k = 0; k < RPW; k++) {
           const int sr = r_first + k + 2;
           // radial face at the left of this column (.f90:233-308)
-          const double fl = face_r (SA (s, sr, sc - 2), SA (s, sr, sc - 1), SA (s, sr, sc),
-                                    SA (s, sr, sc + 1), cm[s] * SA (A_F + 0, sr, sc - 1), ddr[s]);
+          const double vl = cm[s] * SA (A_F + 0, sr, sc - 1);
+          const double fl = FAST ? face_r_fast (SA (s, sr, sc - 2), SA (s, sr, sc - 1), SA (s, sr, sc), SA (s, sr, sc + 1), vl, ddr[s])
+                                 : face_r (SA (s, sr, sc - 2), SA (s, sr, sc - 1), SA (s, sr, sc), SA (s, sr, sc + 1), vl, ddr[s]);
           double fr = __shfl_down_sync (0xffffffffu, fl, 1);
-          if (last_lane)
-            fr = face_r (SA (s, sr, sc - 1), SA (s, sr, sc), SA (s, sr, sc + 1), SA (s, sr, sc + 2),
-                         cm[s] * SA (A_F + 0, sr, sc), ddr[s]);
+          if (last_lane) {
+            const double vr = cm[s] * SA (A_F + 0, sr, sc);
+            fr = FAST ? face_r_fast (SA (s, sr, sc - 1), SA (s, sr, sc), SA (s, sr, sc + 1), SA (s, sr, sc + 2), vr, ddr[s])
+                      : face_r (SA (s, sr, sc - 1), SA (s, sr, sc), SA (s, sr, sc + 1), SA (s, sr, sc + 2), vr, ddr[s]);
+          }
           double dv = acc[k][s];
           dv = dv + erm * fl - erp * fr;                         // .f90:113-117
           dv = dv + gdz * (fz[k] - fz[k + 1]);                   // .f90:128-130
@@ -421,27 +565,35 @@ k_stage (const __grid_constant__ Model M, const StageArgs A)
     }
 
     // ---- write ----
+    double *out_p[NS];
+    const double *cen_n[NS];
+    const double *cen_d[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      out_p[s] = (MODE == M_DERIV) ? P.arr (A.dset, K_DDENS, s)
+               : (MODE == M_S1) ? P.arr (0, K_DDENS, s)
+               : P.arr (MODE == M_S2 ? A.dst : 0, K_DENS, s);
+      cen_n[s] = (MODE == M_S2) ? P.arr (A.src, K_DENS, s) : P.arr (0, K_DENS, s);
+      cen_d[s] = P.arr (0, K_DDENS, s);
+    }
+    double *chg_p = (MODE == M_S2 && A.want_charge) ? P.arr (A.dst, K_CHARGE) : nullptr;
+    const double hh = 0.5 * h;
 #pragma unroll
     for (int k = 0; k < RPW; k++) {
       const int tr = r_first + k;
       if (!active || tr >= w.zlen) continue;
-      const int iz = zb + tr;
-      const long long o = P.off (c, iz, plane);
-      if (MODE == M_DERIV) {
+      const long long o = P.off (c, zb + tr, plane);
+      if (MODE == M_DERIV || MODE == M_S1) {
 #pragma unroll
-        for (int s = 0; s < NS; s++) P.arr (A.dset, K_DDENS, s)[o] = acc[k][s];
-      } else if (MODE == M_S1) {
-#pragma unroll
-        for (int s = 0; s < NS; s++) P.arr (0, K_DDENS, s)[o] = acc[k][s];
+        for (int s = 0; s < NS; s++) out_p[s][o] = acc[k][s];
       } else {
         double chg = 0.0;
-        const double hh = 0.5 * h;
 #pragma unroll
         for (int s = 0; s < NS; s++) {
-          const double n0c = (MODE == M_S2) ? clamp0 (P.arr (A.src, K_DENS, s)[o]) : P.arr (0, K_DENS, s)[o];
-          const double d0 = (MODE == M_S2) ? SA (A_D + s, tr + 2, sc) : P.arr (0, K_DDENS, s)[o];
+          const double n0c = (MODE == M_S2) ? clamp0 (cen_n[s][o]) : cen_n[s][o];
+          const double d0 = (MODE == M_S2) ? SA (A_D + s, tr + 2, sc) : cen_d[s][o];
           const double n1 = n0c + hh * d0 + hh * acc[k][s];                // cdr.c:1128-1131
-          P.arr (MODE == M_S2 ? A.dst : 0, K_DENS, s)[o] = n1;
+          out_p[s][o] = n1;
           if (MODE == M_S2) {
             chg += (n1 * M.charge[s]) / nt;                                // cdr.c:380-381
             if (M.mobile[s] && P.level == 0) {
@@ -450,9 +602,10 @@ k_stage (const __grid_constant__ Model M, const StageArgs A)
             }
           }
         }
-        if (MODE == M_S2 && A.want_charge) P.arr (A.dst, K_CHARGE)[o] = chg;
+        if (chg_p) chg_p[o] = chg;
       }
     }
+
     // ---- block max of the mobile densities -> next step's CFL (M_S2) ----
     if (MODE == M_S2 && A.fam_state && P.level == 0) {
       unsigned long long key = seen ? dkey (dmax_local) : 0ULL;

@@ -167,9 +167,18 @@ int arcos_field_post (void *ctx, int set);
 /* 1: launch every kernel once per patch (the plain form the batched
  * persistent launch is compared with); 0: batched (default). */
 int arcos_set_per_patch (void *ctx, int on);
-/* Tile shape of the stencil kernel: 0 = 32x16 cells (128 threads),
- * 1 = 32x32 (128 threads), 2 = 32x32 (256 threads).  Any time. */
+/* Flux-limiter arithmetic.  1: the reference's operations one for one
+ * (results bit-identical to the CPU code).  0 (default): the same Koren
+ * limiter without forming the ratio p = num/dC (no divisions); differs from
+ * the reference only in the last bits of a face flux, far inside the 1e-12
+ * relative per-step agreement. */
+int arcos_set_exact (void *ctx, int on);
+/* Tile shape of the stencil kernel: 0 = 32x16 cells with 128 threads,
+ * 1 = 32x32 cells with 256 threads.  Any time. */
 int arcos_set_tile (void *ctx, int cfg);
+/* 1 (default): stage stencil tiles in shared memory with TMA bulk tensor
+ * copies; 0: with per-thread cp.async.  Same results either way. */
+int arcos_set_tma (void *ctx, int on);
 int arcos_get_tile (void *ctx);
 int arcos_num_items (void *ctx);
 /* Device-timed runs: arcos_run_prepare sets the attempted step, computes the
@@ -180,6 +189,11 @@ int arcos_run_enqueue (void *ctx, int nsteps);
 /* Enqueue one fused stage kernel (1: stage 1, 2: stage 2) reading dens[src]. */
 int arcos_enqueue_stage (void *ctx, int mode, int src);
 int arcos_family_state (void *ctx, int fam, int *steps, double *h, int *error_bits);
+/* Host-side evaluation of the device's reaction-table lookup (no CUDA call):
+ * rates[i] = k(|eabs[i]|) as react_apply computes it (reaction.c:127-142). */
+int arcos_table_rates (double e_min, double e_step, int steps, double underflow,
+                       double overflow, const double *values, const double *eabs,
+                       int n, double *rates);
 
 /* ---- narrow seam (arcos_f90/src/cdr_advect_diffu_wrap.c:25-41) ----------
  * Same signature and argument meaning as the reference wrapper around the

@@ -18,8 +18,8 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
-def device_tree(pb, **kw):
-    t = CdrTree(pb.params, pb.model, pb.specs, **kw)
+def device_tree(pb, exact=True, **kw):
+    t = CdrTree(pb.params, pb.model, pb.specs, exact=exact, **kw)
     for g, per in enumerate(pb.dens):
         for s, a in enumerate(per):
             t.upload(g, "dens", a, s)
@@ -117,7 +117,7 @@ def test_field_in_loop(cuda_device):
     pb = workloads.plain(nr=32, nz=64, ion_mass=0.0, seed=9)
     port = port_tree(pb, field_mode=bind.FIELD_POISSON)
     port.call("port_calc_charge")
-    dev = CdrTree(pb.params, pb.model, pb.specs)
+    dev = CdrTree(pb.params, pb.model, pb.specs, exact=True)
     for s in range(2):
         dev.upload(0, "dens", pb.dens[0][s], s)
     dev.cdr_calc_charge_r(0)
@@ -167,3 +167,34 @@ def test_narrow_seam(cuda_device):
     lib.port_advect_vec(1.0, -1.0, P(dens), P(d_port), P(er), P(ez), 0.1, 1 / 64, 1 / 64,
                         r0, r1, z0, z1)
     assert max_ulp(d_dev, d_port) == 0
+
+
+@pytest.mark.parametrize("ntheta", [1, 4])
+def test_fast_limiter_within_tolerance(cuda_device, ntheta):
+    """The division-free limiter (the default) against the oracle: 1e-12
+    relative per step, the north-star tolerance."""
+    pb = workloads.plain(nr=40, nz=72, ntheta=ntheta, ion_mass=1.0, noise=1e-3, seed=13)
+    port = port_tree(pb)
+    dev = device_tree(pb, exact=False)
+    for _ in range(5):
+        hp = port.rk2(50.0)[0]
+        hd = dev.run(1, 50.0)[0][0]
+        assert abs(hd - hp) <= TOL * hp
+        for s in range(2):
+            a, b = dev.download(0, "dens", s), port.dens(0, s)
+            assert rel_err(a, b) <= TOL, rel_err(a, b)
+            # resynchronise so the check is per step
+            dev.upload(0, "dens", b, s)
+
+
+def test_fast_limiter_long_run(cuda_device):
+    """1000 steps with the division-free limiter stay within 1e-9 of the oracle."""
+    pb = workloads.plain(nr=32, nz=64, ion_mass=1.0, noise=1e-3, seed=17)
+    port = port_tree(pb)
+    dev = device_tree(pb, exact=False)
+    for _ in range(1000):
+        port.rk2(50.0)
+    dev.run(1000, 50.0)
+    for s in range(2):
+        a, b = dev.download(0, "dens", s), port.dens(0, s)
+        assert rel_err(a, b) <= 1e-9, rel_err(a, b)
