@@ -1,0 +1,42 @@
+"""Tile-shape autotuner for the stencil kernel.
+
+The stage kernel works on tiles of 32 columns by WY*RPW rows; which shape is
+fastest depends on the grid sizes (tile count against SM count, halo share)
+and on the number of species.  The tuner times a few device-timed steps with
+each shape on the caller's own problem and keeps the fastest.  Timing runs
+advance the simulation (the state moves on by the tuning steps).
+"""
+from __future__ import annotations
+
+from typing import Dict, Optional
+
+from ._lib import check
+
+N_TILE_SHAPES = 2
+TILE_SHAPES = {0: "32 x 16 cells, 128 threads", 1: "32 x 16 cells, 256 threads (2 rows/warp pair)"}
+
+
+def autotune_tiles(tree, steps: int = 6, h: float = 50.0, stream=None) -> Dict[int, float]:
+    """Times ``steps`` fused RK2 steps (even) per tile shape on ``tree`` (a
+    CdrTree of single-grid families with a fixed field) and selects the
+    fastest.  Returns {shape: ms per step}."""
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream()
+    steps += steps & 1
+    L, h_ = tree.L, tree.h
+    times = {}
+    for cfg in range(N_TILE_SHAPES):
+        tree.set_tile(cfg)
+        check(L.arcos_run_prepare(h_, h))
+        check(L.arcos_run_enqueue(h_, 2))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        check(L.arcos_run_enqueue(h_, steps))
+        e1.record(s)
+        e1.synchronize()
+        times[cfg] = e0.elapsed_time(e1) / steps
+    best = min(times, key=times.get)
+    tree.set_tile(best)
+    return times

@@ -77,7 +77,8 @@ struct Ctx {
   int n_items = 0;
   std::vector<int> item_off, item_cnt;
   int tile_cfg = 1;                   // index into TILE_WY / TILE_RPW
-  int occ[2][4][N_TILE_CFG_MAX] = {};
+  int occ[2][2][4][N_TILE_CFG_MAX] = {};
+  int stage_eabs = 0;                 // some set holds a non-zero E_theta
   int exact = 0;                      // 1: bit-exact flux limiter, 0: division-free form
   int use_tma = 1;                    // stage tiles with bulk tensor copies (else cp.async)
   CUtensorMap *maps_d = nullptr;      // [patch][set][array]
@@ -100,6 +101,7 @@ struct Ctx {
   int max_level = 0;
   bool fused_ok = false;              // every family is one root grid with all sides external
   cudaGraphExec_t graph2 = nullptr;   // two fused steps
+  cudaGraphExec_t graph_tree = nullptr;   // one step of a tree (batched launches)
   int graph_items = -1;
 };
 
@@ -181,7 +183,7 @@ grid_blocks (long long work, int threads, int cap = 4096)
   return (int) b;
 }
 
-constexpr int NODES_SMEM_MAX = 24 * 1024 / (int) sizeof (TableNode);
+constexpr int NODES_SMEM_MAX = 4 * 1024 / (int) sizeof (TableNode);
 
 // Tile shapes the autotuner chooses from: (warps per block, rows per thread);
 // tiles are 32 columns wide and WY * RPW rows high.
@@ -191,9 +193,10 @@ constexpr int TILE_RPW[N_TILE_CFG] = {4, 4};
 
 template <int NS, int MODE, int WY, int RPW>
 size_t
-stage_smem_t (int n_nodes)
+stage_smem_t (int n_nodes, int stage_eabs)
 {
-  size_t b = sizeof (double) * (size_t) TileLayout<NS, MODE, WY, RPW>::DOUBLES;
+  using LY = TileLayout<NS, MODE, WY, RPW>;
+  size_t b = sizeof (double) * (size_t) ((stage_eabs ? LY::NA : LY::NA - 1) * LY::PLANE + LY::OPP);
   if (n_nodes > 0 && n_nodes <= NODES_SMEM_MAX) b += sizeof (TableNode) * (size_t) n_nodes;
   return b;
 }
@@ -202,7 +205,7 @@ template <int NS, int MODE, int WY, int RPW, bool FAST>
 cudaError_t
 launch_stage_t (const Model &M, const StageArgs &A, int blocks, cudaStream_t s, int *occ)
 {
-  const size_t sm = stage_smem_t<NS, MODE, WY, RPW> (A.n_nodes);
+  const size_t sm = stage_smem_t<NS, MODE, WY, RPW> (A.n_nodes, A.stage_eabs);
   cudaFuncSetAttribute (k_stage<NS, MODE, WY, RPW, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
   if (occ) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor (occ, k_stage<NS, MODE, WY, RPW, FAST>, 32 * WY, sm);
@@ -256,10 +259,11 @@ launch_stage (int mode, int ns, int cfg, const Model &M, const StageArgs &A, int
 int
 stage_blocks (Ctx *c, int mode, int n_items)
 {
-  int &o = c->occ[c->exact][mode][c->tile_cfg];
+  int &o = c->occ[c->stage_eabs][c->exact][mode][c->tile_cfg];
   if (o == 0) {
     StageArgs A{};
     A.exact = c->exact;
+    A.stage_eabs = c->stage_eabs;
     A.n_nodes = (int) c->nodes_h.size ();
     int b = 0;
     launch_stage (mode, c->M.ns, c->tile_cfg, c->M, A, 0, 0, &b);
@@ -284,6 +288,7 @@ base_args (Ctx *c)
   A.n_nodes = (int) c->nodes_h.size ();
   A.nodes_smem = A.n_nodes > 0 && A.n_nodes <= NODES_SMEM_MAX;
   A.exact = c->exact;
+  A.stage_eabs = c->stage_eabs;
   A.maps = (c->use_tma && c->maps_d) ? c->maps_d : nullptr;
   A.maps_per_patch = c->maps_per_patch;
   return A;
@@ -450,6 +455,25 @@ do_charge (Ctx *c, int set)
   });
 }
 
+// Does any patch need the staged |E| (E_theta not identically zero)?  The
+// stage kernels size their shared memory from this.
+int
+refresh_stage_eabs (Ctx *c)
+{
+  const int np = (int) c->pd_h.size ();
+  std::vector<int> h (np * 2);
+  CK (cudaMemcpyAsync (h.data (), c->etz_d, sizeof (int) * np * 2, cudaMemcpyDeviceToHost, c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  int any = 0;
+  for (int v : h) any |= v != 0;
+  if (any != c->stage_eabs) {
+    c->stage_eabs = any;
+    if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
+  }
+  return ARCOS_OK;
+}
+
 // The on-device part of cdr_calc_field_r after the field solve: external
 // field, |E| (+ the root's field maxima) and theta periodicity.
 int
@@ -483,7 +507,8 @@ do_field_post (Ctx *c, int set)
     k_eabs<<<g, 256, 0, c->stream>>> (c->pd_d, pl, set, c->st_d);
   });
   if (r) return r;
-  return do_periodic (c, set, 2);
+  if ((r = do_periodic (c, set, 2))) return r;
+  return refresh_stage_eabs (c);
 }
 
 int
@@ -588,7 +613,8 @@ rk2_general (Ctx *c)
 {
   int r;
   StageArgs A = base_args (c);
-  if ((r = reset_dmax (c, 0))) return r;
+  k_reset_dmax<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->st_d, c->nfam, 0);
+  CKL ();
   if ((r = do_nonneg (c, 0))) return r;                 // cdr.c:1276
   if ((r = do_prepare (c, 0))) return r;                // cdr.c:1279
   if (c->fn && (r = field_from_callback (c, 0, 0))) return r;   // cdr.c:1283
@@ -690,6 +716,7 @@ arcos_destroy (void *ctx)
   Ctx *c = (Ctx *) ctx;
   if (!c) return ARCOS_OK;
   if (c->graph2) cudaGraphExecDestroy (c->graph2);
+  if (c->graph_tree) cudaGraphExecDestroy (c->graph_tree);
   cudaFree (c->pool); cudaFree (c->pd_d); cudaFree (c->nodes_d); cudaFree (c->st_d);
   cudaFree (c->dtlog_d); cudaFree (c->etz_d); cudaFree (c->done_d); cudaFree (c->items_d);
   cudaFree (c->plist_d); cudaFree (c->kids_d); cudaFree (c->strips_d); cudaFree (c->ext_d);
@@ -708,6 +735,7 @@ arcos_set_stream (void *ctx, void *stream)
   if (!c) return fail (ARCOS_ERR_ARG, "null context");
   c->stream = stream ? (cudaStream_t) stream : c->own_stream;
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
   return ARCOS_OK;
 }
 
@@ -749,6 +777,13 @@ arcos_add_reaction (void *ctx, int nin, const int *inputs, int nout, const int *
     }
   }
   M.r_nops[r] = nop;
+  for (int s = 0; s < 8; s++) { M.r_coef[r][s] = 0; M.r_in_count[r][s] = 0; }
+  for (int i = 0; i < nin; i++) {
+    M.r_in_count[r][inputs[i]]++;
+    if (M.charge[inputs[i]] != 0.0) M.r_coef[r][inputs[i]] -= 1;
+  }
+  for (int i = 0; i < nout; i++)
+    if (M.charge[outputs[i]] != 0.0) M.r_coef[r][outputs[i]] += 1;
   build_nodes (e_min, e_step, steps, values, c->nodes_h);
   return ARCOS_OK;
 }
@@ -952,6 +987,7 @@ build_items (Ctx *c)
   CK (cudaMalloc (&c->items_d, sizeof (WorkItem) * items.size ()));
   CK (cudaMemcpy (c->items_d, items.data (), sizeof (WorkItem) * items.size (), cudaMemcpyHostToDevice));
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
   return build_maps (c, ty);
 }
 
@@ -1309,9 +1345,11 @@ arcos_cdr_add_ext_field_r (void *ctx, int set)
   for (auto &P : c->pd_h) w = std::max (w, P.asz);
   const double *er = c->ext_d, *et = c->ext_d + c->nfam * ARCOS_MAXPLANES,
                *ez = c->ext_d + 2 * c->nfam * ARCOS_MAXPLANES;
-  return for_patches (c, w, [&] (dim3 g, const int *pl) {
+  r = for_patches (c, w, [&] (dim3 g, const int *pl) {
     k_add_ext<<<g, 256, 0, c->stream>>> (c->pd_d, pl, set, er, et, ez, c->etz_d);
   });
+  if (r) return r;
+  return refresh_stage_eabs (c);
 }
 
 int
@@ -1453,7 +1491,20 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
   if ((r = read_states (c, st0))) return r;
   const int step0 = st0[0].step;
   if ((r = set_h_attempt (c, h))) return r;
-  if (!c->fused_ok) {
+  if (!c->fused_ok && !c->fn && !c->per_patch && nsteps > 0) {
+    // trees: one step (all its batched launches) captured once, replayed
+    if (!c->graph_tree) {
+      cudaGraph_t gr;
+      CK (cudaStreamBeginCapture (c->stream, cudaStreamCaptureModeThreadLocal));
+      int e = rk2_general (c);
+      cudaError_t ee = cudaStreamEndCapture (c->stream, &gr);
+      if (e) return e;
+      if (ee != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("graph capture: ") + cudaGetErrorString (ee));
+      CK (cudaGraphInstantiate (&c->graph_tree, gr, 0));
+      cudaGraphDestroy (gr);
+    }
+    for (int k = 0; k < nsteps; k++) CK (cudaGraphLaunch (c->graph_tree, c->stream));
+  } else if (!c->fused_ok) {
     for (int k = 0; k < nsteps; k++)
       if ((r = rk2_general (c))) return r;
   } else if (c->fn) {
@@ -1616,6 +1667,7 @@ arcos_set_exact (void *ctx, int on)
   if (!c) return fail (ARCOS_ERR_ARG, "null context");
   c->exact = on ? 1 : 0;
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
   return ARCOS_OK;
 }
 
@@ -1640,6 +1692,7 @@ arcos_set_tma (void *ctx, int on)
   if (!c) return fail (ARCOS_ERR_ARG, "null context");
   c->use_tma = on ? 1 : 0;
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
   if (c->committed) return build_maps (c, TILE_WY[c->tile_cfg] * TILE_RPW[c->tile_cfg]);
   return ARCOS_OK;
 }

@@ -439,6 +439,14 @@ k_cfl (const Model M, DevState *st, int nfam, int eset)
   cfl_step (s, M, k & 1, eset, k);
 }
 
+// Resets the max-density slot (step + slot_rel) of every family.
+__global__ void
+k_reset_dmax (DevState *st, int nfam, int slot_rel)
+{
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < nfam) st[f].dmax_key[(st[f].step + slot_rel) & 1] = dkey (-1.0);
+}
+
 // Ends a step of every family whose stage-2 kernel did not fold the CFL.
 __global__ void
 k_step_end (DevState *st, int nfam)

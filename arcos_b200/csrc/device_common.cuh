@@ -78,6 +78,10 @@ struct Model {
   // accumulation program of each reaction: the d_dens updates of react_apply
   // (reaction.c:147-155) in order, species with zero charge dropped
   int r_nops[ARCOS_MAXR];
+  // the same folded per species (fast form): net count of +rate updates and
+  // the number of times each species is an input
+  signed char r_coef[ARCOS_MAXR][8];
+  signed char r_in_count[ARCOS_MAXR][8];
   signed char r_op_sp[ARCOS_MAXR][ARCOS_MAXIN + ARCOS_MAXOUT];
   signed char r_op_neg[ARCOS_MAXR][ARCOS_MAXIN + ARCOS_MAXOUT];
   int r_node_off[ARCOS_MAXR];     // first node of the reaction in the node array

@@ -50,6 +50,7 @@ struct StageArgs {
   int n_nodes;          // reaction-table nodes
   int nodes_smem;       // copy the nodes to shared memory
   int exact;            // bit-exact flux limiter (host-side dispatch)
+  int stage_eabs;       // some patch has E_theta != 0: stage |E| (else recomputed from er, ez)
   const CUtensorMap *maps;   // TMA descriptors [patch][set][array], or null (cp.async staging)
   int maps_per_patch;
 };
@@ -141,21 +142,34 @@ face_z_fast (double nLL, double nL, double nR, double nRR, double v, double dd)
 // the table position the reference derives from log10/floor is recovered by
 // comparing |E| with exact per-node thresholds (precomputed on the host with
 // the same log10), starting from a single-precision estimate.
+__device__ __noinline__ int
+table_pos_slow (const TableNode *__restrict__ nd, int steps, double eabs, int k)
+{
+  while (k > 0 && eabs < nd[k].thr) k--;
+  while (k < steps && eabs >= nd[k + 1].thr) k++;
+  return k;
+}
+
 __device__ __forceinline__ double
 table_rate (const Model &M, const TableNode *__restrict__ nodes, int r, double eabs)
 {
   const TableNode *nd = nodes + M.r_node_off[r];
   const int steps = M.r_steps[r];
-  if (!(eabs >= nd[0].thr)) return M.r_under[r];        // log_e < e_min (or NaN)
-  if (eabs >= nd[steps + 1].thr) return M.r_over[r];     // log_e > e_min + e_step*steps
+  // single-precision estimate of the position, then one exact correction each
+  // way (the estimate is never off by more than one node for tables with
+  // e_step above ~1e-4); anything else takes the exact search
   const float lf = __log10f ((float) eabs);
   const float pf = (lf - (float) M.r_e_min[r]) * M.r_inv_step_f[r];
-  int k = (pf > 0.f) ? (int) pf : 0;
-  if (!(pf < (float) steps)) k = steps;
-  while (k > 0 && eabs < nd[k].thr) k--;
-  while (k < steps && eabs >= nd[k + 1].thr) k++;
+  int k = (int) fminf (fmaxf (pf, 0.f), (float) steps);
+  k -= (k > 0 && eabs < nd[k].thr) ? 1 : 0;
+  k += (k < steps && eabs >= nd[k + 1].thr) ? 1 : 0;
+  if ((k > 0 && eabs < nd[k].thr) || (k < steps && eabs >= nd[k + 1].thr))
+    k = table_pos_slow (nd, steps, eabs, k);
   const TableNode n = nd[k];
-  return n.val + n.slope * (eabs - n.e1);
+  double rate = n.val + n.slope * (eabs - n.e1);
+  rate = (eabs >= nd[steps + 1].thr) ? M.r_over[r] : rate;   // log_e > e_min + e_step*steps
+  rate = (eabs >= nd[0].thr) ? rate : M.r_under[r];          // log_e < e_min (or NaN)
+  return rate;
 }
 
 // CFL time step of cdr_courant (cdr.c:971-1061) and the step limit of cdr_rk2
@@ -282,14 +296,15 @@ k_stage (const __grid_constant__ Model M, const StageArgs A)
   extern __shared__ __align__ (128) double smem[];
   __shared__ __align__ (8) unsigned long long tma_bar;
   unsigned tma_phase = 0;
-  double *opp = smem + NA * PL;
+  const int na_rt = A.stage_eabs ? NA : NA - 1;     // |E| staged only when E_theta != 0 somewhere
+  double *opp = smem + na_rt * PL;
   const TableNode *nodes = A.nodes;
   __shared__ unsigned long long red_key[WY];
   const int t = threadIdx.x, lane = t & 31, wq = t >> 5;
 
   if (A.maps && t == 0) mbar_init (&tma_bar, 1);
   if (A.nodes_smem) {
-    TableNode *sn = reinterpret_cast<TableNode *> (smem + LY::DOUBLES);
+    TableNode *sn = reinterpret_cast<TableNode *> (smem + na_rt * PL + LY::OPP);
     for (int i = t; i < A.n_nodes; i += NT) sn[i] = A.nodes[i];
     nodes = sn;
   }
@@ -471,60 +486,80 @@ k_stage (const __grid_constant__ Model M, const StageArgs A)
     const bool last_lane = lane == w.width - 1 || lane == 31;
 
     // ---- fluxes, reactions and the update of this thread's RPW cells ----
+    // Every thread computes all its RPW rows (rows past the tile end are
+    // computed from staged padding and not written), so the loops below have
+    // no per-row branches.
     double acc[RPW][NS];
+    const double *sbase = smem + (r_first + 2) * TXP + sc;     // staged (first row, own column)
+#define SV(a_, k_, dr_, dc_) sbase[(a_) * PL + ((k_) + (dr_)) * TXP + (dc_)]
 #pragma unroll
     for (int k = 0; k < RPW; k++)
 #pragma unroll
       for (int s = 0; s < NS; s++) acc[k][s] = 0.0;
     if (MODE == M_DERIV && A.accumulate) {
-      // the Fortran kernel adds to the d_dens it is given (.f90:113-130)
+      // the Fortran kernel adds to the d_dens it is given (.f90:113-130); rare path (narrow seam)
 #pragma unroll
       for (int k = 0; k < RPW; k++) {
         const int tr = r_first + k;
         if (!active || tr >= w.zlen) continue;
         const long long o = P.off (c, zb + tr, plane);
 #pragma unroll
-        for (int s = 0; s < NS; s++) acc[k][s] = P.arr (A.dset, K_DDENS, s)[o];   // rare path (narrow seam)
+        for (int s = 0; s < NS; s++) acc[k][s] = P.arr (A.dset, K_DDENS, s)[o];
       }
     }
 
     // reactions (react_apply, reaction.c:110-156), in list order
     if (M.nreact > 0 && !(MODE == M_DERIV && A.accumulate)) {
+      const double zc0 = ((double) (P.z0 + zb + r_first) + 0.5) * P.dz;
+      const bool all_below = ((double) (P.z0 + zb + r_first + RPW - 1) + 0.5) * P.dz < M.z_cutoff;
 #pragma unroll
       for (int k = 0; k < RPW; k++) {
-        const int tr = r_first + k;               // tile row (0-based, interior)
-        const int sr = tr + 2;
-        if (tr >= w.zlen) continue;
-        const double zc = ((double) (P.z0 + zb + tr) + 0.5) * P.dz;
-        if (!(zc < M.z_cutoff)) continue;
         double eabs;
         if (etz) {
-          const double e_r = 0.5 * (SA (A_F + 0, sr, sc) + SA (A_F + 0, sr, sc - 1));  // cdr.c:681-682
-          const double e_z = 0.5 * (SA (A_F + 1, sr, sc) + SA (A_F + 1, sr - 1, sc));  // cdr.c:683-684
-          eabs = sqrt (e_r * e_r + e_z * e_z + 0.0 * 0.0);                           // cdr.c:691-692
+          const double e_r = 0.5 * (SV (A_F + 0, k, 0, 0) + SV (A_F + 0, k, 0, -1));   // cdr.c:681-682
+          const double e_z = 0.5 * (SV (A_F + 1, k, 0, 0) + SV (A_F + 1, k, -1, 0));   // cdr.c:683-684
+          eabs = sqrt (e_r * e_r + e_z * e_z + 0.0 * 0.0);                            // cdr.c:691-692
         } else {
-          eabs = SA (A_F + 2, sr, sc);
+          eabs = SV (A_F + 2, k, 0, 0);
         }
         eabs = fabs (eabs);
         double cen[NS];
 #pragma unroll
-        for (int s = 0; s < NS; s++) cen[s] = SA (s, sr, sc);
+        for (int s = 0; s < NS; s++) cen[s] = SV (s, k, 0, 0);
+        const bool on = all_below || (((double) (P.z0 + zb + r_first + k) + 0.5) * P.dz < M.z_cutoff);
+        (void) zc0;
         for (int r = 0; r < M.nreact; r++) {
           double rate = table_rate (M, nodes, r, eabs);
-          const int nin = M.r_nin[r];
-          for (int i = 0; i < nin; i++) {
-            const int sp = M.r_in[r][i];
-            double inv = 0.0;
+          if (FAST) {
+            // inputs in species order, net coefficient per species
 #pragma unroll
-            for (int s = 0; s < NS; s++) if (s == sp) inv = fabs (cen[s]);
-            rate *= (0 > inv ? 0 : inv);
-          }
-          const int nop = M.r_nops[r];
-          for (int i = 0; i < nop; i++) {
-            const int sp = M.r_op_sp[r][i];
-            const double rm = M.r_op_neg[r][i] ? -rate : rate;
+            for (int s = 0; s < NS; s++) {
+              const int cnt = M.r_in_count[r][s];
+              const double a = fabs (cen[s]);
+              if (cnt > 0) rate *= (0 > a ? 0 : a);
+              if (cnt > 1) rate *= (0 > a ? 0 : a);
+            }
 #pragma unroll
-            for (int s = 0; s < NS; s++) if (s == sp) acc[k][s] += rm;
+            for (int s = 0; s < NS; s++) {
+              const double cf = (double) M.r_coef[r][s];
+              if (cf != 0.0 && on) acc[k][s] = __fma_rn (cf, rate, acc[k][s]);
+            }
+          } else {
+            const int nin = M.r_nin[r];
+            for (int i = 0; i < nin; i++) {
+              const int sp = M.r_in[r][i];
+              double inv = 0.0;
+#pragma unroll
+              for (int s = 0; s < NS; s++) if (s == sp) inv = fabs (cen[s]);
+              rate *= (0 > inv ? 0 : inv);
+            }
+            const int nop = M.r_nops[r];
+            for (int i = 0; i < nop; i++) {
+              const int sp = M.r_op_sp[r][i];
+              const double rm = M.r_op_neg[r][i] ? -rate : rate;
+#pragma unroll
+              for (int s = 0; s < NS; s++) if (s == sp && on) acc[k][s] += rm;
+            }
           }
         }
       }
@@ -538,23 +573,22 @@ k_stage (const __grid_constant__ Model M, const StageArgs A)
         double fz[RPW + 1];
 #pragma unroll
         for (int k = 0; k <= RPW; k++) {
-          const int sr = r_first + k + 2;         // face below staged row sr
-          const double vz = cm[s] * SA (A_F + 1, sr - 1, sc);
-          fz[k] = FAST ? face_z_fast (SA (s, sr - 2, sc), SA (s, sr - 1, sc), SA (s, sr, sc), SA (s, sr + 1, sc), vz, ddz[s])
-                       : face_z (SA (s, sr - 2, sc), SA (s, sr - 1, sc), SA (s, sr, sc), SA (s, sr + 1, sc), vz, ddz[s]);
+          const double vz = cm[s] * SV (A_F + 1, k, -1, 0);
+          fz[k] = FAST ? face_z_fast (SV (s, k, -2, 0), SV (s, k, -1, 0), SV (s, k, 0, 0), SV (s, k, 1, 0), vz, ddz[s])
+                       : face_z (SV (s, k, -2, 0), SV (s, k, -1, 0), SV (s, k, 0, 0), SV (s, k, 1, 0), vz, ddz[s]);
         }
 #pragma unroll
         for (int k = 0; k < RPW; k++) {
-          const int sr = r_first + k + 2;
-          // radial face at the left of this column (.f90:233-308)
-          const double vl = cm[s] * SA (A_F + 0, sr, sc - 1);
-          const double fl = FAST ? face_r_fast (SA (s, sr, sc - 2), SA (s, sr, sc - 1), SA (s, sr, sc), SA (s, sr, sc + 1), vl, ddr[s])
-                                 : face_r (SA (s, sr, sc - 2), SA (s, sr, sc - 1), SA (s, sr, sc), SA (s, sr, sc + 1), vl, ddr[s]);
+          // radial face at the left of this column (.f90:233-308); the right
+          // one is the neighbour lane's left face
+          const double vl = cm[s] * SV (A_F + 0, k, 0, -1);
+          const double fl = FAST ? face_r_fast (SV (s, k, 0, -2), SV (s, k, 0, -1), SV (s, k, 0, 0), SV (s, k, 0, 1), vl, ddr[s])
+                                 : face_r (SV (s, k, 0, -2), SV (s, k, 0, -1), SV (s, k, 0, 0), SV (s, k, 0, 1), vl, ddr[s]);
           double fr = __shfl_down_sync (0xffffffffu, fl, 1);
           if (last_lane) {
-            const double vr = cm[s] * SA (A_F + 0, sr, sc);
-            fr = FAST ? face_r_fast (SA (s, sr, sc - 1), SA (s, sr, sc), SA (s, sr, sc + 1), SA (s, sr, sc + 2), vr, ddr[s])
-                      : face_r (SA (s, sr, sc - 1), SA (s, sr, sc), SA (s, sr, sc + 1), SA (s, sr, sc + 2), vr, ddr[s]);
+            const double vr = cm[s] * SV (A_F + 0, k, 0, 0);
+            fr = FAST ? face_r_fast (SV (s, k, 0, -1), SV (s, k, 0, 0), SV (s, k, 0, 1), SV (s, k, 0, 2), vr, ddr[s])
+                      : face_r (SV (s, k, 0, -1), SV (s, k, 0, 0), SV (s, k, 0, 1), SV (s, k, 0, 2), vr, ddr[s]);
           }
           double dv = acc[k][s];
           dv = dv + erm * fl - erp * fr;                         // .f90:113-117
@@ -563,6 +597,7 @@ k_stage (const __grid_constant__ Model M, const StageArgs A)
         }
       }
     }
+#undef SV
 
     // ---- write ----
     double *out_p[NS];

@@ -87,7 +87,7 @@ def plain(nr: int = 128, nz: int = 256, ntheta: int = 1, L_r: float = 2.0, L_z: 
     return Problem(params, model, [spec], dens, [uniform_field(spec)])
 
 
-def amr(n_patches: int = 320, levels: int = 4, root_nr: int = 256, root_nz: int = 512,
+def amr(n_patches: int = 320, levels: int = 4, root_nr: int = 512, root_nz: int = 1024,
         side_lo: int = 16, side_hi: int = 256, seed: int = 0, ion_mass: float = 1.0,
         ntheta: int = 1) -> Problem:
     """A refinement tree of ``n_patches`` patches on ``levels`` levels (ratio
@@ -120,11 +120,13 @@ def amr(n_patches: int = 320, levels: int = 4, root_nr: int = 256, root_nz: int 
         k = rem if i == len(weights) - 1 else int(round(target * w / sum(weights)))
         per_level.append(k)
         rem -= k
-    attempts = 0
+    carry = 0
     for l, want in zip(range(1, levels), per_level):
+        want += carry
         parents = [i for i, s in enumerate(specs) if s.level == l - 1]
         made = 0
-        while made < want and attempts < 200000:
+        attempts = 0
+        while made < want and attempts < 20000 * max(1, want):
             attempts += 1
             # prefer parents near the head
             pi = parents[int(rng.integers(len(parents)))]
@@ -159,6 +161,7 @@ def amr(n_patches: int = 320, levels: int = 4, root_nr: int = 256, root_nz: int 
             specs.append(child)
             lst.append(rect)
             made += 1
+        carry = want - made
     dens = []
     for sp in specs:
         per = []

@@ -219,11 +219,13 @@ def run_device(args):
 
     pb = workloads.plain(nr=NR, nz=NZ, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=rank)
     stream = torch.cuda.Stream()
-    tree = CdrTree(pb.params, pb.model, pb.specs, stream=stream.cuda_stream)
+    tree = CdrTree(pb.params, pb.model, pb.specs, stream=stream.cuda_stream, exact=args.exact)
     for s in range(NS):
         tree.upload(0, "dens", pb.dens[0][s], s)
     tree.set_fixed_field(pb.fields)
     L, h = tree.L, tree.h
+    from arcos_b200.autotune import autotune_tiles
+    tune = autotune_tiles(tree, steps=6, stream=stream)
     warm = max(4, args.warmup + (args.warmup & 1))
     steps = args.steps + (args.steps & 1)
     check(L.arcos_run_prepare(h, 50.0))
@@ -341,6 +343,8 @@ def run_device(args):
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 2 * steps, "clocks": clocks,
                 "stage_kernel_ms": {"stage1": s1, "stage2": s2},
+                "tile_autotune_ms_per_step": {str(k): v for k, v in tune.items()},
+                "limiter": "bit-exact" if args.exact else "division-free (1e-12/step)",
                 "dt_last": hlast}
         print(json.dumps(line), flush=True)
     tree.close()
@@ -356,6 +360,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--exact", action="store_true", help="bit-exact flux limiter")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
