@@ -13,6 +13,8 @@
 #include "../../include/arcos_cdr.h"
 #include "device_common.cuh"
 #include "stage_kernel.cuh"
+#include "fused_kernel.cuh"
+#include "adjoint_kernel.cuh"
 #include "aux_kernels.cuh"
 
 using namespace arcos;
@@ -103,6 +105,23 @@ struct Ctx {
   cudaGraphExec_t graph2 = nullptr;   // two fused steps
   cudaGraphExec_t graph_tree = nullptr;   // one step of a tree (batched launches)
   int graph_items = -1;
+  double *colfac_d = nullptr;         // fused kernels: per column ir/((ir+1/2)dr), (ir+1)/((ir+1/2)dr)
+  TableNode *lean_nodes_d = nullptr;  // fused kernels: nodes with under/overflow sentinels
+  bool lean_tables = false;           // every table's position estimate is within one node
+  // discrete adjoint (adjoint_kernel.cuh): per patch a block of work arrays
+  // [lam 0 | lam 1 | lam* | segment n0 (ck) | segment n* (ck) | checkpoints | final], ns each
+  double *adj_pool = nullptr;
+  int adj_nsteps = 0, adj_ck = 0, adj_nseg = 0;
+  std::vector<double> adj_hs;         // [fam][nsteps]
+  double *adj_hs_d = nullptr;
+  double *adj_gtab_d = nullptr;       // [nodes + 2 per reaction]
+  double *adj_gpart_d = nullptr;      // [vjp blocks][ns + 1]
+  double *adj_invde_d = nullptr;
+  AdjTile *adj_tiles_d = nullptr;
+  int adj_ntiles = 0, adj_blocks = 0;
+  int adj_lam = 0;                    // lam buffer holding the current cotangent
+  bool adj_fwd = false;
+  int occ_fused[2][2][N_TILE_CFG_MAX] = {};   // [stage_eabs][stage 2][tile]
 };
 
 // ---- reaction-table thresholds ----------------------------------------------
@@ -256,6 +275,46 @@ launch_stage (int mode, int ns, int cfg, const Model &M, const StageArgs &A, int
   }
 }
 
+// ---- lean fused kernels (fast limiter, single-grid families) ----
+template <int NS, bool S2, int WY, int RPW>
+cudaError_t
+launch_fused_t (const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
+{
+  const size_t sm = sizeof (double) * 2 * fused_buffer_doubles<NS, WY, RPW> (A.stage_eabs);
+  cudaFuncSetAttribute (k_fused<NS, S2, WY, RPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+  if (occ) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor (occ, k_fused<NS, S2, WY, RPW>, 32 * WY, sm);
+    return cudaGetLastError ();
+  }
+  k_fused<NS, S2, WY, RPW><<<blocks, 32 * WY, sm, s>>> (M, A);
+  return cudaGetLastError ();
+}
+
+template <int NS, bool S2>
+cudaError_t
+launch_fused_c (int cfg, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
+{
+  switch (cfg) {
+  case 0: return launch_fused_t<NS, S2, 4, 4> (M, A, blocks, s, occ);
+  default: return launch_fused_t<NS, S2, 8, 4> (M, A, blocks, s, occ);
+  }
+}
+
+template <bool S2>
+cudaError_t
+launch_fused_m (int ns, int cfg, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
+{
+  switch (ns) {
+  case 1: return launch_fused_c<1, S2> (cfg, M, A, blocks, s, occ);
+  case 2: return launch_fused_c<2, S2> (cfg, M, A, blocks, s, occ);
+  case 3: return launch_fused_c<3, S2> (cfg, M, A, blocks, s, occ);
+  case 4: return launch_fused_c<4, S2> (cfg, M, A, blocks, s, occ);
+  case 5: return launch_fused_c<5, S2> (cfg, M, A, blocks, s, occ);
+  case 6: return launch_fused_c<6, S2> (cfg, M, A, blocks, s, occ);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
 int
 stage_blocks (Ctx *c, int mode, int n_items)
 {
@@ -292,6 +351,107 @@ base_args (Ctx *c)
   A.maps = (c->use_tma && c->maps_d) ? c->maps_d : nullptr;
   A.maps_per_patch = c->maps_per_patch;
   return A;
+}
+
+// Node arrays of the fused kernels: per reaction an underflow sentinel, the
+// nodes 0..steps and the overflow node turned into a sentinel (slope 0), so
+// the lookup needs no under/overflow selects.
+int
+upload_lean_nodes (Ctx *c)
+{
+  const Model &M = c->M;
+  std::vector<TableNode> ln;
+  c->lean_tables = true;
+  for (int r = 0; r < M.nreact; r++) {
+    TableNode u{};
+    u.val = M.r_under[r]; u.e1 = 0.0; u.slope = 0.0; u.thr = -1.0;
+    ln.push_back (u);
+    const int n0 = M.r_node_off[r], steps = M.r_steps[r];
+    for (int k = 0; k <= steps; k++) ln.push_back (c->nodes_h[n0 + k]);
+    TableNode o = c->nodes_h[n0 + steps + 1];
+    o.val = M.r_over[r]; o.e1 = 0.0; o.slope = 0.0;
+    ln.push_back (o);
+    // the single-precision position estimate is within one node for e_step >= 1e-3
+    if (!(M.r_e_step[r] >= 1e-3) || fabs (M.r_e_min[r]) > 30.0) c->lean_tables = false;
+  }
+  if (ln.empty ()) ln.push_back (TableNode{});
+  if (c->lean_nodes_d) cudaFree (c->lean_nodes_d);
+  CK (cudaMalloc (&c->lean_nodes_d, sizeof (TableNode) * ln.size ()));
+  CK (cudaMemcpy (c->lean_nodes_d, ln.data (), sizeof (TableNode) * ln.size (), cudaMemcpyHostToDevice));
+  return ARCOS_OK;
+}
+
+// The lean fused kernels apply: fast limiter, fixed field, TMA staging,
+// single-grid families, one launch over all of them.
+bool
+lean_ok (Ctx *c)
+{
+  return c->fused_ok && c->lean_tables && !c->exact && c->use_tma && c->maps_d && c->colfac_d
+         && c->lean_nodes_d && !c->fn && !c->per_patch;
+}
+
+FusedArgs
+fused_args (Ctx *c)
+{
+  FusedArgs A{};
+  A.patches = c->pd_d;
+  A.items = c->items_d;
+  A.n_items = c->n_items;
+  A.nodes = c->lean_nodes_d;
+  A.n_nodes = (int) c->nodes_h.size () + c->M.nreact;
+  A.st = c->st_d;
+  A.nfam = c->nfam;
+  A.etz = c->etz_d;
+  A.done = c->done_d;
+  A.stage_eabs = c->stage_eabs;
+  A.maps = c->maps_d;
+  A.maps_per_patch = c->maps_per_patch;
+  A.colfac = c->colfac_d;
+  // reaction program: node 0 of reaction r sits after r + 1 sentinels
+  const Model &M = c->M;
+  A.nreact = M.nreact;
+  for (int r = 0; r < M.nreact; r++) {
+    A.r_node0[r] = M.r_node_off[r] + r + 1;
+    A.r_steps[r] = M.r_steps[r];
+    A.r_emin_f[r] = (float) M.r_e_min[r];
+    A.r_inv_f[r] = M.r_inv_step_f[r];
+    A.r_nin[r] = M.r_nin[r];
+    for (int i = 0; i < M.r_nin[r]; i++) A.r_in[r][i] = (signed char) M.r_in[r][i];
+    for (int sp = 0; sp < M.ns && sp < FUSED_MAXS; sp++) A.r_coef[r][sp] = (double) M.r_coef[r][sp];
+  }
+  const double dr = c->dr[0], dz = c->dz[0];
+  for (int s = 0; s < c->M.ns; s++) {
+    const double mass = c->M.mass[s];
+    if (mass > 0) {
+      const double d_iso0 = c->p.diffusion_coeff / mass;
+      A.cm[s] = c->M.charge[s] / mass;
+      A.ddr[s] = d_iso0 / dr;
+      A.ddz[s] = d_iso0 / dz;
+    }
+  }
+  A.gdz = 1.0 / dz;
+  A.dz = dz;
+  return A;
+}
+
+int
+run_fused (Ctx *c, bool s2, int fold, int fam_state = 1)
+{
+  FusedArgs A = fused_args (c);
+  if (s2) { A.fam_state = fam_state; A.cfl_fold = fold; }
+  int &o = c->occ_fused[c->stage_eabs][s2 ? 1 : 0][c->tile_cfg];
+  if (o == 0) {
+    int b = 0;
+    if (s2) launch_fused_m<true> (c->M.ns, c->tile_cfg, c->M, A, 0, 0, &b);
+    else launch_fused_m<false> (c->M.ns, c->tile_cfg, c->M, A, 0, 0, &b);
+    o = b > 0 ? b : 1;
+  }
+  const int blocks = std::min (c->n_items, c->num_sms * o);
+  if (blocks <= 0) return ARCOS_OK;
+  cudaError_t e = s2 ? launch_fused_m<true> (c->M.ns, c->tile_cfg, c->M, A, blocks, c->stream, nullptr)
+                     : launch_fused_m<false> (c->M.ns, c->tile_cfg, c->M, A, blocks, c->stream, nullptr);
+  if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("fused launch: ") + cudaGetErrorString (e));
+  return ARCOS_OK;
 }
 
 // Runs a stage-kernel mode over all patches (one persistent launch) or once per
@@ -642,6 +802,11 @@ rk2_general (Ctx *c)
 int
 rk2_fused_launches (Ctx *c, int src, int fold)
 {
+  if (lean_ok (c)) {
+    // the state stays in set 0; n* goes to set 1
+    int r = run_fused (c, false, 0);
+    return r ? r : run_fused (c, true, fold);
+  }
   StageArgs A = base_args (c);
   A.src = src;
   A.dst = 1 - src;
@@ -651,6 +816,150 @@ rk2_fused_launches (Ctx *c, int src, int fold)
   A.cfl_fold = fold;
   A.want_charge = c->fn ? 1 : 0;
   return run_stage (c, A, M_S2);
+}
+
+
+// ---- discrete adjoint -----------------------------------------------------------
+constexpr int ADJ_WY = 4, ADJ_BAND = 16;
+
+inline int adj_lam_idx (Ctx *c, int which) { return which * c->M.ns; }
+inline int adj_lams_idx (Ctx *c) { return 2 * c->M.ns; }
+inline int adj_seg_n0 (Ctx *c, int j) { return 3 * c->M.ns + j * c->M.ns; }
+inline int adj_seg_ns (Ctx *c, int j) { return 3 * c->M.ns + (c->adj_ck + j) * c->M.ns; }
+inline int adj_ckpt (Ctx *c, int seg) { return 3 * c->M.ns + (2 * c->adj_ck + seg) * c->M.ns; }
+inline int adj_final (Ctx *c) { return 3 * c->M.ns + (2 * c->adj_ck + c->adj_nseg) * c->M.ns; }
+inline int adj_arrays (Ctx *c) { return adj_final (c) + c->M.ns; }
+
+// copies the densities of `set` to (to_adj) or from adjoint arrays idx .. idx+ns-1
+int
+adj_copy (Ctx *c, bool to_adj, int set, int idx)
+{
+  for (auto &P : c->pd_h)
+    for (int s = 0; s < P.ns; s++) {
+      double *a = P.arr (set, K_DENS, s), *b = P.adj + (size_t) (idx + s) * P.asz;
+      CK (cudaMemcpyAsync (to_adj ? b : a, to_adj ? a : b, sizeof (double) * P.asz, cudaMemcpyDeviceToDevice, c->stream));
+    }
+  return ARCOS_OK;
+}
+
+int
+adj_alloc (Ctx *c, int nsteps, int ck)
+{
+  const int ns = c->M.ns;
+  if (c->adj_pool && c->adj_nsteps == nsteps && c->adj_ck == ck) return ARCOS_OK;
+  cudaFree (c->adj_pool); c->adj_pool = nullptr;
+  cudaFree (c->adj_hs_d); c->adj_hs_d = nullptr;
+  c->adj_nsteps = nsteps;
+  c->adj_ck = ck;
+  c->adj_nseg = (nsteps + ck - 1) / ck;
+  size_t total = 0;
+  for (auto &P : c->pd_h) total += (size_t) adj_arrays (c) * P.asz;
+  CK (cudaMalloc (&c->adj_pool, sizeof (double) * total));
+  CK (cudaMemsetAsync (c->adj_pool, 0, sizeof (double) * total, c->stream));
+  size_t o = 0;
+  for (auto &P : c->pd_h) { P.adj = c->adj_pool + o; o += (size_t) adj_arrays (c) * P.asz; }
+  CK (cudaMemcpyAsync (c->pd_d, c->pd_h.data (), sizeof (PatchDesc) * c->pd_h.size (), cudaMemcpyHostToDevice, c->stream));
+  CK (cudaMalloc (&c->adj_hs_d, sizeof (double) * (size_t) c->nfam * nsteps));
+  c->adj_hs.assign ((size_t) c->nfam * nsteps, 0.0);
+  if (!c->adj_tiles_d) {
+    std::vector<AdjTile> tl;
+    for (int p = 0; p < (int) c->pd_h.size (); p++) {
+      const PatchDesc &P = c->pd_h[p];
+      for (int zb = 0; zb < P.nz; zb += ADJ_WY * ADJ_BAND)
+        for (int c0 = 0; c0 < P.nr; c0 += ADJ_STRIP) tl.push_back (AdjTile{p, c0, zb, 0});
+    }
+    c->adj_ntiles = (int) tl.size ();
+    CK (cudaMalloc (&c->adj_tiles_d, sizeof (AdjTile) * tl.size ()));
+    CK (cudaMemcpy (c->adj_tiles_d, tl.data (), sizeof (AdjTile) * tl.size (), cudaMemcpyHostToDevice));
+    c->adj_blocks = std::min (c->adj_ntiles, c->num_sms * 4);
+    CK (cudaMalloc (&c->adj_gpart_d, sizeof (double) * (size_t) c->adj_blocks * (ns + 1)));
+    const size_t ng = c->nodes_h.size () + 2 * (size_t) c->M.nreact;
+    CK (cudaMalloc (&c->adj_gtab_d, sizeof (double) * std::max<size_t> (ng, 1)));
+  }
+  // 1 / (e2 - e1) of every node (reaction.c:139-142)
+  {
+    std::vector<double> inv (std::max<size_t> (c->nodes_h.size (), 1), 0.0);
+    for (int r = 0; r < c->M.nreact; r++)
+      for (int k = 0; k <= c->M.r_steps[r]; k++) {
+        const double e1 = pow (10, c->M.r_e_min[r] + c->M.r_e_step[r] * (double) k);
+        const double e2 = e1 * pow (10, c->M.r_e_step[r]);
+        inv[c->M.r_node_off[r] + k] = 1.0 / (e2 - e1);
+      }
+    if (!c->adj_invde_d) CK (cudaMalloc (&c->adj_invde_d, sizeof (double) * inv.size ()));
+    CK (cudaMemcpy (c->adj_invde_d, inv.data (), sizeof (double) * inv.size (), cudaMemcpyHostToDevice));
+  }
+  c->adj_lam = 0;
+  c->adj_fwd = false;
+  return ARCOS_OK;
+}
+
+// One RK2 step with the frozen step sizes hs[:, k] (no CFL); stage 2 optional.
+int
+adj_frozen_step (Ctx *c, int k, bool s2)
+{
+  k_set_h<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->st_d, c->nfam, c->adj_hs_d, c->adj_nsteps, k);
+  CKL ();
+  int r = run_fused (c, false, 0);
+  if (r || !s2) return r;
+  return run_fused (c, true, 0, 0);
+}
+
+int
+run_vjp (Ctx *c, int mode, int st_idx, int lam_idx, int lams_idx, int out_idx, int k)
+{
+  VjpArgs A{};
+  A.patches = c->pd_d;
+  A.tiles = c->adj_tiles_d;
+  A.n_tiles = c->adj_ntiles;
+  A.mode = mode;
+  A.st_idx = st_idx; A.lam_idx = lam_idx; A.lams_idx = lams_idx; A.out_idx = out_idx;
+  A.hs = c->adj_hs_d;
+  A.hs_stride = c->adj_nsteps;
+  A.k = k;
+  A.nodes = c->nodes_d;
+  A.inv_de = c->adj_invde_d;
+  A.g_table = c->adj_gtab_d;
+  A.n_nodes = (int) c->nodes_h.size ();
+  A.g_part = c->adj_gpart_d;
+  A.colfac = c->colfac_d;
+  const double dr = c->dr[0], dz = c->dz[0], D = c->p.diffusion_coeff;
+  for (int s = 0; s < c->M.ns; s++) {
+    const double mass = c->M.mass[s];
+    if (mass > 0) {
+      const double mu = 1.0 / mass;
+      A.cm[s] = c->M.charge[s] / mass;
+      A.ddr[s] = (D / mass) / dr;
+      A.ddz[s] = (D / mass) / dz;
+      A.mudr[s] = mu / dr;
+      A.mudz[s] = mu / dz;
+    }
+  }
+  A.Ddr = D / dr;
+  A.Ddz = D / dz;
+  A.gdz = 1.0 / dz;
+  cudaError_t e = cudaSuccess;
+  switch (c->M.ns) {
+  case 1: k_vjp<1, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
+  case 2: k_vjp<2, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
+  case 3: k_vjp<3, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
+  case 4: k_vjp<4, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
+  case 5: k_vjp<5, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
+  case 6: k_vjp<6, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
+  default: return fail (ARCOS_ERR_ARG, "adjoint: 1..6 species");
+  }
+  e = cudaGetLastError ();
+  if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("vjp launch: ") + cudaGetErrorString (e));
+  return ARCOS_OK;
+}
+
+int
+adj_check (Ctx *c)
+{
+  if (!lean_ok (c))
+    return fail (ARCOS_ERR_STATE, "adjoint: needs single-grid families, fixed field, the division-free limiter and TMA staging");
+  for (auto &P : c->pd_h)
+    if (P.ntheta != 1) return fail (ARCOS_ERR_ARG, "adjoint: 2-D grids only");
+  return ARCOS_OK;
 }
 
 }  // namespace
@@ -717,6 +1026,10 @@ arcos_destroy (void *ctx)
   if (!c) return ARCOS_OK;
   if (c->graph2) cudaGraphExecDestroy (c->graph2);
   if (c->graph_tree) cudaGraphExecDestroy (c->graph_tree);
+  cudaFree (c->colfac_d);
+  cudaFree (c->lean_nodes_d);
+  cudaFree (c->adj_pool); cudaFree (c->adj_hs_d); cudaFree (c->adj_gtab_d);
+  cudaFree (c->adj_gpart_d); cudaFree (c->adj_invde_d); cudaFree (c->adj_tiles_d);
   cudaFree (c->pool); cudaFree (c->pd_d); cudaFree (c->nodes_d); cudaFree (c->st_d);
   cudaFree (c->dtlog_d); cudaFree (c->etz_d); cudaFree (c->done_d); cudaFree (c->items_d);
   cudaFree (c->plist_d); cudaFree (c->kids_d); cudaFree (c->strips_d); cudaFree (c->ext_d);
@@ -1034,6 +1347,7 @@ arcos_commit (void *ctx)
   CK (cudaMalloc (&c->pd_d, sizeof (PatchDesc) * np));
   CK (cudaMemcpyAsync (c->pd_d, c->pd_h.data (), sizeof (PatchDesc) * np, cudaMemcpyHostToDevice, c->stream));
   // tables
+  if ((r_ = upload_lean_nodes (c))) return r_;
   if (!c->nodes_h.empty ()) {
     CK (cudaMalloc (&c->nodes_d, sizeof (TableNode) * c->nodes_h.size ()));
     CK (cudaMemcpyAsync (c->nodes_d, c->nodes_h.data (), sizeof (TableNode) * c->nodes_h.size (), cudaMemcpyHostToDevice, c->stream));
@@ -1180,7 +1494,23 @@ arcos_commit (void *ctx)
   // the fused path needs single-grid families with every side external
   c->fused_ok = true;
   for (int i = 0; i < np; i++)
-    if (c->g[i].parent >= 0 || c->g[i].ext_bound != 15 || c->g[i].r0 != 0) c->fused_ok = false;
+    if (c->g[i].parent >= 0 || c->g[i].ext_bound != 15 || c->g[i].r0 != 0 || c->pd_h[i].level != 0)
+      c->fused_ok = false;
+  if (c->fused_ok) {
+    // radial divergence factors of every column of the root level (.f90:408-412),
+    // padded to whole 32-column tiles
+    int maxnr = 0;
+    for (auto &P : c->pd_h) maxnr = std::max (maxnr, P.nr);
+    const int ncol = (maxnr + 31) / 32 * 32 + 32;
+    std::vector<double> cf (2 * (size_t) ncol);
+    for (int ir = 0; ir < ncol; ir++) {
+      const double r_inv = 1.0 / (((double) ir + 0.5) * c->dr[0]);
+      cf[2 * ir] = (double) ir * r_inv;
+      cf[2 * ir + 1] = (double) (ir + 1) * r_inv;
+    }
+    CK (cudaMalloc (&c->colfac_d, sizeof (double) * cf.size ()));
+    CK (cudaMemcpy (c->colfac_d, cf.data (), sizeof (double) * cf.size (), cudaMemcpyHostToDevice));
+  }
   CK (cudaStreamSynchronize (c->stream));
   return ARCOS_OK;
 }
@@ -1303,6 +1633,8 @@ arcos_set_field_fn (void *ctx, arcos_field_fn fn, void *user)
   if (!c) return fail (ARCOS_ERR_ARG, "null context");
   c->fn = fn;
   c->user = user;
+  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
   return ARCOS_OK;
 }
 
@@ -1312,6 +1644,8 @@ arcos_set_per_patch (void *ctx, int on)
   Ctx *c = (Ctx *) ctx;
   if (!c) return fail (ARCOS_ERR_ARG, "null context");
   c->per_patch = on != 0;
+  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
   return ARCOS_OK;
 }
 
@@ -1561,8 +1895,9 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
     }
     if (nsteps & 1) {
       if ((r = rk2_fused_launches (c, 0, 1))) return r;
-      for (auto &P : c->pd_h)
-        CK (cudaMemcpyAsync (P.arr (0, K_DENS, 0), P.arr (1, K_DENS, 0), sizeof (double) * P.asz * P.ns, cudaMemcpyDeviceToDevice, c->stream));
+      if (!lean_ok (c))
+        for (auto &P : c->pd_h)
+          CK (cudaMemcpyAsync (P.arr (0, K_DENS, 0), P.arr (1, K_DENS, 0), sizeof (double) * P.asz * P.ns, cudaMemcpyDeviceToDevice, c->stream));
     }
     // ghosts of the final state as prepare_grid leaves them (cdr.c:1322)
     if ((r = do_ext_bnd (c, 0))) return r;
@@ -1629,10 +1964,220 @@ arcos_enqueue_stage (void *ctx, int mode, int src)
   Ctx *c = (Ctx *) ctx;
   int r = chk_committed (c);
   if (r) return r;
+  if (lean_ok (c)) return run_fused (c, mode == 2, 1);
   StageArgs A = base_args (c);
   A.src = src; A.dst = 1 - src;
   if (mode == 2) { A.fam_state = 1; A.cfl_fold = 1; }
   return run_stage (c, A, mode == 1 ? M_S1 : M_S2);
+}
+
+// ---- discrete adjoint (C ABI) ----
+int
+arcos_adj_forward (void *ctx, int nsteps, int ckpt_every, double h_attempt, const double *h_seq,
+                   double *h_used)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if ((r = adj_check (c))) return r;
+  if (nsteps < 1 || ckpt_every < 1) return fail (ARCOS_ERR_ARG, "adjoint: nsteps and ckpt_every must be >= 1");
+  if ((r = adj_alloc (c, nsteps, ckpt_every))) return r;
+  const int nf = c->nfam;
+  if (h_seq) {
+    for (size_t i = 0; i < c->adj_hs.size (); i++) c->adj_hs[i] = h_seq[i];
+    CK (cudaMemcpyAsync (c->adj_hs_d, c->adj_hs.data (), sizeof (double) * c->adj_hs.size (), cudaMemcpyHostToDevice, c->stream));
+  }
+  std::vector<double> dts;
+  for (int seg = 0; seg < c->adj_nseg; seg++) {
+    const int k0 = seg * c->adj_ck, k1 = std::min (nsteps, k0 + c->adj_ck);
+    if ((r = adj_copy (c, true, 0, adj_ckpt (c, seg)))) return r;
+    if (h_seq) {
+      for (int k = k0; k < k1; k++)
+        if ((r = adj_frozen_step (c, k, true))) return r;
+    } else {
+      dts.assign ((size_t) nf * (k1 - k0), 0.0);
+      if ((r = arcos_run (ctx, k1 - k0, h_attempt, dts.data ()))) return r;
+      for (int f = 0; f < nf; f++)
+        for (int k = k0; k < k1; k++) c->adj_hs[(size_t) f * nsteps + k] = dts[(size_t) f * (k1 - k0) + (k - k0)];
+    }
+  }
+  if ((r = adj_copy (c, true, 0, adj_final (c)))) return r;
+  if (!h_seq)
+    CK (cudaMemcpyAsync (c->adj_hs_d, c->adj_hs.data (), sizeof (double) * c->adj_hs.size (), cudaMemcpyHostToDevice, c->stream));
+  else {
+    if ((r = do_ext_bnd (c, 0))) return r;
+    if ((r = do_periodic (c, 0, 1))) return r;
+  }
+  CK (cudaStreamSynchronize (c->stream));
+  if (h_used)
+    for (size_t i = 0; i < c->adj_hs.size (); i++) h_used[i] = c->adj_hs[i];
+  c->adj_fwd = true;
+  c->adj_lam = 0;
+  // the cotangent starts at zero until arcos_adj_set_cotangent
+  for (auto &P : c->pd_h)
+    CK (cudaMemsetAsync (P.adj + (size_t) adj_lam_idx (c, 0) * P.asz, 0, sizeof (double) * P.asz * P.ns, c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  return check_state_errors (c);
+}
+
+int
+arcos_adj_set_cotangent (void *ctx, int grid, int species, const double *host)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (!c->adj_fwd) return fail (ARCOS_ERR_STATE, "adjoint: run arcos_adj_forward first");
+  if (grid < 0 || grid >= (int) c->pd_h.size () || species < 0 || species >= c->M.ns || !host)
+    return fail (ARCOS_ERR_ARG, "arcos_adj_set_cotangent: bad argument");
+  const PatchDesc &P = c->pd_h[grid];
+  const size_t w = sizeof (double) * (P.nr + 4);
+  double *dst = P.adj + (size_t) (adj_lam_idx (c, c->adj_lam) + species) * P.asz;
+  CK (cudaMemcpy2DAsync (dst, sizeof (double) * P.pitch, host, w, w, (size_t) (P.nz + 4), cudaMemcpyHostToDevice, c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
+int
+arcos_adj_get_cotangent (void *ctx, int grid, int species, double *host)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (!c->adj_fwd) return fail (ARCOS_ERR_STATE, "adjoint: run arcos_adj_forward first");
+  if (grid < 0 || grid >= (int) c->pd_h.size () || species < 0 || species >= c->M.ns || !host)
+    return fail (ARCOS_ERR_ARG, "arcos_adj_get_cotangent: bad argument");
+  const PatchDesc &P = c->pd_h[grid];
+  const size_t w = sizeof (double) * (P.nr + 4);
+  const double *src = P.adj + (size_t) (adj_lam_idx (c, c->adj_lam) + species) * P.asz;
+  CK (cudaMemcpy2DAsync (host, w, src, sizeof (double) * P.pitch, w, (size_t) (P.nz + 4), cudaMemcpyDeviceToHost, c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
+int
+arcos_adj_backward (void *ctx, double *grad_mobility, double *grad_diffusion, double *grad_tables)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if ((r = adj_check (c))) return r;
+  if (!c->adj_fwd) return fail (ARCOS_ERR_STATE, "adjoint: run arcos_adj_forward first");
+  const int ns = c->M.ns;
+  const size_t ng = c->nodes_h.size () + 2 * (size_t) c->M.nreact;
+  CK (cudaMemsetAsync (c->adj_gtab_d, 0, sizeof (double) * std::max<size_t> (ng, 1), c->stream));
+  CK (cudaMemsetAsync (c->adj_gpart_d, 0, sizeof (double) * (size_t) c->adj_blocks * (ns + 1), c->stream));
+  int lam = c->adj_lam;
+  for (int seg = c->adj_nseg - 1; seg >= 0; seg--) {
+    const int k0 = seg * c->adj_ck, k1 = std::min (c->adj_nsteps, k0 + c->adj_ck);
+    // recompute the segment from its checkpoint, keeping n0 and n* of every step
+    if ((r = adj_copy (c, false, 0, adj_ckpt (c, seg)))) return r;
+    for (int k = k0; k < k1; k++) {
+      if ((r = adj_copy (c, true, 0, adj_seg_n0 (c, k - k0)))) return r;
+      if ((r = adj_frozen_step (c, k, false))) return r;
+      if ((r = adj_copy (c, true, 1, adj_seg_ns (c, k - k0)))) return r;
+      if (k + 1 < k1 && (r = run_fused (c, true, 0, 0))) return r;
+    }
+    // reverse sweep of the segment
+    for (int k = k1 - 1; k >= k0; k--) {
+      if ((r = run_vjp (c, 1, adj_seg_ns (c, k - k0), adj_lam_idx (c, lam), 0, adj_lams_idx (c), k))) return r;
+      if ((r = run_vjp (c, 2, adj_seg_n0 (c, k - k0), adj_lam_idx (c, lam), adj_lams_idx (c),
+                        adj_lam_idx (c, 1 - lam), k))) return r;
+      lam = 1 - lam;
+    }
+  }
+  c->adj_lam = lam;
+  // the state goes back to the end of the forward run
+  if ((r = adj_copy (c, false, 0, adj_final (c)))) return r;
+  if ((r = do_ext_bnd (c, 0))) return r;
+  if ((r = do_periodic (c, 0, 1))) return r;
+  std::vector<double> gp ((size_t) c->adj_blocks * (ns + 1)), gt (std::max<size_t> (ng, 1));
+  CK (cudaMemcpyAsync (gp.data (), c->adj_gpart_d, sizeof (double) * gp.size (), cudaMemcpyDeviceToHost, c->stream));
+  CK (cudaMemcpyAsync (gt.data (), c->adj_gtab_d, sizeof (double) * gt.size (), cudaMemcpyDeviceToHost, c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  if (grad_mobility)
+    for (int s = 0; s < ns; s++) {
+      double v = 0.0;
+      for (int b = 0; b < c->adj_blocks; b++) v += gp[(size_t) b * (ns + 1) + s];
+      grad_mobility[s] = c->M.mass[s] > 0 ? v : 0.0;
+    }
+  if (grad_diffusion) {
+    double v = 0.0;
+    for (int b = 0; b < c->adj_blocks; b++) v += gp[(size_t) b * (ns + 1) + ns];
+    *grad_diffusion = v;
+  }
+  if (grad_tables)
+    for (size_t i = 0; i < ng; i++) grad_tables[i] = gt[i];
+  return check_state_errors (c);
+}
+
+int
+arcos_adj_table_entries (void *ctx)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return -1;
+  return (int) (c->nodes_h.size () + 2 * (size_t) c->M.nreact);
+}
+
+int
+arcos_adj_table_offset (void *ctx, int reaction)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c || reaction < 0 || reaction >= c->M.nreact) return -1;
+  return c->M.r_node_off[reaction];
+}
+
+// ---- model parameters after commit (the adjoint's inputs) ----
+static void
+drop_graphs (Ctx *c)
+{
+  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
+}
+
+int
+arcos_set_species_mass (void *ctx, int species, double mass)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  if (species < 0 || species >= c->M.ns) return fail (ARCOS_ERR_ARG, "species out of range");
+  if ((mass > 0) != (c->M.mass[species] > 0))
+    return fail (ARCOS_ERR_ARG, "a species cannot change between mobile and immobile");
+  c->M.mass[species] = mass;
+  c->p.mass[species] = mass;
+  drop_graphs (c);
+  return ARCOS_OK;
+}
+
+int
+arcos_set_diffusion (void *ctx, double diffusion_coeff)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  c->M.diffusion_coeff = diffusion_coeff;
+  c->p.diffusion_coeff = diffusion_coeff;
+  drop_graphs (c);
+  return ARCOS_OK;
+}
+
+int
+arcos_set_table_values (void *ctx, int reaction, const double *values, double underflow, double overflow)
+{
+  Ctx *c = (Ctx *) ctx;
+  if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  if (reaction < 0 || reaction >= c->M.nreact || !values) return fail (ARCOS_ERR_ARG, "bad reaction or values");
+  Model &M = c->M;
+  std::vector<TableNode> tmp;
+  build_nodes (M.r_e_min[reaction], M.r_e_step[reaction], M.r_steps[reaction], values, tmp);
+  for (size_t k = 0; k < tmp.size (); k++) c->nodes_h[M.r_node_off[reaction] + k] = tmp[k];
+  M.r_under[reaction] = underflow;
+  M.r_over[reaction] = overflow;
+  drop_graphs (c);
+  if (c->committed) {
+    CK (cudaMemcpy (c->nodes_d, c->nodes_h.data (), sizeof (TableNode) * c->nodes_h.size (), cudaMemcpyHostToDevice));
+    int r = upload_lean_nodes (c);
+    if (r) return r;
+  }
+  return ARCOS_OK;
 }
 
 // Per-family steps taken so far and the error bits.
@@ -1671,8 +2216,8 @@ arcos_set_exact (void *ctx, int on)
   return ARCOS_OK;
 }
 
-// Tile shape of the stencil kernel (0: 32x16 cells, 128 threads; 1: 32x16,
-// 256 threads... see TILE_WY/TILE_RPW).  May be changed after arcos_commit.
+// Tile shape of the stencil kernels (0: 32 x 16 cells, 128 threads; 1: 32 x 32
+// cells, 256 threads).  May be changed after arcos_commit.
 int
 arcos_set_tile (void *ctx, int cfg)
 {

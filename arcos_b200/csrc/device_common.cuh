@@ -33,6 +33,7 @@ struct PatchDesc {
   double *base;                 // start of this patch's arrays
   int fam;                      // family (independent grid tree) this patch belongs to
   int pad_;
+  double *adj;                  // adjoint work arrays of this patch (same layout), or null
 
   // index of an array within the block: [set][dens s | d_dens s | er ez etheta eabs charge]
   __host__ __device__ inline int array_index (int set, int kind, int s) const {
@@ -62,8 +63,8 @@ struct WorkItem {
 // One node of a reaction table as the device uses it.  thr is the smallest
 // |E| whose reference lookup (reaction.c:127-136) lands at or above this node;
 // val/e1/slope reproduce reaction.c:137-142 with pow() evaluated on the host.
-struct TableNode {
-  double thr, val, e1, slope;
+struct __align__ (16) TableNode {
+  double val, e1, slope, thr;
 };
 
 struct Model {

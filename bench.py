@@ -224,8 +224,12 @@ def run_device(args):
         tree.upload(0, "dens", pb.dens[0][s], s)
     tree.set_fixed_field(pb.fields)
     L, h = tree.L, tree.h
-    from arcos_b200.autotune import autotune_tiles
-    tune = autotune_tiles(tree, steps=6, stream=stream)
+    if args.tile is None:
+        from arcos_b200.autotune import autotune_tiles
+        tune = autotune_tiles(tree, steps=6, stream=stream)
+    else:
+        tree.set_tile(args.tile)
+        tune = {}
     warm = max(4, args.warmup + (args.warmup & 1))
     steps = args.steps + (args.steps & 1)
     check(L.arcos_run_prepare(h, 50.0))
@@ -361,6 +365,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--exact", action="store_true", help="bit-exact flux limiter")
+    ap.add_argument("--tile", type=int, default=None,
+                    help="fixed tile shape (0: 32x16 cells, 1: 32x32); default: autotuned")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -195,6 +195,47 @@ int arcos_table_rates (double e_min, double e_step, int steps, double underflow,
                        double overflow, const double *values, const double *eabs,
                        int n, double *rates);
 
+/* ---- model parameters after arcos_commit (no reference counterpart: the
+ * reference reads them once from its input files, cdr.c:50-101,
+ * react_table.c:73-111) ---- */
+/* Mass of a species (mobility = 1/mass); it stays mobile or immobile. */
+int arcos_set_species_mass (void *ctx, int species, double mass);
+/* diffusion_coeff (cstream.c:133). */
+int arcos_set_diffusion (void *ctx, double diffusion_coeff);
+/* New values[0..steps] (and under/overflow) of a reaction table; the
+ * |E| grid (e_min, e_step, steps) stays. */
+int arcos_set_table_values (void *ctx, int reaction, const double *values,
+                            double underflow, double overflow);
+
+/* ---- discrete adjoint of the fused RK2 step (no reference counterpart) -----
+ * For single-grid 2-D families with a fixed field and the division-free
+ * limiter.  arcos_adj_forward runs nsteps steps from the state in set 0,
+ * keeping a checkpoint of the state every ckpt_every steps; with h_seq
+ * (nfam x nsteps, row per family) the steps are frozen to those sizes,
+ * otherwise they come from the CFL rule with the attempted h_attempt.
+ * h_used (nfam x nsteps, may be NULL) receives the sizes.  The cotangent
+ * dJ/dn(T) is then set per grid and species (rz-array layout, like
+ * arcos_upload) and arcos_adj_backward runs the reverse sweep (recomputing
+ * every segment from its checkpoint): afterwards arcos_adj_get_cotangent
+ * returns dJ/dn(0) and the gradients are
+ *   grad_mobility[species]   dJ/d(1/mass) (0 for immobile species),
+ *   grad_diffusion[0]        dJ/d diffusion_coeff,
+ *   grad_tables[...]         arcos_adj_table_entries() values: entry
+ *                            arcos_adj_table_offset(r) + k is dJ/d values[k]
+ *                            of reaction r (k = 0..steps); the last
+ *                            2 * nreact entries are dJ/d underflow,
+ *                            dJ/d overflow of each reaction.
+ * The limiter is differentiated branch by branch (subgradients at its switch
+ * points).  The state returns to the end of the forward run. */
+int arcos_adj_forward (void *ctx, int nsteps, int ckpt_every, double h_attempt,
+                       const double *h_seq, double *h_used);
+int arcos_adj_set_cotangent (void *ctx, int grid, int species, const double *host);
+int arcos_adj_get_cotangent (void *ctx, int grid, int species, double *host);
+int arcos_adj_backward (void *ctx, double *grad_mobility, double *grad_diffusion,
+                        double *grad_tables);
+int arcos_adj_table_entries (void *ctx);
+int arcos_adj_table_offset (void *ctx, int reaction);
+
 /* ---- narrow seam (arcos_f90/src/cdr_advect_diffu_wrap.c:25-41) ----------
  * Same signature and argument meaning as the reference wrapper around the
  * Fortran cdr_advect_vec: adds the drift/diffusion divergence of one species
