@@ -88,6 +88,15 @@ def lib():
     L.arcos_cdr_advect_vec_dev.argtypes = [C.c_double, C.c_double, VP, VP, VP, VP, C.c_double,
                                            C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
                                            C.c_int, VP]
+    L.arcos_set_species_mass.argtypes = [VP, C.c_int, C.c_double]
+    L.arcos_set_diffusion.argtypes = [VP, C.c_double]
+    L.arcos_set_table_values.argtypes = [VP, C.c_int, DP, C.c_double, C.c_double]
+    L.arcos_adj_forward.argtypes = [VP, C.c_int, C.c_int, C.c_double, DP, DP]
+    L.arcos_adj_set_cotangent.argtypes = [VP, C.c_int, C.c_int, DP]
+    L.arcos_adj_get_cotangent.argtypes = [VP, C.c_int, C.c_int, DP]
+    L.arcos_adj_backward.argtypes = [VP, DP, DP, DP]
+    L.arcos_adj_table_entries.argtypes = [VP]
+    L.arcos_adj_table_offset.argtypes = [VP, C.c_int]
     _lib = L
     return L
 

@@ -219,6 +219,17 @@ class CdrTree:
         check(self.L.arcos_family_state(self.h, fam, C.byref(st), C.byref(h), C.byref(e)))
         return st.value, h.value, e.value
 
+    # ---- model parameters after commit ----
+    def set_species_mass(self, s: int, mass: float):
+        check(self.L.arcos_set_species_mass(self.h, s, mass))
+
+    def set_diffusion(self, diffusion_coeff: float):
+        check(self.L.arcos_set_diffusion(self.h, diffusion_coeff))
+
+    def set_table_values(self, reaction: int, values, underflow: float, overflow: float):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        check(self.L.arcos_set_table_values(self.h, reaction, _dp(v), underflow, overflow))
+
     def set_tma(self, on: bool):
         check(self.L.arcos_set_tma(self.h, 1 if on else 0))
 

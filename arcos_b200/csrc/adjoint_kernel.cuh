@@ -202,6 +202,10 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         za[0][s] = za[1][s]; za[1][s] = za[2][s]; za[2][s] = za[3][s]; za[3][s] = 0.0;
       }
       const bool zreal = zcol && a >= 0 && a <= nz;
+      // the parameter sums take every face once: the band holding row a
+      // (row nz-1 for the top face) and the strip holding column c
+      const bool zown = lane < ADJ_STRIP && ((a >= rb0 && a < rb0 + BAND && a < nz)
+                                             || (a == nz && nz - 1 >= rb0 && nz - 1 < rb0 + BAND));
 #pragma unroll
       for (int s = 0; s < NS; s++)
         wn[3][s] = (zcol && a + 1 >= -2 && a + 1 <= nz + 1) ? ST (s, c, a + 1) : 0.0;
@@ -219,8 +223,10 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
           za[1][s] = __fma_rn (g, fg.pL, za[1][s]);
           za[2][s] = __fma_rn (g, fg.pR, za[2][s]);
           za[3][s] = __fma_rn (g, fg.pRR, za[3][s]);
-          gmu[s] += g * (fg.dv * M.charge[s] * e + fg.ddd * A.Ddz);
-          gD += g * fg.ddd * A.mudz[s];
+          if (zown) {
+            gmu[s] += g * (fg.dv * M.charge[s] * e + fg.ddd * A.Ddz);
+            gD += g * fg.ddd * A.mudz[s];
+          }
         }
       } else {
 #pragma unroll
@@ -252,6 +258,8 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
       // radial faces of row j, lanes over faces ar - 1/2
       {
         const bool rreal = ar >= 0 && ar <= nr;
+        const bool rown = (ar >= c0 && ar < c0 + ADJ_STRIP && ar < nr)
+                          || (ar == nr && nr - 1 >= c0 && nr - 1 < c0 + ADJ_STRIP);
         const double e = rreal ? er[Pp->off (ar - 1, j, 0)] : 0.0;
         const double fm = (rreal && ar < nr) ? A.colfac[2 * ar] : 0.0;            // erm(ar)
         const double fp = (rreal && ar >= 1) ? A.colfac[2 * (ar - 1) + 1] : 0.0;  // erp(ar-1)
@@ -264,8 +272,10 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
               const FaceGrad fg = face_grad (true, ST (s, ar - 2, j), ST (s, ar - 1, j), ST (s, ar, j),
                                              ST (s, ar + 1, j), A.cm[s] * e, A.ddr[s]);
               pLL = g * fg.pLL; pL = g * fg.pL; pR = g * fg.pR; pRR = g * fg.pRR;
-              gmu[s] += g * (fg.dv * M.charge[s] * e + fg.ddd * A.Ddr);
-              gD += g * fg.ddd * A.mudr[s];
+              if (rown) {
+                gmu[s] += g * (fg.dv * M.charge[s] * e + fg.ddd * A.Ddr);
+                gD += g * fg.ddd * A.mudr[s];
+              }
             }
           }
           // cell c0 + lane: RR of face lane, R of lane+1, L of lane+2, LL of lane+3

@@ -21,6 +21,7 @@ grid per step.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -186,6 +187,183 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- device ----
+
+# ------------------------------------------------------------ extra rows ----
+def _events(stream):
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _load(tree, pb):
+    for g, per in enumerate(pb.dens):
+        for s, a in enumerate(per):
+            tree.upload(g, "dens", a, s)
+    for f, E in enumerate(pb.family_E):
+        tree.set_family_field(f, *E)
+    tree.set_fixed_field(pb.fields)
+
+
+def extra_amr(stream, steps: int = 10):
+    """Batched AMR: 4 levels, 320 patches (sides 16..256) advanced by one
+    launch per kernel kind over all patches (replayed from a CUDA graph)
+    against one launch per patch, same GPU, same steps."""
+    import numpy as np
+    from arcos_b200 import workloads
+    from arcos_b200.cdr import CdrTree
+    from arcos_b200._lib import check
+    pb = workloads.amr()
+    out = {"workload": f"{len(pb.specs)} patches on 4 levels (root 512x1024, sides 16..256), "
+                       f"{pb.cells} cells, 2 species, fixed field", "patches": len(pb.specs),
+           "cells": pb.cells}
+    for mode in ("batched", "per_patch"):
+        tree = CdrTree(pb.params, pb.model, pb.specs, stream=stream.cuda_stream, per_patch=(mode == "per_patch"))
+        _load(tree, pb)
+        nf = sum(1 for sp in pb.specs if sp.parent < 0)
+        dts = np.zeros(nf * steps)
+        tree.run(2, 50.0)
+        e0, e1 = _events(stream)
+        e0.record(stream)
+        check(tree.L.arcos_run(tree.h, steps, 50.0, dts.ctypes.data_as(C.POINTER(C.c_double))))
+        e1.record(stream)
+        e1.synchronize()
+        out[f"{mode}_ms_per_step"] = e0.elapsed_time(e1) / steps
+        tree.close()
+    out["batched_value"] = pb.cells * 2 / (out["batched_ms_per_step"] / 1e3)
+    out["batched_over_per_patch"] = out["per_patch_ms_per_step"] / out["batched_ms_per_step"]
+    return out
+
+
+def extra_adjoint(stream, K: int = 64, ck: int = 8, ndir: int = 32):
+    """Discrete adjoint: 256 x 512 grid, 64 RK2 steps, checkpoints every 8;
+    J = 1/2 sum (n_e(T) - n_target)^2 cell_volume; reverse sweep time over the
+    forward run's time, and central finite differences (step 1e-6 relative,
+    32 seeded smooth directions over densities, mobility, diffusion and the
+    256 table values) of the frozen-step forward."""
+    import numpy as np
+    from arcos_b200 import workloads
+    from arcos_b200.adjoint import Adjoint, cell_volume, fd_objective_difference, smooth_direction
+    from arcos_b200.cdr import CdrTree
+    from arcos_b200._lib import check
+    pb = workloads.plain(nr=256, nz=512, ion_mass=0.0, noise=1e-6, seed=3)
+    spec = pb.specs[0]
+    tree = CdrTree(pb.params, pb.model, pb.specs, stream=stream.cuda_stream)
+    _load(tree, pb)
+    adj = Adjoint(tree)
+    vol = cell_volume(spec, pb.params.dr(0), pb.params.dz(0))
+    rng = np.random.default_rng(5)
+    tgt = workloads.seed_dens(spec, pb.params, rng, amp=0.11, sigma=0.09, noise=1e-6)
+    for s in range(2):
+        tree.upload(0, "dens", tgt, s)
+    tree.run(K, 50.0)
+    target = tree.download(0, "dens", 0)
+    tab = pb.model.reactions[0].table
+    base_vals = np.array(tab.values, dtype=np.float64)
+
+    def apply(d0, mu, D, vals):
+        for s in range(2):
+            tree.upload(0, "dens", d0[s], s)
+        tree.set_species_mass(0, 1.0 / mu)
+        tree.set_diffusion(D)
+        tree.set_table_values(0, vals, tab.underflow, tab.overflow)
+
+    d0 = [a.copy() for a in pb.dens[0]]
+    mu0, D0 = 1.0, pb.params.diffusion_coeff
+    # forward cost: the plain fused run of K steps
+    apply(d0, mu0, D0, base_vals)
+    dts = np.zeros(K)
+    tree.run(2, 50.0)
+    apply(d0, mu0, D0, base_vals)
+    e0, e1 = _events(stream)
+    e0.record(stream)
+    check(tree.L.arcos_run(tree.h, K, 50.0, dts.ctypes.data_as(C.POINTER(C.c_double))))
+    e1.record(stream)
+    e1.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    apply(d0, mu0, D0, base_vals)
+    e0.record(stream)
+    hs = adj.forward(K, ck, h=50.0)
+    e1.record(stream)
+    e1.synchronize()
+    fwd_ck_ms = e0.elapsed_time(e1)
+    ne = tree.download(0, "dens", 0)
+    adj.set_cotangent(0, 0, (ne - target) * vol)
+    adj.set_cotangent(0, 1, np.zeros_like(ne))
+    e0.record(stream)
+    g = adj.backward()
+    e1.record(stream)
+    e1.synchronize()
+    bwd_ms = e0.elapsed_time(e1)
+    # finite differences
+    eps, worst = 1e-6, 0.0
+    for _ in range(ndir):
+        dd = [np.zeros(spec.shape) for _ in range(2)]
+        for s in range(2):
+            dd[s][0, 2:-2, 2:-2] = smooth_direction(rng, spec.nz, spec.nr)
+        dmu, dD = rng.standard_normal(), rng.standard_normal()
+        dv = rng.standard_normal(base_vals.shape)
+        pred = sum(float(np.sum(g.dens0[0][s] * d0[s] * dd[s])) for s in range(2))
+        pred += g.mobility[0] * mu0 * dmu + g.diffusion * D0 * dD + float(np.sum(g.tables[0] * base_vals * dv))
+        outs = []
+        for sg in (1.0, -1.0):
+            apply([d0[s] * (1 + sg * eps * dd[s]) for s in range(2)], mu0 * (1 + sg * eps * dmu),
+                  D0 * (1 + sg * eps * dD), base_vals * (1 + sg * eps * dv))
+            adj.forward(K, ck, h_seq=hs)
+            outs.append(tree.download(0, "dens", 0))
+        fd = fd_objective_difference(outs[0], outs[1], target, vol, eps)
+        worst = max(worst, abs(fd - pred) / abs(fd))
+    tree.close()
+    return {"workload": "256x512 grid, 2 species (ions immobile), 64 RK2 steps, checkpoints every 8, "
+                        "gradients wrt n_e(0), n_i(0), mobility, diffusion, 256 table values",
+            "forward_ms": fwd_ms, "forward_with_checkpoints_ms": fwd_ck_ms, "adjoint_ms": bwd_ms,
+            "adjoint_over_forward": bwd_ms / fwd_ms, "fd_directions": ndir, "fd_step": eps,
+            "fd_max_rel_err": worst}
+
+
+def extra_kinetic(stream, K: int = 20):
+    """Kinetic batch: 32 instances of uneven sizes, 6 species, 9 reactions
+    with 1000-entry tables, per-instance applied field; batched fused forward
+    in one launch per stage, and the adjoint of the total electron number at
+    T with respect to all rate tables."""
+    import numpy as np
+    from arcos_b200 import workloads
+    from arcos_b200.adjoint import Adjoint, cell_volume
+    from arcos_b200.cdr import CdrTree
+    from arcos_b200._lib import check
+    pb = workloads.kinetic_batch(n_inst=32)
+    tree = CdrTree(pb.params, pb.model, pb.specs, stream=stream.cuda_stream)
+    _load(tree, pb)
+    L, h = tree.L, tree.h
+    check(L.arcos_run_prepare(h, 50.0))
+    check(L.arcos_run_enqueue(h, 4))
+    e0, e1 = _events(stream)
+    e0.record(stream)
+    check(L.arcos_run_enqueue(h, K))
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    ns = pb.model.no_species
+    _load(tree, pb)
+    adj = Adjoint(tree)
+    Ka, ck = 16, 8
+    adj.forward(Ka, ck, h=50.0)
+    for g, sp in enumerate(pb.specs):
+        vol = cell_volume(sp, pb.params.dr(0), pb.params.dz(0))
+        adj.set_cotangent(g, 0, vol)
+        for s in range(1, ns):
+            adj.set_cotangent(g, s, np.zeros(sp.shape))
+    e0.record(stream)
+    gr = adj.backward()
+    e1.record(stream)
+    e1.synchronize()
+    bwd = e0.elapsed_time(e1)
+    tree.close()
+    return {"workload": f"{len(pb.specs)} instances, {pb.cells} cells, {ns} species, "
+                        f"{len(pb.model.reactions)} reactions (1000-entry tables)",
+            "cells": pb.cells, "ms_per_step": ms, "value": pb.cells * ns / (ms / 1e3),
+            "adjoint_steps": Ka, "adjoint_ms": bwd, "adjoint_over_forward": bwd / (ms * Ka),
+            "table_grad_norm": float(sum(np.linalg.norm(t) for t in gr.tables))}
+
+
 def run_device(args):
     import ctypes as C
 
@@ -277,8 +455,8 @@ def run_device(args):
         s2 += ev[1].elapsed_time(ev[2])
     s1 /= nk
     s2 /= nk
-    bytes_s1 = 8 * (2 * NS + 2) * cells          # reads n0[S], er, ez; writes d0[S]
-    bytes_s2 = 8 * (3 * NS + 2) * cells          # reads n0[S], d0[S], er, ez; writes n1[S]
+    bytes_s1 = 8 * (2 * NS + 2) * cells          # reads n0[S], er, ez; writes n*[S]
+    bytes_s2 = 8 * (3 * NS + 2) * cells          # reads n0[S], n*[S], er, ez; writes n1[S]
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fp:
@@ -332,6 +510,14 @@ def run_device(args):
            "h2d_bytes_per_step": NS * arr_bytes, "d2h_bytes_per_step": NS * arr_bytes,
            "steps": e2e_steps, "api": "arcos_upload + arcos_run(1 step) + arcos_download"}
 
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        for name, fn in (("amr_batched", extra_amr), ("adjoint", extra_adjoint),
+                         ("kinetic_batch", extra_kinetic)):
+            try:
+                extras[name] = fn(stream)
+            except Exception as exc:          # reported, the main line stands
+                extras[name] = {"error": f"{type(exc).__name__}: {exc}"}
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
@@ -349,7 +535,7 @@ def run_device(args):
                 "stage_kernel_ms": {"stage1": s1, "stage2": s2},
                 "tile_autotune_ms_per_step": {str(k): v for k, v in tune.items()},
                 "limiter": "bit-exact" if args.exact else "division-free (1e-12/step)",
-                "dt_last": hlast}
+                "dt_last": hlast, "extras": extras}
         print(json.dumps(line), flush=True)
     tree.close()
     if world > 1:
@@ -364,6 +550,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched-AMR, adjoint and kinetic-batch measurements")
     ap.add_argument("--exact", action="store_true", help="bit-exact flux limiter")
     ap.add_argument("--tile", type=int, default=None,
                     help="fixed tile shape (0: 32x16 cells, 1: 32x32); default: autotuned")

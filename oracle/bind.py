@@ -218,6 +218,10 @@ class PortTree(_TreeBase):
         h = self.lib.port_courant(C.byref(self.m), C.byref(self.grids[0]), C.byref(st))
         return h, st.value
 
+    def rk2_frozen(self, h: float):
+        """One cdr_rk2 step with exactly the step size h (no CFL limit)."""
+        self.lib.port_rk2_frozen(C.byref(self.m), C.byref(self.grids[0]), C.c_double(h))
+
     def calc_d_dens(self):
         self.lib.port_calc_d_dens(C.byref(self.m), C.byref(self.grids[0]))
 

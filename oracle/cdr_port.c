@@ -827,6 +827,27 @@ port_rk2 (const port_model *m, port_grid *root, double h, int *status)
   return h;
 }
 
+/* cdr_rk2 with the step size given (no CFL limit): the forward map the
+ * discrete adjoint differentiates, with the step sizes frozen to a recorded
+ * sequence. */
+void
+port_rk2_frozen (const port_model *m, port_grid *root, double h)
+{
+  port_grid *inter;
+  nonegative_r (m, root);
+  port_prepare (m, root);
+  port_calc_field (m, root, root);
+  port_calc_d_dens (m, root);
+  inter = like_tree (m, root, NULL);
+  update_r (m, root, inter, h);
+  port_prepare (m, inter);
+  port_calc_field (m, inter, root);
+  port_calc_d_dens (m, inter);
+  rk2_update_r (m, root, inter, h);
+  port_prepare (m, root);
+  free_tree (m, inter);
+}
+
 /* Single-grid derivative entry used for kernel-level parity: zero + reactions
  * + drift/diffusion on one grid. */
 void

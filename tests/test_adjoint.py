@@ -1,0 +1,209 @@
+"""Discrete adjoint of the fused RK2 step against central finite differences
+(step 1e-6 relative) of the forward map with the step sizes frozen to the
+recorded sequence: the device forward, and at a smaller size the CPU oracle
+(oracle/cdr_port.c, itself pinned to the reference sources).
+
+The objective is J = 1/2 sum (n_e(T) - n_target)^2 * cell_volume with
+cell_volume = 2 pi r_i dr dz; the parameters are the initial electron and
+ion densities, the electron mobility 1/mass, diffusion_coeff and the alpha
+table values.
+"""
+import copy
+
+import numpy as np
+import pytest
+
+from arcos_b200 import workloads
+from arcos_b200.adjoint import Adjoint, cell_volume, fd_objective_difference, smooth_direction
+from arcos_b200.cdr import CdrTree
+from oracle import bind
+from parity_util import port_tree
+
+pytestmark = pytest.mark.gpu
+
+EPS = 1e-6
+TOL = 1e-6
+
+
+def problem(nr, nz, seed=0, ion_mass=0.0):
+    pb = workloads.plain(nr=nr, nz=nz, ion_mass=ion_mass, noise=1e-3, seed=seed)
+    return pb
+
+
+class Params:
+    """The differentiated inputs: densities (interior), mobility, D, table."""
+
+    def __init__(self, pb):
+        self.dens = [a.copy() for a in pb.dens[0]]
+        self.mu = np.array([1.0 / s.mass if s.mass > 0 else 0.0 for s in pb.model.species])
+        self.D = pb.params.diffusion_coeff
+        t = pb.model.reactions[0].table
+        self.table = np.array(t.values[: t.steps + 1], dtype=np.float64)
+
+    def perturbed(self, dirs, eps):
+        q = copy.deepcopy(self)
+        for s in range(len(q.dens)):
+            q.dens[s][0, 2:-2, 2:-2] *= 1.0 + eps * dirs["dens"][s]
+        q.mu = q.mu * (1.0 + eps * dirs["mu"])
+        q.D = q.D * (1.0 + eps * dirs["D"])
+        q.table = q.table * (1.0 + eps * dirs["table"])
+        return q
+
+
+def smooth_field(rng, nz, nr, modes=4):
+    return smooth_direction(rng, nz, nr, modes)
+
+
+def directions(pb, rng, which):
+    spec = pb.specs[0]
+    ns = pb.model.no_species
+    z = {"dens": [np.zeros((spec.nz, spec.nr)) for _ in range(ns)], "mu": np.zeros(ns), "D": 0.0,
+         "table": np.zeros(pb.model.reactions[0].table.steps + 1)}
+    if "dens" in which:
+        z["dens"] = [smooth_field(rng, spec.nz, spec.nr) for _ in range(ns)]
+    if "mu" in which:
+        z["mu"] = np.array([rng.standard_normal() if s.mass > 0 else 0.0 for s in pb.model.species])
+    if "D" in which:
+        z["D"] = rng.standard_normal()
+    if "table" in which:
+        z["table"] = rng.standard_normal(z["table"].shape)
+    return z
+
+
+def predicted(grads, base, dirs):
+    """sum_i dJ/dx_i * x_i * d_i for the relative perturbation x_i (1 + eps d_i)."""
+    v = 0.0
+    for s in range(len(base.dens)):
+        v += np.sum(grads.dens0[0][s][0, 2:-2, 2:-2] * base.dens[s][0, 2:-2, 2:-2] * dirs["dens"][s])
+    v += np.sum(grads.mobility * base.mu * dirs["mu"])
+    v += grads.diffusion * base.D * dirs["D"]
+    v += np.sum(grads.tables[0] * base.table * dirs["table"])
+    return v
+
+
+def apply_device(tree, pb, q):
+    for s, a in enumerate(q.dens):
+        tree.upload(0, "dens", a, s)
+    for s, sp in enumerate(pb.model.species):
+        if sp.mass > 0:
+            tree.set_species_mass(s, 1.0 / q.mu[s])
+    tree.set_diffusion(q.D)
+    t = pb.model.reactions[0].table
+    tree.set_table_values(0, q.table, t.underflow, t.overflow)
+
+
+def objective(ne, target, vol):
+    return 0.5 * float(np.sum((ne - target) ** 2 * vol))
+
+
+def device_setup(nr, nz, K, ck, seed=0):
+    pb = problem(nr, nz, seed=seed)
+    tree = CdrTree(pb.params, pb.model, pb.specs)
+    tree.set_fixed_field(pb.fields)
+    adj = Adjoint(tree)
+    base = Params(pb)
+    apply_device(tree, pb, base)
+    # target: forward run from a perturbed seed (amplitude x1.1, radius x0.9)
+    tgt = problem(nr, nz, seed=seed)
+    spec = pb.specs[0]
+    rng = np.random.default_rng(seed + 100)
+    tgt_e = workloads.seed_dens(spec, pb.params, rng, amp=0.11, sigma=0.09, noise=1e-3)
+    tree.upload(0, "dens", tgt_e, 0)
+    tree.upload(0, "dens", tgt_e, 1)
+    tree.run(K, 50.0)
+    target = tree.download(0, "dens", 0)
+    apply_device(tree, pb, base)
+    hs = adj.forward(K, ck, h=50.0)
+    vol = cell_volume(spec, pb.params.dr(0), pb.params.dz(0))
+    return pb, tree, adj, base, hs, target, vol
+
+
+def device_grads(tree, adj, target, vol):
+    ne = tree.download(0, "dens", 0)
+    lam = (ne - target) * vol
+    adj.set_cotangent(0, 0, lam)
+    adj.set_cotangent(0, 1, np.zeros_like(lam))
+    return adj.backward(), objective(ne, target, vol)
+
+
+def device_ne(tree, adj, pb, q, hs, K, ck):
+    apply_device(tree, pb, q)
+    adj.forward(K, ck, h_seq=hs)
+    return tree.download(0, "dens", 0)
+
+
+def fd_difference(ne_p, ne_m, target, vol, eps):
+    return fd_objective_difference(ne_p, ne_m, target, vol, eps)
+
+
+def device_J(tree, adj, pb, q, hs, K, ck, target, vol):
+    return objective(device_ne(tree, adj, pb, q, hs, K, ck), target, vol)
+
+
+@pytest.mark.parametrize("which", [("dens",), ("mu",), ("D",), ("table",), ("dens", "mu", "D", "table")])
+def test_adjoint_matches_device_fd(cuda_device, which):
+    K, ck = 16, 4
+    pb, tree, adj, base, hs, target, vol = device_setup(32, 64, K, ck, seed=1)
+    grads, J0 = device_grads(tree, adj, target, vol)
+    assert J0 > 0
+    rng = np.random.default_rng(7)
+    # A table-only direction moves n_e(T) by ~1e-11 relative at this size, so a
+    # 1e-6 step leaves the difference of the two runs at rounding level; the
+    # rate is linear in the table values, so a 1e-4 step has no truncation
+    # error to speak of.  Every other direction uses the 1e-6 step.
+    eps = 1e-4 if which == ("table",) else EPS
+    for _ in range(2):
+        dirs = directions(pb, rng, which)
+        ne_p = device_ne(tree, adj, pb, base.perturbed(dirs, eps), hs, K, ck)
+        ne_m = device_ne(tree, adj, pb, base.perturbed(dirs, -eps), hs, K, ck)
+        fd = fd_difference(ne_p, ne_m, target, vol, eps)
+        pr = predicted(grads, base, dirs)
+        assert abs(fd - pr) <= TOL * max(abs(fd), 1e-300), (which, fd, pr)
+
+
+def test_adjoint_matches_oracle_fd(cuda_device):
+    """FD of the CPU oracle's frozen-step forward against the device adjoint."""
+    K, ck, nr, nz = 8, 4, 24, 48
+    pb, tree, adj, base, hs, target, vol = device_setup(nr, nz, K, ck, seed=2)
+    grads, _ = device_grads(tree, adj, target, vol)
+
+    def oracle_ne(q):
+        pq = copy.deepcopy(pb)
+        pq.dens = [[a.copy() for a in q.dens]]
+        for s, sp in enumerate(pq.model.species):
+            if sp.mass > 0:
+                sp.mass = 1.0 / q.mu[s]
+        pq.params.diffusion_coeff = q.D
+        pq.model.reactions[0].table.values = q.table.copy()
+        port = port_tree(pq)
+        for k in range(K):
+            port.rk2_frozen(float(hs[0, k]))
+        return port.dens(0, 0).copy()
+
+    rng = np.random.default_rng(11)
+    for _ in range(2):
+        dirs = directions(pb, rng, ("dens", "mu", "D", "table"))
+        fd = fd_difference(oracle_ne(base.perturbed(dirs, EPS)), oracle_ne(base.perturbed(dirs, -EPS)),
+                           target, vol, EPS)
+        pr = predicted(grads, base, dirs)
+        assert abs(fd - pr) <= TOL * abs(fd), (fd, pr)
+
+
+def test_adjoint_keeps_forward_state(cuda_device):
+    K, ck = 6, 4
+    pb, tree, adj, base, hs, target, vol = device_setup(32, 64, K, ck, seed=3)
+    before = [tree.download(0, "dens", s) for s in range(2)]
+    device_grads(tree, adj, target, vol)
+    for s in range(2):
+        assert np.array_equal(tree.download(0, "dens", s)[0, 2:-2, 2:-2], before[s][0, 2:-2, 2:-2])
+
+
+def test_frozen_forward_reproduces_cfl_run(cuda_device):
+    """The frozen-step forward with the recorded sizes gives the CFL run's state."""
+    K, ck = 10, 4
+    pb, tree, adj, base, hs, target, vol = device_setup(32, 64, K, ck, seed=4)
+    a = [tree.download(0, "dens", s) for s in range(2)]
+    apply_device(tree, pb, base)
+    adj.forward(K, ck, h_seq=hs)
+    for s in range(2):
+        assert np.array_equal(tree.download(0, "dens", s)[0, 2:-2, 2:-2], a[s][0, 2:-2, 2:-2])
