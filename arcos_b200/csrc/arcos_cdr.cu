@@ -2347,6 +2347,110 @@ arcos_cdr_advect_vec_dev (double mass, double charge, const double *dens, double
   return seam_run (dens, d_dens, er, ez, cudaMemcpyDeviceToDevice, (cudaStream_t) stream);
 }
 
+// ---- the narrow seam without allocations ----------------------------------
+// All device memory of this entry point is one file-scope array: a header
+// (patch descriptor, E_theta flags, tile list) and the four padded arrays
+// the stencil kernel reads (dens, d_dens, er, ez).  Its address is looked up
+// once per device; every call re-writes what it uses, nothing has to start
+// at zero except the E_theta flags, which each call clears.
+constexpr size_t NOALLOC_DOUBLES = (size_t) 2 << 20;        // 16 MiB
+constexpr size_t NOALLOC_HEADER = 8192;                       // doubles (64 KiB)
+static __device__ __align__ (256) double g_noalloc_scratch[NOALLOC_DOUBLES];
+constexpr int NOALLOC_MAXDEV = 64;
+static double *g_noalloc_ptr[NOALLOC_MAXDEV];
+
+static int
+noalloc_setup (double **out)
+{
+  int dev = 0;
+  cudaError_t e = cudaGetDevice (&dev);
+  if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("cudaGetDevice: ") + cudaGetErrorString (e));
+  if (dev < 0 || dev >= NOALLOC_MAXDEV) return fail (ARCOS_ERR_ARG, "device index above 63");
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress (&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail (ARCOS_ERR_CUDA, std::string ("cudaGetSymbolAddress (scratch): ") + cudaGetErrorString (e));
+    g_noalloc_ptr[dev] = (double *) p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return ARCOS_OK;
+}
+
+int
+arcos_cdr_advect_vec_dev_noalloc (double mass, double charge, const double *dens, double *d_dens,
+                                  const double *er, const double *ez, double diffusion_coeff,
+                                  double dr, double dz, int r0, int r1, int z0, int z1, void *stream)
+{
+  if (mass <= 0) return ARCOS_OK;                    // .f90:82
+  if (r1 - r0 < 2 || z1 - z0 < 2 || !dens || !d_dens || !er || !ez)
+    return fail (ARCOS_ERR_ARG, "arcos_cdr_advect_vec_dev_noalloc: bad slab");
+  const int nr = r1 - r0, nz = z1 - z0;
+  const int pitch = (nr + 6 + 3) / 4 * 4;
+  const size_t asz = (size_t) pitch * (nz + 4);
+  constexpr int ty = TILE_WY[0] * TILE_RPW[0];
+  const size_t n_items = (size_t) ((nr + TX - 1) / TX) * ((nz + ty - 1) / ty);
+  const size_t head_bytes = 256 + 256 + sizeof (WorkItem) * n_items;
+  if (NOALLOC_HEADER + 4 * asz > NOALLOC_DOUBLES || head_bytes > sizeof (double) * NOALLOC_HEADER)
+    return fail (ARCOS_ERR_ARG, "arcos_cdr_advect_vec_dev_noalloc: slab larger than the 16 MiB static "
+                                "scratch (at most 4 padded arrays of (nr+6 rounded to 4) x (nz+4) doubles "
+                                "plus the tile list); use arcos_cdr_advect_vec_dev");
+  double *scr = nullptr;
+  int r = noalloc_setup (&scr);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t) stream;
+  // header: [PatchDesc @0 | etz flags @256 B | tiles @512 B], arrays after NOALLOC_HEADER doubles
+  char *head = (char *) scr;
+  PatchDesc P{};
+  P.nr = nr; P.nz = nz; P.ntheta = 1; P.planes = 1;
+  P.r0 = r0; P.z0 = z0; P.level = 0; P.ext_bound = 0;
+  P.pitch = pitch; P.ns = 1; P.theta0 = 0; P.parent = -1;
+  P.plane_stride = (long long) pitch * (nz + 4);
+  P.asz = (long long) asz;
+  P.dr = dr; P.dz = dz;                              // the slab's own spacing (cdr.c:947)
+  P.base = scr + NOALLOC_HEADER;
+  P.fam = 0;
+  static WorkItem items[(sizeof (double) * NOALLOC_HEADER - 512) / sizeof (WorkItem)];
+  int ni = 0;
+  for (int zb = 0; zb < nz; zb += ty)
+    for (int c0 = 0; c0 < nr; c0 += TX) items[ni++] = WorkItem{0, 0, c0, std::min (TX, nr - c0), zb, std::min (ty, nz - zb)};
+  CK (cudaMemcpyAsync (head, &P, sizeof (P), cudaMemcpyHostToDevice, st));
+  CK (cudaMemsetAsync (head + 256, 0, 2 * sizeof (int), st));
+  CK (cudaMemcpyAsync (head + 512, items, sizeof (WorkItem) * ni, cudaMemcpyHostToDevice, st));
+  const size_t w = sizeof (double) * (nr + 4), hgt = (size_t) (nz + 4), dp = sizeof (double) * pitch;
+  CK (cudaMemcpy2DAsync (P.arr (0, K_DENS, 0), dp, dens, w, w, hgt, cudaMemcpyDeviceToDevice, st));
+  CK (cudaMemcpy2DAsync (P.arr (0, K_DDENS, 0), dp, d_dens, w, w, hgt, cudaMemcpyDeviceToDevice, st));
+  CK (cudaMemcpy2DAsync (P.arr (0, K_ER), dp, er, w, w, hgt, cudaMemcpyDeviceToDevice, st));
+  CK (cudaMemcpy2DAsync (P.arr (0, K_EZ), dp, ez, w, w, hgt, cudaMemcpyDeviceToDevice, st));
+  Model M{};
+  M.ns = 1; M.nreact = 0;
+  M.mobile[0] = 1; M.charge[0] = charge; M.mass[0] = mass;
+  M.diffusion_coeff = diffusion_coeff;
+  M.z_cutoff = 1e7;
+  M.bnd_sign[1] = M.bnd_sign[2] = M.bnd_sign[3] = 1;
+  M.per_plane = 1;
+  StageArgs A{};
+  A.patches = (const PatchDesc *) head;
+  A.items = (const WorkItem *) (head + 512);
+  A.n_items = ni;
+  A.nset = 0; A.dset = 0; A.accumulate = 1;
+  A.etz = (const int *) (head + 256);
+  A.exact = 1;                                       // the Fortran kernel's arithmetic exactly
+  A.stage_eabs = 0;
+  A.maps = nullptr;                                  // cp.async staging
+  int occ = 0;
+  cudaError_t e = launch_stage (M_DERIV, 1, 0, M, A, 0, 0, &occ);
+  if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("occupancy: ") + cudaGetErrorString (e));
+  int dev = 0, sms = 148;
+  cudaGetDevice (&dev);
+  cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = std::min (ni, std::max (1, occ) * sms);
+  e = launch_stage (M_DERIV, 1, 0, M, A, blocks, st);
+  if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("stage launch: ") + cudaGetErrorString (e));
+  CK (cudaMemcpy2DAsync (d_dens, w, P.arr (0, K_DDENS, 0), dp, w, hgt, cudaMemcpyDeviceToDevice, st));
+  return ARCOS_OK;
+}
+
 void
 arcos_cdr_advect_vec (double mass, double charge, double *dens_array, double *d_dens_array,
                       double *er_array, int er_len, double *ez_array, int ez_len,

@@ -252,6 +252,21 @@ int arcos_cdr_advect_vec_dev (double mass, double charge, const double *dens,
                               double *d_dens, const double *er, const double *ez,
                               double diffusion_coeff, double dr, double dz,
                               int r0, int r1, int z0, int z1, void *stream);
+/* No reference counterpart.  arcos_cdr_advect_vec_dev without any device
+ * allocation, for callers that cannot allocate device memory (a process whose
+ * caching allocator already holds the GPU's memory, or code that must not
+ * take cudaMalloc's implicit device synchronisation): all device memory is
+ * one static 16 MiB array inside the library (the slab's four padded arrays,
+ * (nr+6 rounded up to 4) x (nz+4) doubles each, plus the tile list), whose
+ * address is looked up on the first call for each device, with that device
+ * current.  Larger slabs return ARCOS_ERR_ARG.  Asynchronous on `stream`;
+ * the scratch is shared, so calls that overlap (two streams, two threads, or
+ * two devices' calls racing on the per-device lookup) race; make the first
+ * call on a device before any stream capture, since it does the lookup. */
+int arcos_cdr_advect_vec_dev_noalloc (double mass, double charge, const double *dens,
+                                      double *d_dens, const double *er, const double *ez,
+                                      double diffusion_coeff, double dr, double dz,
+                                      int r0, int r1, int z0, int z1, void *stream);
 
 #ifdef __cplusplus
 }
