@@ -12,8 +12,9 @@ from typing import Dict, Optional
 
 from ._lib import check
 
-N_TILE_SHAPES = 2
-TILE_SHAPES = {0: "32 x 16 cells, 128 threads", 1: "32 x 16 cells, 256 threads (2 rows/warp pair)"}
+N_TILE_SHAPES = 3
+TILE_SHAPES = {0: "32 x 16 cells, 128 threads", 1: "32 x 32 cells, 256 threads",
+               2: "32 x 16 cells, 256 threads"}
 
 
 def autotune_tiles(tree, steps: int = 6, h: float = 50.0, stream=None) -> Dict[int, float]:

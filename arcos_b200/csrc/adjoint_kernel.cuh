@@ -108,20 +108,46 @@ struct VjpArgs {
   double gdz;
 };
 
-// Adds g to a table-gradient entry, one atomic per warp when every lane
-// targets the same entry.
+// Adds g to entry idx of a table gradient (idx < 0 or g == 0: nothing); one
+// atomic per warp when every contributing lane targets the same entry.
 __device__ __forceinline__ void
 warp_add (double *base, int idx, double g)
 {
-  const int i0 = __shfl_sync (0xffffffffu, idx, 0);
-  if (__all_sync (0xffffffffu, idx == i0)) {
+  const bool on = idx >= 0 && g != 0.0;
+  const unsigned act = __ballot_sync (0xffffffffu, on);
+  if (!act) return;
+  const int leader = __ffs (act) - 1;
+  const int i0 = __shfl_sync (0xffffffffu, idx, leader);
+  if (__all_sync (0xffffffffu, !on || idx == i0)) {
+    double v = on ? g : 0.0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync (0xffffffffu, g, o);
-    if ((threadIdx.x & 31) == 0 && i0 >= 0 && g != 0.0) atomicAdd (base + i0, g);
-  } else if (idx >= 0 && g != 0.0) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync (0xffffffffu, v, o);
+    if ((int) (threadIdx.x & 31) == leader) atomicAdd (base + i0, v);
+  } else if (on) {
     atomicAdd (base + idx, g);
   }
 }
+
+// Run-length cache of one reaction's table-gradient contributions: a lane
+// keeps adding while its cells land on the same node pair (a smooth field
+// keeps them there for many rows) and the warp flushes when any lane moves.
+struct TabCache {
+  int i_lo, i_ex;
+  double lo, hi, ex;
+  __device__ void reset () { i_lo = -1; i_ex = -1; lo = hi = ex = 0.0; }
+  __device__ void flush (double *base) {
+    warp_add (base, i_lo, lo);
+    warp_add (base, i_lo >= 0 ? i_lo + 1 : -1, hi);
+    warp_add (base, i_ex, ex);
+    reset ();
+  }
+  __device__ void add (double *base, int il, double gl, double gh, int ie, double ge) {
+    const bool moved = (il >= 0 && i_lo >= 0 && il != i_lo) || (ie >= 0 && i_ex >= 0 && ie != i_ex);
+    if (__any_sync (0xffffffffu, moved)) flush (base);
+    if (il >= 0) { i_lo = il; lo += gl; hi += gh; }
+    if (ie >= 0) { i_ex = ie; ex += ge; }
+  }
+};
 
 template <int NS, int WY, int BAND>
 __global__ void __launch_bounds__ (32 * WY)
@@ -132,6 +158,10 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
   double gmu[NS], gD = 0.0;
 #pragma unroll
   for (int s = 0; s < NS; s++) gmu[s] = 0.0;
+  constexpr int NCACHE = 12;                 // reactions with a run-length cache; later ones add directly
+  TabCache tc[NCACHE];
+#pragma unroll
+  for (int r = 0; r < NCACHE; r++) tc[r].reset ();
 
   for (int ti = blockIdx.x; ti < A.n_tiles; ti += gridDim.x) {
     const AdjTile T = A.tiles[ti];
@@ -193,8 +223,9 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
       for (int s = 0; s < NS; s++) wz_lo[s] = W (s, c, a_begin - 1);
     }
 
-#pragma unroll 1
-    for (int a = a_begin; a <= rb0 + BAND + 1; a++) {
+#pragma unroll
+    for (int ai = 0; ai < BAND + 3; ai++) {
+      const int a = a_begin + ai;
       // shift the window: slots hold rows a-2 .. a+1
 #pragma unroll
       for (int s = 0; s < NS; s++) {
@@ -368,9 +399,12 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
               g_ex = gr;
             }
           }
-          warp_add (A.g_table, i_lo, g_lo);
-          warp_add (A.g_table, i_lo >= 0 ? i_lo + 1 : -1, g_hi);
-          warp_add (A.g_table, i_ex, g_ex);
+          if (r < NCACHE) tc[r].add (A.g_table, i_lo, g_lo, g_hi, i_ex, g_ex);
+          else {
+            warp_add (A.g_table, i_lo, g_lo);
+            warp_add (A.g_table, i_lo >= 0 ? i_lo + 1 : -1, g_hi);
+            warp_add (A.g_table, i_ex, g_ex);
+          }
         }
       }
       if (own) {
@@ -388,6 +422,8 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
     }
   }
 
+#pragma unroll 1
+  for (int r = 0; r < NCACHE && r < M.nreact; r++) tc[r].flush (A.g_table);
   // ---- block partial sums of the mobility and diffusion gradients ----
 #pragma unroll
   for (int s = 0; s < NS; s++)
@@ -406,14 +442,6 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
     for (int w = 0; w < WY; w++) v += red[w][t];
     A.g_part[(size_t) blockIdx.x * (NS + 1) + t] += v;
   }
-}
-
-// Frozen step sizes: st[f].h = hs[f * stride + k].
-__global__ void
-k_set_h (DevState *st, int nfam, const double *hs, int stride, int k)
-{
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f < nfam) st[f].h = hs[(size_t) f * stride + k];
 }
 
 }  // namespace arcos

@@ -44,7 +44,7 @@ fail (int code, const std::string &msg)
       return fail (ARCOS_ERR_CUDA, std::string ("kernel launch: ") + cudaGetErrorString (e_)); \
   } while (0)
 
-constexpr int N_TILE_CFG_MAX = 2;
+constexpr int N_TILE_CFG_MAX = 3;
 
 struct GridH {
   int r0, z0, r1, z1, ntheta, level, ext_bound, parent, fam;
@@ -121,6 +121,7 @@ struct Ctx {
   int adj_ntiles = 0, adj_blocks = 0;
   int adj_lam = 0;                    // lam buffer holding the current cotangent
   bool adj_fwd = false;
+  cudaGraphExec_t adj_graph = nullptr;   // the whole reverse sweep
   int occ_fused[2][2][N_TILE_CFG_MAX] = {};   // [stage_eabs][stage 2][tile]
 };
 
@@ -206,9 +207,9 @@ constexpr int NODES_SMEM_MAX = 4 * 1024 / (int) sizeof (TableNode);
 
 // Tile shapes the autotuner chooses from: (warps per block, rows per thread);
 // tiles are 32 columns wide and WY * RPW rows high.
-constexpr int N_TILE_CFG = 2;
-constexpr int TILE_WY[N_TILE_CFG] = {4, 8};
-constexpr int TILE_RPW[N_TILE_CFG] = {4, 4};
+constexpr int N_TILE_CFG = 3;
+constexpr int TILE_WY[N_TILE_CFG] = {4, 8, 8};
+constexpr int TILE_RPW[N_TILE_CFG] = {4, 4, 2};
 
 template <int NS, int MODE, int WY, int RPW>
 size_t
@@ -242,8 +243,10 @@ launch_stage_c (int cfg, const Model &M, const StageArgs &A, int blocks, cudaStr
   switch (cfg) {
   case 0: return fast ? launch_stage_t<NS, MODE, 4, 4, true> (M, A, blocks, s, occ)
                       : launch_stage_t<NS, MODE, 4, 4, false> (M, A, blocks, s, occ);
-  default: return fast ? launch_stage_t<NS, MODE, 8, 4, true> (M, A, blocks, s, occ)
-                       : launch_stage_t<NS, MODE, 8, 4, false> (M, A, blocks, s, occ);
+  case 1: return fast ? launch_stage_t<NS, MODE, 8, 4, true> (M, A, blocks, s, occ)
+                      : launch_stage_t<NS, MODE, 8, 4, false> (M, A, blocks, s, occ);
+  default: return fast ? launch_stage_t<NS, MODE, 8, 2, true> (M, A, blocks, s, occ)
+                       : launch_stage_t<NS, MODE, 8, 2, false> (M, A, blocks, s, occ);
   }
 }
 
@@ -296,7 +299,8 @@ launch_fused_c (int cfg, const Model &M, const FusedArgs &A, int blocks, cudaStr
 {
   switch (cfg) {
   case 0: return launch_fused_t<NS, S2, 4, 4> (M, A, blocks, s, occ);
-  default: return launch_fused_t<NS, S2, 8, 4> (M, A, blocks, s, occ);
+  case 1: return launch_fused_t<NS, S2, 8, 4> (M, A, blocks, s, occ);
+  default: return launch_fused_t<NS, S2, 8, 2> (M, A, blocks, s, occ);
   }
 }
 
@@ -435,10 +439,15 @@ fused_args (Ctx *c)
 }
 
 int
-run_fused (Ctx *c, bool s2, int fold, int fam_state = 1)
+run_fused (Ctx *c, bool s2, int fold, int fam_state = 1, int frozen_k = -1)
 {
   FusedArgs A = fused_args (c);
   if (s2) { A.fam_state = fam_state; A.cfl_fold = fold; }
+  if (frozen_k >= 0) {                  // step sizes frozen to the adjoint's record
+    A.h_seq = c->adj_hs_d;
+    A.h_stride = c->adj_nsteps;
+    A.h_k = frozen_k;
+  }
   int &o = c->occ_fused[c->stage_eabs][s2 ? 1 : 0][c->tile_cfg];
   if (o == 0) {
     int b = 0;
@@ -630,6 +639,7 @@ refresh_stage_eabs (Ctx *c)
     c->stage_eabs = any;
     if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
   if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
+  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
   }
   return ARCOS_OK;
 }
@@ -820,7 +830,7 @@ rk2_fused_launches (Ctx *c, int src, int fold)
 
 
 // ---- discrete adjoint -----------------------------------------------------------
-constexpr int ADJ_WY = 4, ADJ_BAND = 16;
+constexpr int ADJ_WY = 4, ADJ_BAND = 4;
 
 inline int adj_lam_idx (Ctx *c, int which) { return which * c->M.ns; }
 inline int adj_lams_idx (Ctx *c) { return 2 * c->M.ns; }
@@ -847,6 +857,7 @@ adj_alloc (Ctx *c, int nsteps, int ck)
 {
   const int ns = c->M.ns;
   if (c->adj_pool && c->adj_nsteps == nsteps && c->adj_ck == ck) return ARCOS_OK;
+  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
   cudaFree (c->adj_pool); c->adj_pool = nullptr;
   cudaFree (c->adj_hs_d); c->adj_hs_d = nullptr;
   c->adj_nsteps = nsteps;
@@ -897,11 +908,9 @@ adj_alloc (Ctx *c, int nsteps, int ck)
 int
 adj_frozen_step (Ctx *c, int k, bool s2)
 {
-  k_set_h<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->st_d, c->nfam, c->adj_hs_d, c->adj_nsteps, k);
-  CKL ();
-  int r = run_fused (c, false, 0);
+  int r = run_fused (c, false, 0, 1, k);
   if (r || !s2) return r;
-  return run_fused (c, true, 0, 0);
+  return run_fused (c, true, 0, 0, k);
 }
 
 int
@@ -950,6 +959,40 @@ run_vjp (Ctx *c, int mode, int st_idx, int lam_idx, int lams_idx, int out_idx, i
   e = cudaGetLastError ();
   if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("vjp launch: ") + cudaGetErrorString (e));
   return ARCOS_OK;
+}
+
+// Enqueues the reverse sweep (graph-capturable: no host synchronisation):
+// per segment, last first, the recomputation from its checkpoint keeping n0
+// and n* of every step, then the transposed steps; the state ends where the
+// forward run left it.
+int
+adj_enqueue_sweep (Ctx *c)
+{
+  int r;
+  const int ns = c->M.ns;
+  const size_t ng = c->nodes_h.size () + 2 * (size_t) c->M.nreact;
+  CK (cudaMemsetAsync (c->adj_gtab_d, 0, sizeof (double) * std::max<size_t> (ng, 1), c->stream));
+  CK (cudaMemsetAsync (c->adj_gpart_d, 0, sizeof (double) * (size_t) c->adj_blocks * (ns + 1), c->stream));
+  int lam = 0;
+  for (int seg = c->adj_nseg - 1; seg >= 0; seg--) {
+    const int k0 = seg * c->adj_ck, k1 = std::min (c->adj_nsteps, k0 + c->adj_ck);
+    if ((r = adj_copy (c, false, 0, adj_ckpt (c, seg)))) return r;
+    for (int k = k0; k < k1; k++) {
+      if ((r = adj_copy (c, true, 0, adj_seg_n0 (c, k - k0)))) return r;
+      if ((r = adj_frozen_step (c, k, false))) return r;
+      if ((r = adj_copy (c, true, 1, adj_seg_ns (c, k - k0)))) return r;
+      if (k + 1 < k1 && (r = run_fused (c, true, 0, 0, k))) return r;
+    }
+    for (int k = k1 - 1; k >= k0; k--) {
+      if ((r = run_vjp (c, 1, adj_seg_ns (c, k - k0), adj_lam_idx (c, lam), 0, adj_lams_idx (c), k))) return r;
+      if ((r = run_vjp (c, 2, adj_seg_n0 (c, k - k0), adj_lam_idx (c, lam), adj_lams_idx (c),
+                        adj_lam_idx (c, 1 - lam), k))) return r;
+      lam = 1 - lam;
+    }
+  }
+  if ((r = adj_copy (c, false, 0, adj_final (c)))) return r;
+  if ((r = do_ext_bnd (c, 0))) return r;
+  return do_periodic (c, 0, 1);
 }
 
 int
@@ -1026,6 +1069,7 @@ arcos_destroy (void *ctx)
   if (!c) return ARCOS_OK;
   if (c->graph2) cudaGraphExecDestroy (c->graph2);
   if (c->graph_tree) cudaGraphExecDestroy (c->graph_tree);
+  if (c->adj_graph) cudaGraphExecDestroy (c->adj_graph);
   cudaFree (c->colfac_d);
   cudaFree (c->lean_nodes_d);
   cudaFree (c->adj_pool); cudaFree (c->adj_hs_d); cudaFree (c->adj_gtab_d);
@@ -1049,6 +1093,7 @@ arcos_set_stream (void *ctx, void *stream)
   c->stream = stream ? (cudaStream_t) stream : c->own_stream;
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
   if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
+  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
   return ARCOS_OK;
 }
 
@@ -1301,6 +1346,7 @@ build_items (Ctx *c)
   CK (cudaMemcpy (c->items_d, items.data (), sizeof (WorkItem) * items.size (), cudaMemcpyHostToDevice));
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
   if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
+  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
   return build_maps (c, ty);
 }
 
@@ -1635,6 +1681,7 @@ arcos_set_field_fn (void *ctx, arcos_field_fn fn, void *user)
   c->user = user;
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
   if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
+  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
   return ARCOS_OK;
 }
 
@@ -1646,6 +1693,7 @@ arcos_set_per_patch (void *ctx, int on)
   c->per_patch = on != 0;
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
   if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
+  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
   return ARCOS_OK;
 }
 
@@ -2064,32 +2112,25 @@ arcos_adj_backward (void *ctx, double *grad_mobility, double *grad_diffusion, do
   if (!c->adj_fwd) return fail (ARCOS_ERR_STATE, "adjoint: run arcos_adj_forward first");
   const int ns = c->M.ns;
   const size_t ng = c->nodes_h.size () + 2 * (size_t) c->M.nreact;
-  CK (cudaMemsetAsync (c->adj_gtab_d, 0, sizeof (double) * std::max<size_t> (ng, 1), c->stream));
-  CK (cudaMemsetAsync (c->adj_gpart_d, 0, sizeof (double) * (size_t) c->adj_blocks * (ns + 1), c->stream));
-  int lam = c->adj_lam;
-  for (int seg = c->adj_nseg - 1; seg >= 0; seg--) {
-    const int k0 = seg * c->adj_ck, k1 = std::min (c->adj_nsteps, k0 + c->adj_ck);
-    // recompute the segment from its checkpoint, keeping n0 and n* of every step
-    if ((r = adj_copy (c, false, 0, adj_ckpt (c, seg)))) return r;
-    for (int k = k0; k < k1; k++) {
-      if ((r = adj_copy (c, true, 0, adj_seg_n0 (c, k - k0)))) return r;
-      if ((r = adj_frozen_step (c, k, false))) return r;
-      if ((r = adj_copy (c, true, 1, adj_seg_ns (c, k - k0)))) return r;
-      if (k + 1 < k1 && (r = run_fused (c, true, 0, 0))) return r;
-    }
-    // reverse sweep of the segment
-    for (int k = k1 - 1; k >= k0; k--) {
-      if ((r = run_vjp (c, 1, adj_seg_ns (c, k - k0), adj_lam_idx (c, lam), 0, adj_lams_idx (c), k))) return r;
-      if ((r = run_vjp (c, 2, adj_seg_n0 (c, k - k0), adj_lam_idx (c, lam), adj_lams_idx (c),
-                        adj_lam_idx (c, 1 - lam), k))) return r;
-      lam = 1 - lam;
-    }
+  // the sweep starts from the cotangent in lam buffer 0
+  if (c->adj_lam != 0) {
+    for (auto &P : c->pd_h)
+      CK (cudaMemcpyAsync (P.adj + (size_t) adj_lam_idx (c, 0) * P.asz, P.adj + (size_t) adj_lam_idx (c, 1) * P.asz,
+                           sizeof (double) * P.asz * P.ns, cudaMemcpyDeviceToDevice, c->stream));
+    c->adj_lam = 0;
   }
-  c->adj_lam = lam;
-  // the state goes back to the end of the forward run
-  if ((r = adj_copy (c, false, 0, adj_final (c)))) return r;
-  if ((r = do_ext_bnd (c, 0))) return r;
-  if ((r = do_periodic (c, 0, 1))) return r;
+  if (!c->adj_graph) {
+    cudaGraph_t gr;
+    CK (cudaStreamBeginCapture (c->stream, cudaStreamCaptureModeThreadLocal));
+    int e = adj_enqueue_sweep (c);
+    cudaError_t ee = cudaStreamEndCapture (c->stream, &gr);
+    if (e) return e;
+    if (ee != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("adjoint graph capture: ") + cudaGetErrorString (ee));
+    CK (cudaGraphInstantiate (&c->adj_graph, gr, 0));
+    cudaGraphDestroy (gr);
+  }
+  CK (cudaGraphLaunch (c->adj_graph, c->stream));
+  c->adj_lam = c->adj_nsteps & 1;
   std::vector<double> gp ((size_t) c->adj_blocks * (ns + 1)), gt (std::max<size_t> (ng, 1));
   CK (cudaMemcpyAsync (gp.data (), c->adj_gpart_d, sizeof (double) * gp.size (), cudaMemcpyDeviceToHost, c->stream));
   CK (cudaMemcpyAsync (gt.data (), c->adj_gtab_d, sizeof (double) * gt.size (), cudaMemcpyDeviceToHost, c->stream));
@@ -2132,6 +2173,7 @@ drop_graphs (Ctx *c)
 {
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
   if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
+  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
 }
 
 int
@@ -2213,11 +2255,13 @@ arcos_set_exact (void *ctx, int on)
   c->exact = on ? 1 : 0;
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
   if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
+  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
   return ARCOS_OK;
 }
 
 // Tile shape of the stencil kernels (0: 32 x 16 cells, 128 threads; 1: 32 x 32
-// cells, 256 threads).  May be changed after arcos_commit.
+// cells, 256 threads; 2: 32 x 16 cells, 256 threads).  May be changed after
+// arcos_commit.
 int
 arcos_set_tile (void *ctx, int cfg)
 {
@@ -2238,6 +2282,7 @@ arcos_set_tma (void *ctx, int on)
   c->use_tma = on ? 1 : 0;
   if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
   if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
+  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
   if (c->committed) return build_maps (c, TILE_WY[c->tile_cfg] * TILE_RPW[c->tile_cfg]);
   return ARCOS_OK;
 }

@@ -55,6 +55,8 @@ struct FusedArgs {
   double ddz[FUSED_MAXS];    // (diffusion_coeff / mass) / dz (.f90:85,224)
   double gdz;                // 1 / dz (.f90:88)
   double dz;
+  const double *h_seq;       // frozen step sizes [fam][h_stride] (adjoint), or null: DevState h
+  int h_stride, h_k;
   // reaction program (react_apply, reaction.c:110-156, folded per species)
   int nreact;
   int r_node0[FUSED_MAXR];   // index of node 0 (the under sentinel sits before it)
@@ -126,13 +128,31 @@ face_o (double upup, double up, double dn, double v, double dd)
   return __fma_rn (up + aux, v, (POS ? -dd : dd) * d1);
 }
 
-// Orientation of a group of faces: 1 all v >= 0, 2 all v < 0, 0 mixed.
+// Sign votes of a warp's field values on a group of faces: bit 0 = every
+// value has a clear sign bit, bit 1 = every value has it set.
+template <int N>
 __device__ __forceinline__ int
-warp_orient (bool all_pos, bool all_neg)
+field_signs (const double (&e)[N])
 {
-  if (__all_sync (0xffffffffu, all_pos)) return 1;
-  if (__all_sync (0xffffffffu, all_neg)) return 2;
-  return 0;
+  bool p = true, n = true;
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    const bool sb = __double_as_longlong (e[j]) < 0;
+    p = p && !sb;
+    n = n && sb;
+  }
+  return (__all_sync (0xffffffffu, p) ? 1 : 0) | (__all_sync (0xffffffffu, n) ? 2 : 0);
+}
+
+// Orientation of a species' faces from the field signs: 1 all v = cm E >= 0,
+// 2 all v < 0, 0 mixed.  Where v is a signed zero the two orientations give
+// the same flux (the upwind value is multiplied by v), so the sign bit decides.
+__device__ __forceinline__ int
+species_orient (int signs, double cm)
+{
+  const bool pos_all = cm < 0.0 ? (signs & 2) : (signs & 1);
+  const bool neg_all = cm < 0.0 ? (signs & 1) : (signs & 2);
+  return pos_all ? 1 : (neg_all ? 2 : 0);
 }
 
 template <bool RADIAL>
@@ -192,7 +212,7 @@ fused_issue (const FusedArgs &A, int item, double *buf, int plane_doubles, unsig
     ti->n0[s] = P.arr (0, K_DENS, s) + o;
   }
   ti->chg = P.arr (0, K_CHARGE) + o;
-  ti->h = A.st[P.fam].h;
+  ti->h = A.h_seq ? A.h_seq[(size_t) P.fam * A.h_stride + A.h_k] : A.st[P.fam].h;
   ti->nr = P.nr; ti->nz = P.nz; ti->nt = P.ntheta; ti->pitch = P.pitch;
   ti->c0 = w.c0; ti->zb = w.zb; ti->width = w.width; ti->zlen = w.zlen; ti->plane = w.plane;
   ti->patch = w.patch; ti->fam = P.fam; ti->level = P.level; ti->etz = etz;
@@ -225,6 +245,26 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
   __syncthreads ();
 
   double dmax_local = -1.0;
+  int fam_cur = -1;                            // family whose max density dmax_local holds
+  // block max -> atomicMax of the family's next-step key (block-collective)
+  auto dmax_flush = [&] (int fam) {
+    unsigned long long key = dmax_local >= 0.0 ? dkey (dmax_local) : 0ULL;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long other = __shfl_xor_sync (0xffffffffu, key, o);
+      key = other > key ? other : key;
+    }
+    if (lane == 0) red_key[wq] = key;
+    __syncthreads ();
+    if (t == 0) {
+      unsigned long long kk = red_key[0];
+      for (int i = 1; i < WY; i++) kk = red_key[i] > kk ? red_key[i] : kk;
+      DevState *st = A.st + fam;
+      if (kk) atomicMax (&st->dmax_key[(st->step + 1) & 1], kk);
+    }
+    __syncthreads ();
+    dmax_local = -1.0;
+  };
   const int r_first = wq * RPW;
   const int sc = lane + 2;                     // own column in the staged rows
 
@@ -312,12 +352,27 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
                                &tinfo[(it + 1) & 1]);
 
     // ---- phase A: axial faces, reactions, the tile's right boundary faces ----
+    const bool active = lane < T.width;
+    const int pitch = T.pitch;
+    const long long ro = (long long) r_first * pitch + lane;
+    // stage 2 reads n0 at its own cells only; small species counts fetch it
+    // now so the loads overlap phase A
+    constexpr bool PRE = S2 && NS <= 2;
+    double n0pre[PRE ? NS : 1][PRE ? RPW : 1];
+    if (PRE) {
+#pragma unroll
+      for (int s = 0; s < (PRE ? NS : 1); s++)
+#pragma unroll
+        for (int k = 0; k < (PRE ? RPW : 1); k++)
+          n0pre[s][k] = (active && r_first + k < T.zlen) ? T.n0[s][ro + (long long) k * pitch] : 0.0;
+    }
     const double *sb = sm + (r_first + 2) * TXP + sc;             // (first own row, own column)
 #define SV(a_, k_, dr_, dc_) sb[(a_) * PL + ((k_) + (dr_)) * TXP + (dc_)]
     double ezw[RPW + 1];                    // ez rows r_first-1 .. r_first+RPW-1
 #pragma unroll
     for (int j = 0; j <= RPW; j++) ezw[j] = SV (NS + 1, j - 1, 0, 0);
     double fzt[RPW][NS], fzb[NS], acc[RPW][NS];
+    const int zsigns = field_signs (ezw);
 #pragma unroll
     for (int s = 0; s < NS; s++) {
       // face above row k (.f90:310-386) for k = 0..RPW-1, and (warp 0) below row 0
@@ -325,15 +380,10 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
 #pragma unroll
       for (int j = 0; j < RPW + 4; j++) nw[j] = SV (s, j - 2, 0, 0);
       double vz[RPW + 1];
-      bool ap = true, an = true;
       fzb[s] = 0.0;
 #pragma unroll
-      for (int j = 0; j <= RPW; j++) {
-        vz[j] = A.cm[s] * ezw[j];
-        ap = ap && vz[j] >= 0.0;
-        an = an && vz[j] < 0.0;
-      }
-      const int orient = warp_orient (ap, an);
+      for (int j = 0; j <= RPW; j++) vz[j] = A.cm[s] * ezw[j];
+      const int orient = species_orient (zsigns, A.cm[s]);
       const double dd = A.ddz[s];
       if (orient == 1) {
 #pragma unroll
@@ -350,13 +400,12 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       }
       if (wq < WY - 1) zt[wq][s][lane] = fzt[RPW - 1][s];
     }
-    if (wq == WY - 1) {
-      // radial faces right of column c0 + 31, lanes over (row, species)
-      for (int i = lane; i < TY * NS; i += 32) {
-        const int row = i % TY, s = i / TY;
-        const double *q = sm + s * PL + (row + 2) * TXP;
-        rb[s][row] = face_any<true> (0, q[32], q[33], q[34], q[35], A.cm[s] * sm[NS * PL + (row + 2) * TXP + 33], A.ddr[s]);
-      }
+    // radial faces right of column c0 + 31: every warp its own rows, lanes
+    // over (row, species)
+    for (int i = lane; i < RPW * NS; i += 32) {
+      const int row = r_first + i % RPW, s = i / RPW;
+      const double *q = sm + s * PL + (row + 2) * TXP;
+      rb[s][row] = face_any<true> (0, q[32], q[33], q[34], q[35], A.cm[s] * sm[NS * PL + (row + 2) * TXP + 33], A.ddr[s]);
     }
 #pragma unroll
     for (int k = 0; k < RPW; k++)
@@ -412,16 +461,17 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       for (int s = 0; s < NS; s++) fzb[s] = zt[wq - 1][s][lane];
     }
     const int c = c0 + lane;
-    const bool active = lane < T.width;
     const double erm = A.colfac[2 * c], erp = A.colfac[2 * c + 1];   // .f90:408-412
     const bool last = lane == 31;
-    const int pitch = T.pitch;
-    const long long ro = (long long) r_first * pitch + lane;
     const double h = T.h, hh = 0.5 * h;
     double erl[RPW];
-    bool ap = true, an = true;
 #pragma unroll
     for (int k = 0; k < RPW; k++) erl[k] = SV (NS, k, 0, -1);
+    const int rsigns = field_signs (erl);
+    if (S2 && A.fam_state && T.fam != fam_cur) {    // block-uniform
+      if (fam_cur >= 0) dmax_flush (fam_cur);
+      fam_cur = T.level == 0 ? T.fam : -1;
+    }
     double chg[RPW];
 #pragma unroll
     for (int k = 0; k < RPW; k++) chg[k] = 0.0;
@@ -432,17 +482,13 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
         const double *n0p = T.n0[s] + ro;
 #pragma unroll
         for (int k = 0; k < RPW; k++)
-          n0v[k] = (active && r_first + k < T.zlen) ? n0p[(long long) k * pitch] : 0.0;
+          n0v[k] = PRE ? n0pre[PRE ? s : 0][PRE ? k : 0]
+                       : ((active && r_first + k < T.zlen) ? n0p[(long long) k * pitch] : 0.0);
       }
       double vr[RPW];
-      ap = true; an = true;
 #pragma unroll
-      for (int k = 0; k < RPW; k++) {
-        vr[k] = A.cm[s] * erl[k];
-        ap = ap && vr[k] >= 0.0;
-        an = an && vr[k] < 0.0;
-      }
-      const int orient = warp_orient (ap, an);
+      for (int k = 0; k < RPW; k++) vr[k] = A.cm[s] * erl[k];
+      const int orient = species_orient (rsigns, A.cm[s]);
       const double dd = A.ddr[s];
       double *outp = T.out[s] + ro;
       const bool mob = M.mobile[s];
@@ -471,7 +517,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
             outp[(long long) k * pitch] = n1;
             if (A.want_charge) chg[k] += (n1 * M.charge[s]) / T.nt;     // cdr.c:380-381
             // max of the mobile densities; fmax drops NaN as the key reduction does
-            if (mob) dmax_local = fmax (dmax_local, clamp0 (n1));
+            if (mob && fam_cur >= 0) dmax_local = fmax (dmax_local, clamp0 (n1));
           }
         }
       }
@@ -484,25 +530,9 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
     }
 #undef SV
 #undef SM
-    // ---- block max of the mobile densities -> next step's CFL ----
-    if (S2 && A.fam_state && T.level == 0) {
-      unsigned long long key = dmax_local >= 0.0 ? dkey (dmax_local) : 0ULL;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        unsigned long long other = __shfl_xor_sync (0xffffffffu, key, o);
-        key = other > key ? other : key;
-      }
-      if (lane == 0) red_key[wq] = key;
-      __syncthreads ();
-      if (t == 0) {
-        unsigned long long kk = red_key[0];
-        for (int i = 1; i < WY; i++) kk = red_key[i] > kk ? red_key[i] : kk;
-        DevState *st = A.st + T.fam;
-        if (kk) atomicMax (&st->dmax_key[(st->step + 1) & 1], kk);
-      }
-      dmax_local = -1.0;
-    }
   }
+  // ---- block max of the mobile densities of the last family -> next step's CFL
+  if (S2 && A.fam_state && fam_cur >= 0) dmax_flush (fam_cur);
 
   // ---- the last block to finish starts the next step of every family ----
   if (S2 && A.cfl_fold) {
