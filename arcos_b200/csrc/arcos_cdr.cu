@@ -536,9 +536,12 @@ int
 do_ext_bnd (Ctx *c, int set)
 {
   const int np = (int) c->pd_h.size ();
-  if (!c->per_patch) k_ext_bnd<<<np, 256, 0, c->stream>>> (c->M, c->pd_d, c->plist_d, set);
+  int maxnt = 1;
+  for (auto &P : c->pd_h) maxnt = std::max (maxnt, P.ntheta);
+  if (!c->per_patch) k_ext_bnd<<<dim3 (np, maxnt, c->M.ns), 256, 0, c->stream>>> (c->M, c->pd_d, c->plist_d, set);
   else
-    for (int p = 0; p < np; p++) k_ext_bnd<<<1, 256, 0, c->stream>>> (c->M, c->pd_d, c->plist_d + p, set);
+    for (int p = 0; p < np; p++)
+      k_ext_bnd<<<dim3 (1, c->pd_h[p].ntheta, c->M.ns), 256, 0, c->stream>>> (c->M, c->pd_d, c->plist_d + p, set);
   CKL ();
   return ARCOS_OK;
 }

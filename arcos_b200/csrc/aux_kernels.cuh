@@ -111,47 +111,48 @@ k_charge_star (const Model M, const PatchDesc *pd, const int *plist, int src,
 __global__ void
 k_ext_bnd (const Model M, const PatchDesc *pd, const int *plist, int set)
 {
+  // one block per (patch, theta plane, species); the sides in the reference
+  // order, since the z sides copy the r sides' ghost columns (the corners)
   const PatchDesc &P = pd[plist[blockIdx.x]];
   const int nr = P.nr, nz = P.nz, nt = P.ntheta;
+  const int it = blockIdx.y, s = blockIdx.z;
+  if (it >= nt || s >= P.ns) return;
   const int t = threadIdx.x;
-  for (int s = 0; s < P.ns; s++) {
-    double *a = P.arr (set, K_DENS, s);
-    if (P.ext_bound & 1) {                           // axis
-      for (int i = t; i < (nz + 4) * nt; i += blockDim.x) {
-        const int iz = i % (nz + 4) - 2, it = i / (nz + 4);
-        const int it2 = (it + nt / 2) % nt;
-        a[P.off (-1, iz, it)] = a[P.off (0, iz, it2)];
-        a[P.off (-2, iz, it)] = a[P.off (1, iz, it2)];
-      }
+  double *a = P.arr (set, K_DENS, s);
+  if (P.ext_bound & 1) {                             // axis
+    const int it2 = (it + nt / 2) % nt;
+    for (int i = t; i < nz + 4; i += blockDim.x) {
+      const int iz = i - 2;
+      a[P.off (-1, iz, it)] = a[P.off (0, iz, it2)];
+      a[P.off (-2, iz, it)] = a[P.off (1, iz, it2)];
     }
-    __syncthreads ();
-    if (P.ext_bound & 2) {                           // r = r1
-      const double sg = (double) M.bnd_sign[1];
-      for (int i = t; i < (nz + 4) * nt; i += blockDim.x) {
-        const int iz = i % (nz + 4) - 2, it = i / (nz + 4);
-        a[P.off (nr, iz, it)] = sg * a[P.off (nr - 1, iz, it)];
-        a[P.off (nr + 1, iz, it)] = sg * a[P.off (nr - 2, iz, it)];
-      }
+  }
+  __syncthreads ();
+  if (P.ext_bound & 2) {                             // r = r1
+    const double sg = (double) M.bnd_sign[1];
+    for (int i = t; i < nz + 4; i += blockDim.x) {
+      const int iz = i - 2;
+      a[P.off (nr, iz, it)] = sg * a[P.off (nr - 1, iz, it)];
+      a[P.off (nr + 1, iz, it)] = sg * a[P.off (nr - 2, iz, it)];
     }
-    __syncthreads ();
-    if (P.ext_bound & 4) {                           // z = z0
-      const double sg = (double) M.bnd_sign[2];
-      for (int i = t; i < (nr + 4) * nt; i += blockDim.x) {
-        const int ir = i % (nr + 4) - 2, it = i / (nr + 4);
-        a[P.off (ir, -1, it)] = sg * a[P.off (ir, 0, it)];
-        a[P.off (ir, -2, it)] = sg * a[P.off (ir, 1, it)];
-      }
+  }
+  __syncthreads ();
+  if (P.ext_bound & 4) {                             // z = z0
+    const double sg = (double) M.bnd_sign[2];
+    for (int i = t; i < nr + 4; i += blockDim.x) {
+      const int ir = i - 2;
+      a[P.off (ir, -1, it)] = sg * a[P.off (ir, 0, it)];
+      a[P.off (ir, -2, it)] = sg * a[P.off (ir, 1, it)];
     }
-    __syncthreads ();
-    if (P.ext_bound & 8) {                           // z = z1
-      const double sg = (double) M.bnd_sign[3];
-      for (int i = t; i < (nr + 4) * nt; i += blockDim.x) {
-        const int ir = i % (nr + 4) - 2, it = i / (nr + 4);
-        a[P.off (ir, nz, it)] = sg * a[P.off (ir, nz - 1, it)];
-        a[P.off (ir, nz + 1, it)] = sg * a[P.off (ir, nz - 2, it)];
-      }
+  }
+  __syncthreads ();
+  if (P.ext_bound & 8) {                             // z = z1
+    const double sg = (double) M.bnd_sign[3];
+    for (int i = t; i < nr + 4; i += blockDim.x) {
+      const int ir = i - 2;
+      a[P.off (ir, nz, it)] = sg * a[P.off (ir, nz - 1, it)];
+      a[P.off (ir, nz + 1, it)] = sg * a[P.off (ir, nz - 2, it)];
     }
-    __syncthreads ();
   }
 }
 
