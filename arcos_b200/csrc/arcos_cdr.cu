@@ -764,7 +764,12 @@ reset_dmax (Ctx *c, int slot_rel)
   std::vector<DevState> st;
   int r = read_states (c, st);
   if (r) return r;
-  for (auto &s : st) s.dmax_key[(s.step + slot_rel) & 1] = dkey (-1.0);
+  for (auto &s : st) {
+    s.dmax_key[(s.step + slot_rel) & 1] = dkey (-1.0);
+    // a run starts from a state nobody has checked: the first stage clamps
+    s.neg[s.step & 1] = 1;
+    s.neg[(s.step + 1) & 1] = 0;
+  }
   CK (cudaMemcpyAsync (c->st_d, st.data (), sizeof (DevState) * c->nfam, cudaMemcpyHostToDevice, c->stream));
   CK (cudaStreamSynchronize (c->stream));
   return ARCOS_OK;

@@ -105,6 +105,7 @@ struct DevState {
   int small_dt_count;             // steps below warn_min_timestep
   int error;                      // sticky ARCOS_ERR_* bits (1 << code)
   unsigned int done_blocks;       // last-block detection in the stage-2 kernel
+  unsigned int neg[2];            // per step (ping-pong): the state may hold negative densities
   double courant_const[4];        // dr_min, dz_min, rdtheta_min, is_3d
   int dt_cap;                     // capacity of the dt log
   int pad_;

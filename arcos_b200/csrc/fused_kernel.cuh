@@ -90,6 +90,7 @@ struct TileInfo {
   double h;
   int nr, nz, nt, pitch, c0, zb, width, zlen, plane, patch, fam, level, etz, edge;
   int z0zb;                  // absolute index of the tile's first row (z cutoff)
+  int clamp;                 // stage 1: the state may hold negatives (cdr_nonegative has work)
 };
 
 __device__ __forceinline__ double
@@ -218,6 +219,9 @@ fused_issue (const FusedArgs &A, int item, double *buf, int plane_doubles, unsig
   ti->patch = w.patch; ti->fam = P.fam; ti->level = P.level; ti->etz = etz;
   ti->edge = (w.c0 == 0) || (w.c0 + 34 > P.nr) || (w.zb == 0) || (w.zb + TY + 2 > P.nz);
   ti->z0zb = P.z0 + w.zb;
+  // max(0, n) is the identity on a state without negatives (stage 2 of the
+  // previous step records whether it wrote any); frozen steps always clamp
+  ti->clamp = A.h_seq ? 1 : (int) A.st[P.fam].neg[A.st[P.fam].step & 1];
 }
 
 template <int NS, bool S2, int WY, int RPW>
@@ -245,8 +249,10 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
   __syncthreads ();
 
   double dmax_local = -1.0;
+  bool neg_local = false;                      // some n1 this thread wrote is negative
   int fam_cur = -1;                            // family whose max density dmax_local holds
-  // block max -> atomicMax of the family's next-step key (block-collective)
+  // block max -> atomicMax of the family's next-step key, and the family's
+  // negative-state flag for the next step (block-collective)
   auto dmax_flush = [&] (int fam) {
     unsigned long long key = dmax_local >= 0.0 ? dkey (dmax_local) : 0ULL;
 #pragma unroll
@@ -255,15 +261,17 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       key = other > key ? other : key;
     }
     if (lane == 0) red_key[wq] = key;
-    __syncthreads ();
+    const bool anyneg = __syncthreads_or (neg_local);
     if (t == 0) {
       unsigned long long kk = red_key[0];
       for (int i = 1; i < WY; i++) kk = red_key[i] > kk ? red_key[i] : kk;
       DevState *st = A.st + fam;
       if (kk) atomicMax (&st->dmax_key[(st->step + 1) & 1], kk);
+      if (anyneg) atomicOr (&st->neg[(st->step + 1) & 1], 1u);
     }
     __syncthreads ();
     dmax_local = -1.0;
+    neg_local = false;
   };
   const int r_first = wq * RPW;
   const int sc = lane + 2;                     // own column in the staged rows
@@ -286,11 +294,18 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
     const int nr = T.nr, nz = T.nz;
     const int zb = T.zb, c0 = T.c0;
     const bool edge = T.edge;
+    // shared-memory work before the stencil (block-uniform): the clamp of
+    // stage 1 and the ghost cells of edge tiles
+    const bool otf = edge || (!S2 && T.clamp);
+    if (!otf && t == 0 && item + (int) gridDim.x < A.n_items)
+      // every thread is past the previous tile: its buffer is free
+      fused_issue<NS, S2, TY> (A, item + gridDim.x, (it & 1) ? buf0 : buf1, PL, &bar[(it + 1) & 1],
+                               &tinfo[(it + 1) & 1]);
 
     // ---- stencil values: clamp n0 (stage 1), ghost cells from the boundary
     // conditions on edge tiles (prepare_grid, cdr.c:1334-1351) ----
     const int gr0 = zb - 2, gc0 = c0 - 2;
-    if (!S2) {
+    if (!S2 && T.clamp) {
       if (!edge) {
         double2 *v2 = reinterpret_cast<double2 *> (sm);
 #pragma unroll 4
@@ -343,13 +358,15 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
         }
       }
     }
-    // generic-proxy writes to this buffer before the async proxy refills it
-    asm volatile ("fence.proxy.async.shared::cta;\n" ::: "memory");
-    __syncthreads ();
-    // the other buffer is free (every thread is past the previous tile)
-    if (t == 0 && item + (int) gridDim.x < A.n_items)
-      fused_issue<NS, S2, TY> (A, item + gridDim.x, (it & 1) ? buf0 : buf1, PL, &bar[(it + 1) & 1],
-                               &tinfo[(it + 1) & 1]);
+    if (otf) {
+      // generic-proxy writes to this buffer before the async proxy refills it
+      asm volatile ("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncthreads ();
+      // the other buffer is free (every thread is past the previous tile)
+      if (t == 0 && item + (int) gridDim.x < A.n_items)
+        fused_issue<NS, S2, TY> (A, item + gridDim.x, (it & 1) ? buf0 : buf1, PL, &bar[(it + 1) & 1],
+                                 &tinfo[(it + 1) & 1]);
+    }
 
     // ---- phase A: axial faces, reactions, the tile's right boundary faces ----
     const bool active = lane < T.width;
@@ -518,6 +535,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
             if (A.want_charge) chg[k] += (n1 * M.charge[s]) / T.nt;     // cdr.c:380-381
             // max of the mobile densities; fmax drops NaN as the key reduction does
             if (mob && fam_cur >= 0) dmax_local = fmax (dmax_local, clamp0 (n1));
+            neg_local = neg_local || n1 < 0.0;
           }
         }
       }
@@ -547,6 +565,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
         DevState *st = A.st + f;
         const int k = st->step + 1;
         st->dmax_key[(k + 1) & 1] = dkey (-1.0);
+        st->neg[(k + 1) & 1] = 0u;
         st->step = k;
         cfl_step (st, M, k & 1, 0, k);
       }
