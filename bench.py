@@ -392,16 +392,10 @@ def run_device(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev_id = torch.cuda.current_device()
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    from arcos_b200.replicas import barrier, max_over_ranks
 
     def allmax(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(x, "cuda")
 
     pb = workloads.plain(nr=NR, nz=NZ, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=rank)
     stream = torch.cuda.Stream()
