@@ -12,19 +12,15 @@
 // differentiated branch by branch (a subgradient at its switch points, as
 // the forward's branch selection decides).
 //
-// One kernel evaluates J_F(n)^T w at every interior cell.  A warp owns a
-// strip of 28 output columns and a band of BAND rows: lane j computes the
-// radial face left of column c0 - 1 + j (32 faces cover the 31 faces that
-// touch the 28 cells), the four partial derivatives of every face flux
-// reach their cells by warp shuffles; axial faces are marched along the
-// band with a four-row register window.  Ghost-cell contributions fold back
-// onto the interior cells the boundary conditions mirror.
+// One kernel (k_vjp) evaluates J_F(n)^T w at every interior cell, a block
+// per 32 x 16 tile with its inputs staged in shared memory; each face flux
+// is differentiated once and its partial derivatives are gathered by the
+// cells they land on.  Ghost-cell contributions fold back onto the interior
+// cells the boundary conditions mirror.
 #pragma once
 #include "fused_kernel.cuh"
 
 namespace arcos {
-
-#define ADJ_STRIP 28
 
 // psi * dC of the division-free limiter (psi_dc_fast) and its partial
 // derivatives with respect to num and dC.
@@ -100,6 +96,7 @@ struct VjpArgs {
   const double *inv_de; // per node: 1 / (e2 - e1)
   double *g_table;      // [nodes] then [under, over] per reaction
   int n_nodes;
+  int tab_smem;         // accumulate the table gradients in shared memory (VjpTile::O_TAB)
   double *g_part;       // [gridDim.x][ns + 1]: mobility gradients, then diffusion
   const double *colfac;
   double cm[ARCOS_MAXS], ddr[ARCOS_MAXS], ddz[ARCOS_MAXS];
@@ -128,40 +125,80 @@ warp_add (double *base, int idx, double g)
   }
 }
 
-// Run-length cache of one reaction's table-gradient contributions: a lane
-// keeps adding while its cells land on the same node pair (a smooth field
-// keeps them there for many rows) and the warp flushes when any lane moves.
-struct TabCache {
-  int i_lo, i_ex;
-  double lo, hi, ex;
-  __device__ void reset () { i_lo = -1; i_ex = -1; lo = hi = ex = 0.0; }
-  __device__ void flush (double *base) {
-    warp_add (base, i_lo, lo);
-    warp_add (base, i_lo >= 0 ? i_lo + 1 : -1, hi);
-    warp_add (base, i_ex, ex);
-    reset ();
+// Keeps the state of a recomputed forward step for its transposed stages:
+// every species' density of set 0 (n0) and of set 1 (n*) of patch
+// blockIdx.y into its adjoint arrays i0 + s and is + s (whole arrays).
+__global__ void __launch_bounds__ (256)
+k_adj_keep (const PatchDesc *__restrict__ pd, int i0, int is)
+{
+  const PatchDesc &P = pd[blockIdx.y];
+  const long long n2 = P.asz / 2;           // asz is a multiple of 32
+  const long long stride = (long long) gridDim.x * blockDim.x;
+  for (int j = 0; j < 2 * P.ns; j++) {
+    const int set = j < P.ns ? 0 : 1, s = j < P.ns ? j : j - P.ns;
+    const double2 *src = reinterpret_cast<const double2 *> (P.arr (set, K_DENS, s));
+    double2 *dst = reinterpret_cast<double2 *> (P.adj + (long long) ((set ? is : i0) + s) * P.asz);
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride) dst[i] = src[i];
   }
-  __device__ void add (double *base, int il, double gl, double gh, int ie, double ge) {
-    const bool moved = (il >= 0 && i_lo >= 0 && il != i_lo) || (ie >= 0 && i_ex >= 0 && ie != i_ex);
-    if (__any_sync (0xffffffffu, moved)) flush (base);
-    if (il >= 0) { i_lo = il; lo += gl; hi += gh; }
-    if (ie >= 0) { i_ex = ie; ex += ge; }
-  }
+}
+
+// Shared-memory layout of one VJP tile: VX output columns x VY output rows.
+template <int NS>
+struct VjpTile {
+  static constexpr int VX = 32, VY = 16, NT = 256;
+  static constexpr int SC = VX + 6, SR = VY + 6;   // state: cols c0-3 .. c0+VX+2, rows j0-3 .. j0+VY+2
+  static constexpr int WC = VX + 4, WR = VY + 4;   // cotangent of F: cols c0-2 .., rows j0-2 ..
+  static constexpr int EC = VX + 3;                // er: cols c0-2 .. c0+VX, rows j0 .. j0+VY-1
+  static constexpr int ZR = VY + 3;                // ez: rows j0-2 .. j0+VY, cols c0 .. c0+VX-1
+  static constexpr int FR = VX + 3;                // radial faces ar = c0-1 .. c0+VX+1 of a row
+  static constexpr int FZ = VY + 3;                // axial faces a = j0-1 .. j0+VY+1 of a column
+  static constexpr int O_ST = 0;
+  static constexpr int O_W = O_ST + NS * SR * SC;
+  static constexpr int O_ER = O_W + NS * WR * WC;
+  static constexpr int O_EZ = O_ER + VY * EC;
+  static constexpr int O_PR = O_EZ + ZR * VX;      // [LL, L, R, RR][row][face]
+  static constexpr int O_PZ = O_PR + 4 * VY * FR;  // [LL, L, R, RR][face][column]
+  static constexpr int O_TAB = O_PZ + 4 * FZ * VX; // table-gradient accumulator (optional)
 };
 
-template <int NS, int WY, int BAND>
-__global__ void __launch_bounds__ (32 * WY)
+// out = J_F(n)^T w (mode 1) or [n0 > 0] (lam + lams + J_F(n0c)^T w) (mode 2)
+// over the tiles of A.tiles, w = h/2 lam (+ h lams in mode 2).
+//
+// Per tile: (1) every input the tile needs is staged in shared memory with
+// one batch of independent loads: the state with the ghost cells of the
+// boundary conditions (clamped in mode 2), w (zero off the interior), er
+// and ez.  (2) Per mobile species, every face flux that touches a cell of
+// the tile is differentiated once; its four partial derivatives, scaled by
+// the face's cotangent, go to shared memory.  (3) Each cell gathers the
+// partials that land on it, plus those that land on the ghost cells it
+// mirrors (axis, r = L_r, z = 0, z = L_z).  (4) Reactions per cell; table
+// gradients add into a shared accumulator (warp-aggregated) that is flushed
+// to A.g_table when the block ends.  The mobility and diffusion sums take
+// every face once (the tile holding the cell left of / below the face; the
+// last cell's tile for the faces at r = L_r and z = L_z).
+template <int NS>
+__global__ void __launch_bounds__ (256)
 k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
 {
+  using L = VjpTile<NS>;
+  constexpr int VX = L::VX, VY = L::VY, NT = L::NT;
+  constexpr int SC = L::SC, SR = L::SR, WC = L::WC, WR = L::WR, EC = L::EC, ZR = L::ZR;
+  constexpr int FR = L::FR, FZ = L::FZ;
+  extern __shared__ __align__ (16) double vsm[];
+  double *const sST = vsm + L::O_ST, *const sW = vsm + L::O_W;
+  double *const sER = vsm + L::O_ER, *const sEZ = vsm + L::O_EZ;
+  double *const sPR = vsm + L::O_PR, *const sPZ = vsm + L::O_PZ, *const sTab = vsm + L::O_TAB;
+  __shared__ double red[NT / 32][NS + 1];
   const int t = threadIdx.x, lane = t & 31, wq = t >> 5;
-  __shared__ double red[WY][NS + 1];
+  const int ntab = A.n_nodes + 2 * M.nreact;
+  double *const gtab = A.tab_smem ? sTab : A.g_table;
+  if (A.tab_smem)
+    for (int i = t; i < ntab; i += NT) sTab[i] = 0.0;
   double gmu[NS], gD = 0.0;
 #pragma unroll
   for (int s = 0; s < NS; s++) gmu[s] = 0.0;
-  constexpr int NCACHE = 12;                 // reactions with a run-length cache; later ones add directly
-  TabCache tc[NCACHE];
-#pragma unroll
-  for (int r = 0; r < NCACHE; r++) tc[r].reset ();
+  const int cc = lane;                          // own column in the tile
+  const int jA = wq;                            // own rows jA and jA + 8
 
   for (int ti = blockIdx.x; ti < A.n_tiles; ti += gridDim.x) {
     const AdjTile T = A.tiles[ti];
@@ -169,8 +206,7 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
     const int nr = Pp->nr, nz = Pp->nz, pitch = Pp->pitch;
     const long long asz = Pp->asz;
     double *adj = Pp->adj;
-    const int c0 = T.c0, rb0 = T.zb + wq * BAND;
-    if (rb0 >= nz) continue;                    // warp-uniform
+    const int c0 = T.c0, j0 = T.zb;
     const double h = A.hs[Pp->fam * A.hs_stride + A.k];
     const double a1 = 0.5 * h, b1 = (A.mode == 2) ? h : 0.0;
     const bool clampst = A.mode == 2;
@@ -178,178 +214,171 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
     const double sg_r = (double) M.bnd_sign[1], sg_b = (double) M.bnd_sign[2], sg_t = (double) M.bnd_sign[3];
     // element (col, row) of an adjoint-block array
     auto AO = [&] (int col, int row) -> long long { return (long long) (col + 2) + (long long) (row + 2) * pitch; };
-    // state with the boundary conditions of the ghost cells (no corners needed)
-    auto ST = [&] (int s, int col, int row) -> double {
-      double sg = 1.0;
+
+    __syncthreads ();                           // the previous tile is done with the shared arrays
+    // ---- (1) staging.  The state, lam, lams, er and ez arrays are read-only in
+    // this launch (the output array is a different one): non-coherent loads ----
+    for (int i = t; i < NS * SR * SC; i += NT) {
+      const int s = i / (SR * SC), rem = i - s * (SR * SC), yy = rem / SC, xx = rem - yy * SC;
+      int col = c0 - 3 + xx, row = j0 - 3 + yy;
+      double sg = 1.0;                          // ghost cells: no corners needed
       if (col < 0) { col = -1 - col; }                              // axis, 2-D
       else if (col >= nr) { col = 2 * nr - 1 - col; sg = sg_r; }
       if (row < 0) { row = -1 - row; sg = sg_b; }
       else if (row >= nz) { row = 2 * nz - 1 - row; sg = sg_t; }
-      double v = adj[(long long) (A.st_idx + s) * asz + AO (col, row)];
-      if (clampst) v = clamp0 (v);
-      return sg * v;
-    };
-    // cotangent of F at an interior cell (0 elsewhere)
-    auto W = [&] (int s, int col, int row) -> double {
-      if (col < 0 || col >= nr || row < 0 || row >= nz) return 0.0;
-      const long long o = AO (col, row);
-      double w = a1 * adj[(long long) (A.lam_idx + s) * asz + o];
-      if (A.mode == 2) w = __fma_rn (b1, adj[(long long) (A.lams_idx + s) * asz + o], w);
-      return w;
-    };
+      double v = 0.0;
+      if (col >= 0 && col < nr && row >= 0 && row < nz) {
+        v = __ldg (adj + (long long) (A.st_idx + s) * asz + AO (col, row));
+        if (clampst) v = clamp0 (v);
+        v = sg * v;
+      }
+      sST[i] = v;
+    }
+    for (int i = t; i < NS * WR * WC; i += NT) {
+      const int s = i / (WR * WC), rem = i - s * (WR * WC), yy = rem / WC, xx = rem - yy * WC;
+      const int col = c0 - 2 + xx, row = j0 - 2 + yy;
+      double w = 0.0;                           // cotangent of F at interior cells only
+      if (col >= 0 && col < nr && row >= 0 && row < nz) {
+        const long long o = AO (col, row);
+        w = a1 * __ldg (adj + (long long) (A.lam_idx + s) * asz + o);
+        if (A.mode == 2) w = __fma_rn (b1, __ldg (adj + (long long) (A.lams_idx + s) * asz + o), w);
+      }
+      sW[i] = w;
+    }
+    for (int i = t; i < VY * EC; i += NT) {
+      const int yy = i / EC, xx = i - yy * EC;
+      const int col = c0 - 2 + xx, row = j0 + yy;
+      sER[i] = (col >= -2 && col <= nr + 1 && row <= nz + 1) ? __ldg (er + Pp->off (col, row, 0)) : 0.0;
+    }
+    for (int i = t; i < ZR * VX; i += NT) {
+      const int yy = i / VX, xx = i - yy * VX;
+      const int col = c0 + xx, row = j0 - 2 + yy;
+      sEZ[i] = (col <= nr + 1 && row >= -2 && row <= nz + 1) ? __ldg (ez + Pp->off (col, row, 0)) : 0.0;
+    }
+    __syncthreads ();
 
-    const int c = c0 + lane;                      // own column (output lanes < 28)
-    const int ar = c0 - 1 + lane;                 // radial face ar - 1/2 of this lane
-    const bool zcol = c < nr;
-    // z window: state rows a-2 .. a+1 and accumulators of the same rows
-    double wn[4][NS], za[4][NS], wz_lo[NS];
+    double out[2][NS];
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+#pragma unroll
+      for (int s = 0; s < NS; s++) out[q][s] = 0.0;
+
+    // ---- (2), (3) drift-diffusion faces, one species at a time ----
 #pragma unroll
     for (int s = 0; s < NS; s++) {
-#pragma unroll
-      for (int q = 0; q < 4; q++) { wn[q][s] = 0.0; za[q][s] = 0.0; }
-      wz_lo[s] = 0.0;
-    }
-    const int a_begin = rb0 - 1;
-    // preload rows a_begin-2 .. a_begin (the window is completed with row a+1 in the loop)
-    if (zcol) {
-#pragma unroll
-      for (int q = 0; q < 3; q++) {
-        const int row = a_begin - 2 + q;
-        if (row >= -2 && row <= nz + 1)
-#pragma unroll
-          for (int s = 0; s < NS; s++) wn[q + 1][s] = ST (s, c, row);
-      }
-#pragma unroll
-      for (int s = 0; s < NS; s++) wz_lo[s] = W (s, c, a_begin - 1);
-    }
-
-#pragma unroll
-    for (int ai = 0; ai < BAND + 3; ai++) {
-      const int a = a_begin + ai;
-      // shift the window: slots hold rows a-2 .. a+1
-#pragma unroll
-      for (int s = 0; s < NS; s++) {
-        wn[0][s] = wn[1][s]; wn[1][s] = wn[2][s]; wn[2][s] = wn[3][s];
-        za[0][s] = za[1][s]; za[1][s] = za[2][s]; za[2][s] = za[3][s]; za[3][s] = 0.0;
-      }
-      const bool zreal = zcol && a >= 0 && a <= nz;
-      // the parameter sums take every face once: the band holding row a
-      // (row nz-1 for the top face) and the strip holding column c
-      const bool zown = lane < ADJ_STRIP && ((a >= rb0 && a < rb0 + BAND && a < nz)
-                                             || (a == nz && nz - 1 >= rb0 && nz - 1 < rb0 + BAND));
-#pragma unroll
-      for (int s = 0; s < NS; s++)
-        wn[3][s] = (zcol && a + 1 >= -2 && a + 1 <= nz + 1) ? ST (s, c, a + 1) : 0.0;
-      // ---- axial face a - 1/2 of column c ----
-      if (zreal) {
-        const double e = ez[Pp->off (c, a - 1, 0)];
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-          const double w_hi = W (s, c, a);
-          const double g = A.gdz * (w_hi - wz_lo[s]);      // F(a) += gdz Phi, F(a-1) -= gdz Phi
-          wz_lo[s] = w_hi;
-          if (!M.mobile[s] || g == 0.0) continue;
-          const FaceGrad fg = face_grad (false, wn[0][s], wn[1][s], wn[2][s], wn[3][s], A.cm[s] * e, A.ddz[s]);
-          za[0][s] = __fma_rn (g, fg.pLL, za[0][s]);
-          za[1][s] = __fma_rn (g, fg.pL, za[1][s]);
-          za[2][s] = __fma_rn (g, fg.pR, za[2][s]);
-          za[3][s] = __fma_rn (g, fg.pRR, za[3][s]);
-          if (zown) {
-            gmu[s] += g * (fg.dv * M.charge[s] * e + fg.ddd * A.Ddz);
-            gD += g * fg.ddd * A.mudz[s];
-          }
-        }
-      } else {
-#pragma unroll
-        for (int s = 0; s < NS; s++) wz_lo[s] = zcol ? W (s, c, a) : 0.0;
-      }
-      // ghost rows fold onto the rows they mirror
-      if (a == 0) {                                  // row -2 complete -> row 1
-#pragma unroll
-        for (int s = 0; s < NS; s++) { za[3][s] = __fma_rn (sg_b, za[0][s], za[3][s]); za[0][s] = 0.0; }
-      }
-      if (a == 1) {                                  // row -1 complete -> row 0
-#pragma unroll
-        for (int s = 0; s < NS; s++) { za[1][s] = __fma_rn (sg_b, za[0][s], za[1][s]); za[0][s] = 0.0; }
-      }
-      if (a == nz) {                                 // rows nz, nz+1 final -> nz-1, nz-2
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-          za[1][s] = __fma_rn (sg_t, za[2][s], za[1][s]);
-          za[0][s] = __fma_rn (sg_t, za[3][s], za[0][s]);
-          za[2][s] = 0.0; za[3][s] = 0.0;
-        }
-      }
-      // ---- row j = a - 2 is complete in z ----
-      const int j = a - 2;
-      if (j < rb0 || j >= rb0 + BAND || j >= nz) continue;     // warp-uniform
-      double out[NS];
-#pragma unroll
-      for (int s = 0; s < NS; s++) out[s] = za[0][s];
-      // radial faces of row j, lanes over faces ar - 1/2
-      {
-        const bool rreal = ar >= 0 && ar <= nr;
-        const bool rown = (ar >= c0 && ar < c0 + ADJ_STRIP && ar < nr)
-                          || (ar == nr && nr - 1 >= c0 && nr - 1 < c0 + ADJ_STRIP);
-        const double e = rreal ? er[Pp->off (ar - 1, j, 0)] : 0.0;
-        const double fm = (rreal && ar < nr) ? A.colfac[2 * ar] : 0.0;            // erm(ar)
-        const double fp = (rreal && ar >= 1) ? A.colfac[2 * (ar - 1) + 1] : 0.0;  // erp(ar-1)
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-          double pLL = 0.0, pL = 0.0, pR = 0.0, pRR = 0.0;
-          if (M.mobile[s] && rreal) {
-            const double g = fm * W (s, ar, j) - fp * W (s, ar - 1, j);
-            if (g != 0.0) {
-              const FaceGrad fg = face_grad (true, ST (s, ar - 2, j), ST (s, ar - 1, j), ST (s, ar, j),
-                                             ST (s, ar + 1, j), A.cm[s] * e, A.ddr[s]);
-              pLL = g * fg.pLL; pL = g * fg.pL; pR = g * fg.pR; pRR = g * fg.pRR;
-              if (rown) {
-                gmu[s] += g * (fg.dv * M.charge[s] * e + fg.ddd * A.Ddr);
-                gD += g * fg.ddd * A.mudr[s];
-              }
+      if (!M.mobile[s]) continue;               // block-uniform
+      for (int i = t; i < VY * FR; i += NT) {   // radial face ar - 1/2 of row j
+        const int jj = i / FR, fi = i - jj * FR;
+        const int ar = c0 - 1 + fi, j = j0 + jj;
+        double pLL = 0.0, pL = 0.0, pR = 0.0, pRR = 0.0;
+        if (ar >= 0 && ar <= nr && j < nz) {
+          const double fm = ar < nr ? A.colfac[2 * ar] : 0.0;             // erm(ar)
+          const double fp = ar >= 1 ? A.colfac[2 * (ar - 1) + 1] : 0.0;   // erp(ar-1)
+          const double *w = sW + (s * WR + jj + 2) * WC + fi;            // columns ar-1, ar
+          const double g = fm * w[1] - fp * w[0];
+          if (g != 0.0) {
+            const double *st = sST + (s * SR + jj + 3) * SC + fi;        // columns ar-2 .. ar+1
+            const double e = sER[jj * EC + fi];                          // er(ar-1, j)
+            const FaceGrad fg = face_grad (true, st[0], st[1], st[2], st[3], A.cm[s] * e, A.ddr[s]);
+            pLL = g * fg.pLL; pL = g * fg.pL; pR = g * fg.pR; pRR = g * fg.pRR;
+            if ((ar >= c0 && ar < c0 + VX && ar < nr) || (ar == nr && nr - 1 >= c0 && nr - 1 < c0 + VX)) {
+              gmu[s] += g * (fg.dv * M.charge[s] * e + fg.ddd * A.Ddr);
+              gD += g * fg.ddd * A.mudr[s];
             }
           }
-          // cell c0 + lane: RR of face lane, R of lane+1, L of lane+2, LL of lane+3
-          double acc = pRR + __shfl_down_sync (0xffffffffu, pR, 1);
-          acc += __shfl_down_sync (0xffffffffu, pL, 2);
-          acc += __shfl_down_sync (0xffffffffu, pLL, 3);
-          if (c0 == 0) {                             // axis ghosts -1, -2 -> cells 0, 1
-            const double l1 = __shfl_down_sync (0xffffffffu, pL, 1);
-            const double ll2 = __shfl_down_sync (0xffffffffu, pLL, 2);
-            if (lane == 0) acc += l1 + ll2;
-            if (lane == 1) acc += pLL;
-          }
-          if (c0 + ADJ_STRIP + 1 >= nr) {            // ghosts nr, nr+1 -> cells nr-1, nr-2
-            const int Lr = nr - 1 - c0;               // lane of cell nr-1 (may be 28: next strip)
-            const double rr1 = __shfl_down_sync (0xffffffffu, pRR, 1);
-            const double r2 = __shfl_down_sync (0xffffffffu, pR, 2);
-            const double rr3 = __shfl_down_sync (0xffffffffu, pRR, 3);
-            if (lane == Lr) acc = __fma_rn (sg_r, rr1 + r2, acc);
-            if (lane == Lr - 1) acc = __fma_rn (sg_r, rr3, acc);
-          }
-          out[s] += acc;
         }
+        double *pr = sPR + jj * FR + fi;
+        pr[0] = pLL; pr[VY * FR] = pL; pr[2 * VY * FR] = pR; pr[3 * VY * FR] = pRR;
       }
-      const bool own = lane < ADJ_STRIP && zcol;
-      // reactions (react_apply, folded form); every lane joins the warp-wide
-      // table-gradient reductions
+      for (int i = t; i < FZ * VX; i += NT) {   // axial face a - 1/2 of column c
+        const int fa = i / VX, xc = i - fa * VX;
+        const int a = j0 - 1 + fa, c = c0 + xc;
+        double pLL = 0.0, pL = 0.0, pR = 0.0, pRR = 0.0;
+        if (a >= 0 && a <= nz && c < nr) {
+          const double *w = sW + (s * WR + fa) * WC + xc + 2;            // rows a-1, a
+          const double g = A.gdz * (w[WC] - w[0]);                       // F(a) += gdz Phi, F(a-1) -= gdz Phi
+          if (g != 0.0) {
+            const double *st = sST + (s * SR + fa) * SC + xc + 3;        // rows a-2 .. a+1
+            const double e = sEZ[fa * VX + xc];                          // ez(c, a-1)
+            const FaceGrad fg = face_grad (false, st[0], st[SC], st[2 * SC], st[3 * SC], A.cm[s] * e, A.ddz[s]);
+            pLL = g * fg.pLL; pL = g * fg.pL; pR = g * fg.pR; pRR = g * fg.pRR;
+            if ((a >= j0 && a < j0 + VY && a < nz) || (a == nz && nz - 1 >= j0 && nz - 1 < j0 + VY)) {
+              gmu[s] += g * (fg.dv * M.charge[s] * e + fg.ddd * A.Ddz);
+              gD += g * fg.ddd * A.mudz[s];
+            }
+          }
+        }
+        double *pz = sPZ + fa * VX + xc;
+        pz[0] = pLL; pz[FZ * VX] = pL; pz[2 * FZ * VX] = pR; pz[3 * FZ * VX] = pRR;
+      }
+      __syncthreads ();
+      // face x - 1/2 touches cells x-2 (LL), x-1 (L), x (R), x+1 (RR): cell y
+      // collects RR of face y-1, R of face y, L of face y+1, LL of face y+2
+      auto RAD = [&] (int jj, int x) -> double {    // partials landing on column x of row jj
+        const int f = x - c0 + 1;                   // face index of face x - 1/2
+        const double *pr = sPR + jj * FR;
+        double v = 0.0;
+        if (f - 1 >= 0 && f - 1 < FR) v += pr[3 * VY * FR + f - 1];
+        if (f >= 0 && f < FR) v += pr[2 * VY * FR + f];
+        if (f + 1 >= 0 && f + 1 < FR) v += pr[VY * FR + f + 1];
+        if (f + 2 >= 0 && f + 2 < FR) v += pr[f + 2];
+        return v;
+      };
+      auto AXI = [&] (int y) -> double {            // partials landing on row y of column cc
+        const int f = y - j0 + 1;
+        const double *pz = sPZ + cc;
+        double v = 0.0;
+        if (f - 1 >= 0 && f - 1 < FZ) v += pz[(3 * FZ + f - 1) * VX];
+        if (f >= 0 && f < FZ) v += pz[(2 * FZ + f) * VX];
+        if (f + 1 >= 0 && f + 1 < FZ) v += pz[(FZ + f + 1) * VX];
+        if (f + 2 >= 0 && f + 2 < FZ) v += pz[(f + 2) * VX];
+        return v;
+      };
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const int jj = jA + 8 * q, j = j0 + jj, c = c0 + cc;
+        if (c >= nr || j >= nz) continue;
+        double z = AXI (j);
+        if (j == 0) z = __fma_rn (sg_b, AXI (-1), z);            // ghost rows fold onto the rows they mirror
+        if (j == 1) z = __fma_rn (sg_b, AXI (-2), z);
+        if (j == nz - 1) z = __fma_rn (sg_t, AXI (nz), z);
+        if (j == nz - 2) z = __fma_rn (sg_t, AXI (nz + 1), z);
+        double rr = RAD (jj, c);
+        if (c == 0) rr += RAD (jj, -1);                           // axis ghosts -1, -2 -> cells 0, 1
+        if (c == 1) rr += RAD (jj, -2);
+        if (c == nr - 1) rr = __fma_rn (sg_r, RAD (jj, nr), rr);  // ghosts nr, nr+1 -> cells nr-1, nr-2
+        if (c == nr - 2) rr = __fma_rn (sg_r, RAD (jj, nr + 1), rr);
+        out[q][s] = z + rr;
+      }
+      __syncthreads ();                         // the partial buffers are reused by the next species
+    }
+
+    // ---- (4) reactions (react_apply, folded form); every lane joins the
+    // warp-wide table-gradient reductions ----
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int jj = jA + 8 * q, j = j0 + jj, c = c0 + cc;
+      const bool own = c < nr && j < nz;
       if (M.nreact > 0) {
         double eabs = 1.0;
         double cen[NS], wc[NS];
 #pragma unroll
-        for (int s = 0; s < NS; s++) { cen[s] = wn[0][s]; wc[s] = 0.0; }
+        for (int s = 0; s < NS; s++) { cen[s] = 0.0; wc[s] = 0.0; }
         if (own) {
-          const double e_r = 0.5 * (er[Pp->off (c, j, 0)] + er[Pp->off (c - 1, j, 0)]);   // cdr.c:681-682
-          const double e_z = 0.5 * (ez[Pp->off (c, j, 0)] + ez[Pp->off (c, j - 1, 0)]);   // cdr.c:683-684
+          const double e_r = 0.5 * (sER[jj * EC + cc + 2] + sER[jj * EC + cc + 1]);     // cdr.c:681-682
+          const double e_z = 0.5 * (sEZ[(jj + 2) * VX + cc] + sEZ[(jj + 1) * VX + cc]); // cdr.c:683-684
           eabs = sqrt (e_r * e_r + e_z * e_z);
 #pragma unroll
-          for (int s = 0; s < NS; s++) wc[s] = W (s, c, j);
+          for (int s = 0; s < NS; s++) {
+            cen[s] = sST[(s * SR + jj + 3) * SC + cc + 3];
+            wc[s] = sW[(s * WR + jj + 2) * WC + cc + 2];
+          }
         }
         const bool on = own && ((double) (Pp->z0 + j) + 0.5) * Pp->dz < M.z_cutoff;
 #pragma unroll 1
         for (int r = 0; r < M.nreact; r++) {
           int i_lo = -1, i_ex = -1;
-          double g_lo = 0.0, g_hi = 0.0, g_ex = 0.0;
+          double g_lo = 0.0, g_hi = 0.0;
           if (on) {
             double rho = 0.0;
 #pragma unroll
@@ -370,14 +399,14 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
               if (cnt == 0) continue;
               double others = 1.0;
 #pragma unroll
-              for (int q = 0; q < NS; q++) {
-                const int cq = M.r_in_count[r][q] - (q == s ? 1 : 0);
-                const double av = fabs (cen[q]);
+              for (int p = 0; p < NS; p++) {
+                const int cq = M.r_in_count[r][p] - (p == s ? 1 : 0);
+                const double av = fabs (cen[p]);
                 if (cq > 0) others *= av;
                 if (cq > 1) others *= av;
               }
               const double sgn = cen[s] > 0.0 ? 1.0 : (cen[s] < 0.0 ? -1.0 : 0.0);
-              out[s] = __fma_rn (rho * k * (double) cnt * sgn, others, out[s]);
+              out[q][s] = __fma_rn (rho * k * (double) cnt * sgn, others, out[q][s]);
             }
             // table entries: rate = v1 + (v2 - v1) (E - e1) / (e2 - e1) (reaction.c:142)
             const TableNode *nd = A.nodes + M.r_node_off[r];
@@ -396,25 +425,21 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
               if (kk == steps) { g_lo += g_hi; g_hi = 0.0; }   // last node: v2 = v1
             } else {
               i_ex = A.n_nodes + 2 * r + (eabs >= nd[steps + 1].thr ? 1 : 0);
-              g_ex = gr;
+              g_lo = gr;
             }
           }
-          if (r < NCACHE) tc[r].add (A.g_table, i_lo, g_lo, g_hi, i_ex, g_ex);
-          else {
-            warp_add (A.g_table, i_lo, g_lo);
-            warp_add (A.g_table, i_lo >= 0 ? i_lo + 1 : -1, g_hi);
-            warp_add (A.g_table, i_ex, g_ex);
-          }
+          warp_add (gtab, i_lo >= 0 ? i_lo : i_ex, g_lo);
+          warp_add (gtab, i_lo >= 0 ? i_lo + 1 : -1, g_hi);
         }
       }
       if (own) {
         const long long o = AO (c, j);
 #pragma unroll
         for (int s = 0; s < NS; s++) {
-          double v = out[s];
+          double v = out[q][s];
           if (A.mode == 2) {
-            v += adj[(long long) (A.lam_idx + s) * asz + o] + adj[(long long) (A.lams_idx + s) * asz + o];
-            if (!(adj[(long long) (A.st_idx + s) * asz + o] > 0.0)) v = 0.0;     // d max(0, n0)
+            v += __ldg (adj + (long long) (A.lam_idx + s) * asz + o) + __ldg (adj + (long long) (A.lams_idx + s) * asz + o);
+            if (!(sST[(s * SR + jj + 3) * SC + cc + 3] > 0.0)) v = 0.0;   // d max(0, n0)
           }
           adj[(long long) (A.out_idx + s) * asz + o] = v;
         }
@@ -422,8 +447,6 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
     }
   }
 
-#pragma unroll 1
-  for (int r = 0; r < NCACHE && r < M.nreact; r++) tc[r].flush (A.g_table);
   // ---- block partial sums of the mobility and diffusion gradients ----
 #pragma unroll
   for (int s = 0; s < NS; s++)
@@ -439,9 +462,12 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
   __syncthreads ();
   if (t <= NS) {
     double v = 0.0;
-    for (int w = 0; w < WY; w++) v += red[w][t];
+    for (int w = 0; w < NT / 32; w++) v += red[w][t];
     A.g_part[(size_t) blockIdx.x * (NS + 1) + t] += v;
   }
+  if (A.tab_smem)
+    for (int i = t; i < ntab; i += NT)
+      if (sTab[i] != 0.0) atomicAdd (A.g_table + i, sTab[i]);
 }
 
 }  // namespace arcos

@@ -119,6 +119,8 @@ struct Ctx {
   double *adj_invde_d = nullptr;
   AdjTile *adj_tiles_d = nullptr;
   int adj_ntiles = 0, adj_blocks = 0;
+  size_t adj_smem = 0;                // dynamic shared memory of a VJP block
+  int adj_tab_smem = 0;               // table gradients accumulate in shared memory
   int adj_lam = 0;                    // lam buffer holding the current cotangent
   bool adj_fwd = false;
   cudaGraphExec_t adj_graph = nullptr;   // the whole reverse sweep
@@ -838,7 +840,48 @@ rk2_fused_launches (Ctx *c, int src, int fold)
 
 
 // ---- discrete adjoint -----------------------------------------------------------
-constexpr int ADJ_WY = 4, ADJ_BAND = 4;
+// Launches k_vjp<NS> (occ == nullptr), or sets its shared-memory limit and
+// returns its resident blocks per SM in *occ.
+template <int NS>
+cudaError_t
+vjp_launch (const Model &M, const VjpArgs &A, int blocks, size_t smem, cudaStream_t st, int *occ)
+{
+  if (occ) {
+    cudaError_t e = cudaFuncSetAttribute (k_vjp<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor (occ, k_vjp<NS>, VjpTile<NS>::NT, smem);
+  }
+  k_vjp<NS><<<blocks, VjpTile<NS>::NT, smem, st>>> (M, A);
+  return cudaGetLastError ();
+}
+
+cudaError_t
+vjp_launch_m (int ns, const Model &M, const VjpArgs &A, int blocks, size_t smem, cudaStream_t st, int *occ)
+{
+  switch (ns) {
+  case 1: return vjp_launch<1> (M, A, blocks, smem, st, occ);
+  case 2: return vjp_launch<2> (M, A, blocks, smem, st, occ);
+  case 3: return vjp_launch<3> (M, A, blocks, smem, st, occ);
+  case 4: return vjp_launch<4> (M, A, blocks, smem, st, occ);
+  case 5: return vjp_launch<5> (M, A, blocks, smem, st, occ);
+  case 6: return vjp_launch<6> (M, A, blocks, smem, st, occ);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+// Shared memory of a VJP block without the table accumulator, in doubles.
+size_t
+vjp_base_doubles (int ns)
+{
+  switch (ns) {
+  case 1: return VjpTile<1>::O_TAB;
+  case 2: return VjpTile<2>::O_TAB;
+  case 3: return VjpTile<3>::O_TAB;
+  case 4: return VjpTile<4>::O_TAB;
+  case 5: return VjpTile<5>::O_TAB;
+  default: return VjpTile<6>::O_TAB;
+  }
+}
 
 inline int adj_lam_idx (Ctx *c, int which) { return which * c->M.ns; }
 inline int adj_lams_idx (Ctx *c) { return 2 * c->M.ns; }
@@ -857,6 +900,19 @@ adj_copy (Ctx *c, bool to_adj, int set, int idx)
       double *a = P.arr (set, K_DENS, s), *b = P.adj + (size_t) (idx + s) * P.asz;
       CK (cudaMemcpyAsync (to_adj ? b : a, to_adj ? a : b, sizeof (double) * P.asz, cudaMemcpyDeviceToDevice, c->stream));
     }
+  return ARCOS_OK;
+}
+
+// dens of set 0 and set 1 into adjoint arrays i0 + s, is + s: one launch
+int
+adj_keep (Ctx *c, int i0, int is)
+{
+  long long amax = 0;
+  for (auto &P : c->pd_h) amax = std::max (amax, P.asz);
+  const int bx = (int) std::min<long long> ((amax / 2 + 255) / 256, 2LL * c->num_sms);
+  k_adj_keep<<<dim3 (bx, (unsigned) c->pd_h.size ()), 256, 0, c->stream>>> (c->pd_d, i0, is);
+  cudaError_t e = cudaGetLastError ();
+  if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("keep launch: ") + cudaGetErrorString (e));
   return ARCOS_OK;
 }
 
@@ -884,15 +940,22 @@ adj_alloc (Ctx *c, int nsteps, int ck)
     std::vector<AdjTile> tl;
     for (int p = 0; p < (int) c->pd_h.size (); p++) {
       const PatchDesc &P = c->pd_h[p];
-      for (int zb = 0; zb < P.nz; zb += ADJ_WY * ADJ_BAND)
-        for (int c0 = 0; c0 < P.nr; c0 += ADJ_STRIP) tl.push_back (AdjTile{p, c0, zb, 0});
+      for (int zb = 0; zb < P.nz; zb += VjpTile<1>::VY)
+        for (int c0 = 0; c0 < P.nr; c0 += VjpTile<1>::VX) tl.push_back (AdjTile{p, c0, zb, 0});
     }
     c->adj_ntiles = (int) tl.size ();
     CK (cudaMalloc (&c->adj_tiles_d, sizeof (AdjTile) * tl.size ()));
     CK (cudaMemcpy (c->adj_tiles_d, tl.data (), sizeof (AdjTile) * tl.size (), cudaMemcpyHostToDevice));
-    c->adj_blocks = std::min (c->adj_ntiles, c->num_sms * 4);
-    CK (cudaMalloc (&c->adj_gpart_d, sizeof (double) * (size_t) c->adj_blocks * (ns + 1)));
     const size_t ng = c->nodes_h.size () + 2 * (size_t) c->M.nreact;
+    // the table accumulator joins the block's shared memory while it fits
+    const size_t base = sizeof (double) * vjp_base_doubles (ns), limit = 227 * 1024;
+    c->adj_tab_smem = base + sizeof (double) * ng <= limit ? 1 : 0;
+    c->adj_smem = base + (c->adj_tab_smem ? sizeof (double) * ng : 0);
+    int occ = 0;
+    cudaError_t e = vjp_launch_m (ns, c->M, VjpArgs{}, 0, c->adj_smem, 0, &occ);
+    if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("vjp occupancy: ") + cudaGetErrorString (e));
+    c->adj_blocks = std::min (c->adj_ntiles, c->num_sms * std::max (occ, 1));
+    CK (cudaMalloc (&c->adj_gpart_d, sizeof (double) * (size_t) c->adj_blocks * (ns + 1)));
     CK (cudaMalloc (&c->adj_gtab_d, sizeof (double) * std::max<size_t> (ng, 1)));
   }
   // 1 / (e2 - e1) of every node (reaction.c:139-142)
@@ -954,17 +1017,9 @@ run_vjp (Ctx *c, int mode, int st_idx, int lam_idx, int lams_idx, int out_idx, i
   A.Ddr = D / dr;
   A.Ddz = D / dz;
   A.gdz = 1.0 / dz;
-  cudaError_t e = cudaSuccess;
-  switch (c->M.ns) {
-  case 1: k_vjp<1, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
-  case 2: k_vjp<2, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
-  case 3: k_vjp<3, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
-  case 4: k_vjp<4, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
-  case 5: k_vjp<5, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
-  case 6: k_vjp<6, ADJ_WY, ADJ_BAND><<<c->adj_blocks, 32 * ADJ_WY, 0, c->stream>>> (c->M, A); break;
-  default: return fail (ARCOS_ERR_ARG, "adjoint: 1..6 species");
-  }
-  e = cudaGetLastError ();
+  A.tab_smem = c->adj_tab_smem;
+  if (c->M.ns < 1 || c->M.ns > 6) return fail (ARCOS_ERR_ARG, "adjoint: 1..6 species");
+  cudaError_t e = vjp_launch_m (c->M.ns, c->M, A, c->adj_blocks, c->adj_smem, c->stream, nullptr);
   if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("vjp launch: ") + cudaGetErrorString (e));
   return ARCOS_OK;
 }
@@ -986,9 +1041,8 @@ adj_enqueue_sweep (Ctx *c)
     const int k0 = seg * c->adj_ck, k1 = std::min (c->adj_nsteps, k0 + c->adj_ck);
     if ((r = adj_copy (c, false, 0, adj_ckpt (c, seg)))) return r;
     for (int k = k0; k < k1; k++) {
-      if ((r = adj_copy (c, true, 0, adj_seg_n0 (c, k - k0)))) return r;
       if ((r = adj_frozen_step (c, k, false))) return r;
-      if ((r = adj_copy (c, true, 1, adj_seg_ns (c, k - k0)))) return r;
+      if ((r = adj_keep (c, adj_seg_n0 (c, k - k0), adj_seg_ns (c, k - k0)))) return r;
       if (k + 1 < k1 && (r = run_fused (c, true, 0, 0, k))) return r;
     }
     for (int k = k1 - 1; k >= k0; k--) {

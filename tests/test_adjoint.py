@@ -207,3 +207,65 @@ def test_frozen_forward_reproduces_cfl_run(cuda_device):
     adj.forward(K, ck, h_seq=hs)
     for s in range(2):
         assert np.array_equal(tree.download(0, "dens", s)[0, 2:-2, 2:-2], a[s][0, 2:-2, 2:-2])
+
+
+def test_kinetic_batch_adjoint_matches_fd(cuda_device):
+    """Three families of different sizes, six species (ions mobile), nine
+    reactions with one- and two-input terms: the adjoint of the total electron
+    number at T with respect to the initial densities of every species and
+    every table value, against central differences of the frozen-step
+    forward.  Two checkpoint segments."""
+    pb = workloads.kinetic_batch(n_inst=3, points=200, sizes_r=(24, 40), sizes_z=(32, 48), seed=1)
+    ns = pb.model.no_species
+    tree = CdrTree(pb.params, pb.model, pb.specs)
+    for f, E in enumerate(pb.family_E):
+        tree.set_family_field(f, *E)
+    tree.set_fixed_field(pb.fields)
+    tabs = [np.array(r.table.values[: r.table.steps + 1], dtype=np.float64) for r in pb.model.reactions]
+
+    def apply(dens, vals):
+        for g, per in enumerate(dens):
+            for s, a in enumerate(per):
+                tree.upload(g, "dens", a, s)
+        for r, re in enumerate(pb.model.reactions):
+            tree.set_table_values(r, vals[r], re.table.underflow, re.table.overflow)
+
+    K, ck = 6, 3
+    adj = Adjoint(tree)
+    apply(pb.dens, tabs)
+    hs = adj.forward(K, ck, h=50.0)
+    vols = [cell_volume(sp, pb.params.dr(0), pb.params.dz(0)) for sp in pb.specs]
+    for g, sp in enumerate(pb.specs):
+        adj.set_cotangent(g, 0, vols[g])
+        for s in range(1, ns):
+            adj.set_cotangent(g, s, np.zeros(sp.shape))
+    grads = adj.backward()
+
+    def total_electrons(dens, vals):
+        apply(dens, vals)
+        adj.forward(K, ck, h_seq=hs)
+        return [tree.download(g, "dens", 0) for g in range(len(pb.specs))]
+
+    rng = np.random.default_rng(23)
+    for which, eps in ((("dens", "table"), EPS), (("table",), 1e-4)):
+        dd = []
+        for g, sp in enumerate(pb.specs):
+            per = []
+            for s in range(ns):
+                d = np.zeros(sp.shape)
+                if "dens" in which:
+                    d[0, 2:-2, 2:-2] = smooth_direction(rng, sp.nz, sp.nr)
+                per.append(d)
+            dd.append(per)
+        dv = [rng.standard_normal(t.shape) if "table" in which else np.zeros(t.shape) for t in tabs]
+        pred = sum(float(np.sum(grads.dens0[g][s] * pb.dens[g][s] * dd[g][s]))
+                   for g in range(len(pb.specs)) for s in range(ns))
+        pred += sum(float(np.sum(grads.tables[r] * tabs[r] * dv[r])) for r in range(len(tabs)))
+        outs = []
+        for sg in (1.0, -1.0):
+            dens = [[pb.dens[g][s] * (1.0 + sg * eps * dd[g][s]) for s in range(ns)] for g in range(len(pb.specs))]
+            vals = [tabs[r] * (1.0 + sg * eps * dv[r]) for r in range(len(tabs))]
+            outs.append(total_electrons(dens, vals))
+        fd = sum(float(np.sum(vols[g] * (outs[0][g] - outs[1][g]))) for g in range(len(pb.specs))) / (2 * eps)
+        assert abs(fd - pred) <= TOL * abs(fd), (which, fd, pred)
+    tree.close()
