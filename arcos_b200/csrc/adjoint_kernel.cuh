@@ -18,6 +18,8 @@
 // cells they land on.  Ghost-cell contributions fold back onto the interior
 // cells the boundary conditions mirror.
 #pragma once
+#include <type_traits>
+
 #include "fused_kernel.cuh"
 
 namespace arcos {
@@ -142,10 +144,39 @@ k_adj_keep (const PatchDesc *__restrict__ pd, int i0, int is)
   }
 }
 
+// f(integral_constant<int, I>) for I = B .. E-1, unrolled at compile time.
+template <int B, int E, typename F>
+__device__ __forceinline__ void
+static_for (F &&f)
+{
+  if constexpr (B < E) {
+    f (std::integral_constant<int, B> {});
+    static_for<B + 1, E> (f);
+  }
+}
+
+// f(row, col) over the items t, t + NT, .. of an H x W array (row-major),
+// without a division per item.
+template <int W, int H, int NT, typename F>
+__device__ __forceinline__ void
+tile_for (int t, F &&f)
+{
+  int yy = t / W, xx = t - (t / W) * W;
+#pragma unroll
+  for (int m = 0; m < (W * H + NT - 1) / NT; m++) {
+    if (yy < H) f (yy, xx);
+    xx += NT % W;
+    yy += NT / W;
+    if (xx >= W) { xx -= W; yy++; }
+  }
+}
+
 // Shared-memory layout of one VJP tile: VX output columns x VY output rows.
 template <int NS>
 struct VjpTile {
-  static constexpr int VX = 32, VY = 16, NT = 256;
+  // up to three species: 32 x 16 tiles, two cells per thread; more species
+  // (more shared memory per cell): 32 x 8 tiles, one cell per thread
+  static constexpr int VX = 32, VY = NS <= 3 ? 16 : 8, NT = 256, CPT = VY / (NT / 32);
   static constexpr int SC = VX + 6, SR = VY + 6;   // state: cols c0-3 .. c0+VX+2, rows j0-3 .. j0+VY+2
   static constexpr int WC = VX + 4, WR = VY + 4;   // cotangent of F: cols c0-2 .., rows j0-2 ..
   static constexpr int EC = VX + 3;                // er: cols c0-2 .. c0+VX, rows j0 .. j0+VY-1
@@ -173,22 +204,27 @@ struct VjpTile {
 // partials that land on it, plus those that land on the ghost cells it
 // mirrors (axis, r = L_r, z = 0, z = L_z).  (4) Reactions per cell; table
 // gradients add into a shared accumulator (warp-aggregated) that is flushed
-// to A.g_table when the block ends.  The mobility and diffusion sums take
-// every face once (the tile holding the cell left of / below the face; the
-// last cell's tile for the faces at r = L_r and z = L_z).
+// to A.g_table when the block ends, or straight into A.g_table.  The
+// mobility and diffusion sums take every face once (the tile holding the
+// cell left of / below the face; the last cell's tile for the faces at
+// r = L_r and z = L_z).  Thread (lane, warp) owns column lane and rows
+// CPT warp .. CPT warp + CPT - 1 of the tile.
 template <int NS>
 __global__ void __launch_bounds__ (256)
 k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
 {
   using L = VjpTile<NS>;
-  constexpr int VX = L::VX, VY = L::VY, NT = L::NT;
+  constexpr int VX = L::VX, VY = L::VY, NT = L::NT, NW = NT / 32;
   constexpr int SC = L::SC, SR = L::SR, WC = L::WC, WR = L::WR, EC = L::EC, ZR = L::ZR;
   constexpr int FR = L::FR, FZ = L::FZ;
+  constexpr int RP = (VY * FR + NT - 1) / NT;        // passes over the radial faces
+  constexpr int CPT = L::CPT;                        // cells (rows) per thread
+  static_assert (VX == 32 && VY == CPT * NW, "tile: a warp per CPT rows of 32 columns");
   extern __shared__ __align__ (16) double vsm[];
   double *const sST = vsm + L::O_ST, *const sW = vsm + L::O_W;
   double *const sER = vsm + L::O_ER, *const sEZ = vsm + L::O_EZ;
   double *const sPR = vsm + L::O_PR, *const sPZ = vsm + L::O_PZ, *const sTab = vsm + L::O_TAB;
-  __shared__ double red[NT / 32][NS + 1];
+  __shared__ double red[NW][NS + 1];
   const int t = threadIdx.x, lane = t & 31, wq = t >> 5;
   const int ntab = A.n_nodes + 2 * M.nreact;
   double *const gtab = A.tab_smem ? sTab : A.g_table;
@@ -197,8 +233,17 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
   double gmu[NS], gD = 0.0;
 #pragma unroll
   for (int s = 0; s < NS; s++) gmu[s] = 0.0;
-  const int cc = lane;                          // own column in the tile
-  const int jA = wq;                            // own rows jA and jA + 8
+  // radial face items t, t + NT, ..: (row, face) without a division per tile
+  int rjj[RP], rfi[RP];
+  {
+    int jj = t / FR, fi = t - (t / FR) * FR;
+#pragma unroll
+    for (int m = 0; m < RP; m++) {
+      rjj[m] = jj; rfi[m] = fi;
+      fi += NT % FR; jj += NT / FR;
+      if (fi >= FR) { fi -= FR; jj++; }
+    }
+  }
 
   for (int ti = blockIdx.x; ti < A.n_tiles; ti += gridDim.x) {
     const AdjTile T = A.tiles[ti];
@@ -218,57 +263,68 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
     __syncthreads ();                           // the previous tile is done with the shared arrays
     // ---- (1) staging.  The state, lam, lams, er and ez arrays are read-only in
     // this launch (the output array is a different one): non-coherent loads ----
-    for (int i = t; i < NS * SR * SC; i += NT) {
-      const int s = i / (SR * SC), rem = i - s * (SR * SC), yy = rem / SC, xx = rem - yy * SC;
-      int col = c0 - 3 + xx, row = j0 - 3 + yy;
-      double sg = 1.0;                          // ghost cells: no corners needed
-      if (col < 0) { col = -1 - col; }                              // axis, 2-D
-      else if (col >= nr) { col = 2 * nr - 1 - col; sg = sg_r; }
-      if (row < 0) { row = -1 - row; sg = sg_b; }
-      else if (row >= nz) { row = 2 * nz - 1 - row; sg = sg_t; }
-      double v = 0.0;
-      if (col >= 0 && col < nr && row >= 0 && row < nz) {
-        v = __ldg (adj + (long long) (A.st_idx + s) * asz + AO (col, row));
-        if (clampst) v = clamp0 (v);
-        v = sg * v;
-      }
-      sST[i] = v;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      const double *src = adj + (long long) (A.st_idx + s) * asz;
+      tile_for<SC, SR, NT> (t, [&] (int yy, int xx) {
+        int col = c0 - 3 + xx, row = j0 - 3 + yy;
+        double sg = 1.0;                        // ghost cells: no corners needed
+        if (col < 0) { col = -1 - col; }                              // axis, 2-D
+        else if (col >= nr) { col = 2 * nr - 1 - col; sg = sg_r; }
+        if (row < 0) { row = -1 - row; sg = sg_b; }
+        else if (row >= nz) { row = 2 * nz - 1 - row; sg = sg_t; }
+        double v = 0.0;
+        if (col >= 0 && col < nr && row >= 0 && row < nz) {
+          v = __ldg (src + AO (col, row));
+          if (clampst) v = clamp0 (v);
+          v = sg * v;
+        }
+        sST[(s * SR + yy) * SC + xx] = v;
+      });
     }
-    for (int i = t; i < NS * WR * WC; i += NT) {
-      const int s = i / (WR * WC), rem = i - s * (WR * WC), yy = rem / WC, xx = rem - yy * WC;
-      const int col = c0 - 2 + xx, row = j0 - 2 + yy;
-      double w = 0.0;                           // cotangent of F at interior cells only
-      if (col >= 0 && col < nr && row >= 0 && row < nz) {
-        const long long o = AO (col, row);
-        w = a1 * __ldg (adj + (long long) (A.lam_idx + s) * asz + o);
-        if (A.mode == 2) w = __fma_rn (b1, __ldg (adj + (long long) (A.lams_idx + s) * asz + o), w);
-      }
-      sW[i] = w;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      const double *lp = adj + (long long) (A.lam_idx + s) * asz;
+      const double *lsp = adj + (long long) (A.lams_idx + s) * asz;
+      tile_for<WC, WR, NT> (t, [&] (int yy, int xx) {
+        const int col = c0 - 2 + xx, row = j0 - 2 + yy;
+        double w = 0.0;                         // cotangent of F at interior cells only
+        if (col >= 0 && col < nr && row >= 0 && row < nz) {
+          const long long o = AO (col, row);
+          w = a1 * __ldg (lp + o);
+          if (A.mode == 2) w = __fma_rn (b1, __ldg (lsp + o), w);
+        }
+        sW[(s * WR + yy) * WC + xx] = w;
+      });
     }
-    for (int i = t; i < VY * EC; i += NT) {
-      const int yy = i / EC, xx = i - yy * EC;
+    tile_for<EC, VY, NT> (t, [&] (int yy, int xx) {
       const int col = c0 - 2 + xx, row = j0 + yy;
-      sER[i] = (col >= -2 && col <= nr + 1 && row <= nz + 1) ? __ldg (er + Pp->off (col, row, 0)) : 0.0;
-    }
-    for (int i = t; i < ZR * VX; i += NT) {
-      const int yy = i / VX, xx = i - yy * VX;
-      const int col = c0 + xx, row = j0 - 2 + yy;
-      sEZ[i] = (col <= nr + 1 && row >= -2 && row <= nz + 1) ? __ldg (ez + Pp->off (col, row, 0)) : 0.0;
+      sER[yy * EC + xx] = (col >= -2 && col <= nr + 1 && row <= nz + 1) ? __ldg (er + AO (col, row)) : 0.0;
+    });
+#pragma unroll
+    for (int y8 = 0; y8 < (ZR + NW - 1) / NW; y8++) {
+      const int yy = wq + NW * y8;
+      if (yy >= ZR) break;
+      const int row = j0 - 2 + yy, col = c0 + lane;
+      sEZ[yy * VX + lane] = (col <= nr + 1 && row >= -2 && row <= nz + 1) ? __ldg (ez + AO (col, row)) : 0.0;
     }
     __syncthreads ();
 
-    double out[2][NS];
+    double out[CPT][NS];
 #pragma unroll
-    for (int q = 0; q < 2; q++)
+    for (int q = 0; q < CPT; q++)
 #pragma unroll
       for (int s = 0; s < NS; s++) out[q][s] = 0.0;
 
-    // ---- (2), (3) drift-diffusion faces, one species at a time ----
+    // ---- (2), (3) drift-diffusion faces, one species at a time (unrolled at
+    // compile time: out and gmu stay in registers) ----
+    static_for<0, NS> ([&] (auto S_) {
+      constexpr int s = decltype (S_)::value;
+      if (!M.mobile[s]) return;                 // block-uniform
 #pragma unroll
-    for (int s = 0; s < NS; s++) {
-      if (!M.mobile[s]) continue;               // block-uniform
-      for (int i = t; i < VY * FR; i += NT) {   // radial face ar - 1/2 of row j
-        const int jj = i / FR, fi = i - jj * FR;
+      for (int m = 0; m < RP; m++) {            // radial face ar - 1/2 of row j
+        const int jj = rjj[m], fi = rfi[m];
+        if (jj >= VY) break;
         const int ar = c0 - 1 + fi, j = j0 + jj;
         double pLL = 0.0, pL = 0.0, pR = 0.0, pRR = 0.0;
         if (ar >= 0 && ar <= nr && j < nz) {
@@ -290,16 +346,18 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         double *pr = sPR + jj * FR + fi;
         pr[0] = pLL; pr[VY * FR] = pL; pr[2 * VY * FR] = pR; pr[3 * VY * FR] = pRR;
       }
-      for (int i = t; i < FZ * VX; i += NT) {   // axial face a - 1/2 of column c
-        const int fa = i / VX, xc = i - fa * VX;
-        const int a = j0 - 1 + fa, c = c0 + xc;
+#pragma unroll
+      for (int m = 0; m < (FZ + NW - 1) / NW; m++) {   // axial face a - 1/2 of column c
+        const int fa = wq + NW * m;
+        if (fa >= FZ) break;
+        const int a = j0 - 1 + fa, c = c0 + lane;
         double pLL = 0.0, pL = 0.0, pR = 0.0, pRR = 0.0;
         if (a >= 0 && a <= nz && c < nr) {
-          const double *w = sW + (s * WR + fa) * WC + xc + 2;            // rows a-1, a
+          const double *w = sW + (s * WR + fa) * WC + lane + 2;          // rows a-1, a
           const double g = A.gdz * (w[WC] - w[0]);                       // F(a) += gdz Phi, F(a-1) -= gdz Phi
           if (g != 0.0) {
-            const double *st = sST + (s * SR + fa) * SC + xc + 3;        // rows a-2 .. a+1
-            const double e = sEZ[fa * VX + xc];                          // ez(c, a-1)
+            const double *st = sST + (s * SR + fa) * SC + lane + 3;      // rows a-2 .. a+1
+            const double e = sEZ[fa * VX + lane];                        // ez(c, a-1)
             const FaceGrad fg = face_grad (false, st[0], st[SC], st[2 * SC], st[3 * SC], A.cm[s] * e, A.ddz[s]);
             pLL = g * fg.pLL; pL = g * fg.pL; pR = g * fg.pR; pRR = g * fg.pRR;
             if ((a >= j0 && a < j0 + VY && a < nz) || (a == nz && nz - 1 >= j0 && nz - 1 < j0 + VY)) {
@@ -308,7 +366,7 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
             }
           }
         }
-        double *pz = sPZ + fa * VX + xc;
+        double *pz = sPZ + fa * VX + lane;
         pz[0] = pLL; pz[FZ * VX] = pL; pz[2 * FZ * VX] = pR; pz[3 * FZ * VX] = pRR;
       }
       __syncthreads ();
@@ -324,9 +382,9 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         if (f + 2 >= 0 && f + 2 < FR) v += pr[f + 2];
         return v;
       };
-      auto AXI = [&] (int y) -> double {            // partials landing on row y of column cc
+      auto AXI = [&] (int y) -> double {            // partials landing on row y of column lane
         const int f = y - j0 + 1;
-        const double *pz = sPZ + cc;
+        const double *pz = sPZ + lane;
         double v = 0.0;
         if (f - 1 >= 0 && f - 1 < FZ) v += pz[(3 * FZ + f - 1) * VX];
         if (f >= 0 && f < FZ) v += pz[(2 * FZ + f) * VX];
@@ -335,8 +393,8 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         return v;
       };
 #pragma unroll
-      for (int q = 0; q < 2; q++) {
-        const int jj = jA + 8 * q, j = j0 + jj, c = c0 + cc;
+      for (int q = 0; q < CPT; q++) {
+        const int jj = CPT * wq + q, j = j0 + jj, c = c0 + lane;
         if (c >= nr || j >= nz) continue;
         double z = AXI (j);
         if (j == 0) z = __fma_rn (sg_b, AXI (-1), z);            // ghost rows fold onto the rows they mirror
@@ -351,98 +409,119 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         out[q][s] = z + rr;
       }
       __syncthreads ();                         // the partial buffers are reused by the next species
-    }
+    });
 
-    // ---- (4) reactions (react_apply, folded form); every lane joins the
-    // warp-wide table-gradient reductions ----
+    // ---- (4) reactions (react_apply, folded form): rate = k(|E|) prod |n_in|,
+    // d_dens[s] += coef[s] rate.  Every lane joins the warp-wide table-gradient
+    // reductions ----
+    if (M.nreact > 0) {
+      double eabs[CPT], wc[CPT][NS];
+      bool on[CPT];
 #pragma unroll
-    for (int q = 0; q < 2; q++) {
-      const int jj = jA + 8 * q, j = j0 + jj, c = c0 + cc;
-      const bool own = c < nr && j < nz;
-      if (M.nreact > 0) {
-        double eabs = 1.0;
-        double cen[NS], wc[NS];
-#pragma unroll
-        for (int s = 0; s < NS; s++) { cen[s] = 0.0; wc[s] = 0.0; }
+      for (int q = 0; q < CPT; q++) {
+        const int jj = CPT * wq + q, j = j0 + jj, c = c0 + lane;
+        const bool own = c < nr && j < nz;
+        eabs[q] = 1.0;
         if (own) {
-          const double e_r = 0.5 * (sER[jj * EC + cc + 2] + sER[jj * EC + cc + 1]);     // cdr.c:681-682
-          const double e_z = 0.5 * (sEZ[(jj + 2) * VX + cc] + sEZ[(jj + 1) * VX + cc]); // cdr.c:683-684
-          eabs = sqrt (e_r * e_r + e_z * e_z);
-#pragma unroll
-          for (int s = 0; s < NS; s++) {
-            cen[s] = sST[(s * SR + jj + 3) * SC + cc + 3];
-            wc[s] = sW[(s * WR + jj + 2) * WC + cc + 2];
-          }
+          const double e_r = 0.5 * (sER[jj * EC + lane + 2] + sER[jj * EC + lane + 1]);     // cdr.c:681-682
+          const double e_z = 0.5 * (sEZ[(jj + 2) * VX + lane] + sEZ[(jj + 1) * VX + lane]); // cdr.c:683-684
+          eabs[q] = sqrt (e_r * e_r + e_z * e_z);
         }
-        const bool on = own && ((double) (Pp->z0 + j) + 0.5) * Pp->dz < M.z_cutoff;
-#pragma unroll 1
-        for (int r = 0; r < M.nreact; r++) {
-          int i_lo = -1, i_ex = -1;
-          double g_lo = 0.0, g_hi = 0.0;
-          if (on) {
-            double rho = 0.0;
 #pragma unroll
-            for (int s = 0; s < NS; s++) rho = __fma_rn ((double) M.r_coef[r][s], wc[s], rho);
-            const double k = table_rate (M, A.nodes, r, eabs);
-            // product of the inputs and its derivatives (d|n|/dn = sign n)
+        for (int s = 0; s < NS; s++) wc[q][s] = own ? sW[(s * WR + jj + 2) * WC + lane + 2] : 0.0;
+        on[q] = own && ((double) (Pp->z0 + j) + 0.5) * Pp->dz < M.z_cutoff;
+      }
+#pragma unroll 1
+      for (int r = 0; r < M.nreact; r++) {
+        const int off = M.r_node_off[r], steps = M.r_steps[r], nin = M.r_nin[r];
+        const TableNode *nd = A.nodes + off;
+        int i_lo[CPT], i_hi[CPT];
+        double g_lo[CPT], g_hi[CPT];
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+          i_lo[q] = -1; i_hi[q] = -1; g_lo[q] = 0.0; g_hi[q] = 0.0;
+          double rho = 0.0;                     // w . coef
+#pragma unroll
+          for (int s = 0; s < NS; s++) rho = __fma_rn ((double) M.r_coef[r][s], wc[q][s], rho);
+          if (on[q] && rho != 0.0) {
+            const double e = eabs[q];
+            const int kk = table_index (M, nd, r, e);
+            const TableNode n = nd[kk];
+            const bool over = e >= nd[steps + 1].thr, inr = e >= nd[0].thr && !over;
+            double k = n.val + n.slope * (e - n.e1);                     // table_rate
+            k = over ? M.r_over[r] : k;
+            k = (e >= nd[0].thr) ? k : M.r_under[r];
+            // inputs |n_in| from the staged state (clamped in mode 2)
+            const double *stq = sST + (CPT * wq + q + 3) * SC + lane + 3;
+            double av[ARCOS_MAXIN], sv[ARCOS_MAXIN];
+            int sp[ARCOS_MAXIN];
             double prod = 1.0;
 #pragma unroll
-            for (int s = 0; s < NS; s++) {
-              const int cnt = M.r_in_count[r][s];
-              const double av = fabs (cen[s]);
-              if (cnt > 0) prod *= av;
-              if (cnt > 1) prod *= av;
+            for (int i = 0; i < ARCOS_MAXIN; i++) {
+              const int si = i < nin ? M.r_in[r][i] : 0;
+              sp[i] = i < nin ? si : -1;
+              const double v = i < nin ? stq[si * (SR * SC)] : 1.0;
+              sv[i] = v;
+              av[i] = fabs (v);
+              prod *= av[i];
             }
+            // d/dn_s of k prod |n_in|: per input, k sign(n) prod of the others
+            const double rk = rho * k;
 #pragma unroll
-            for (int s = 0; s < NS; s++) {
-              const int cnt = M.r_in_count[r][s];
-              if (cnt == 0) continue;
+            for (int i = 0; i < ARCOS_MAXIN; i++) {
               double others = 1.0;
 #pragma unroll
-              for (int p = 0; p < NS; p++) {
-                const int cq = M.r_in_count[r][p] - (p == s ? 1 : 0);
-                const double av = fabs (cen[p]);
-                if (cq > 0) others *= av;
-                if (cq > 1) others *= av;
-              }
-              const double sgn = cen[s] > 0.0 ? 1.0 : (cen[s] < 0.0 ? -1.0 : 0.0);
-              out[q][s] = __fma_rn (rho * k * (double) cnt * sgn, others, out[q][s]);
+              for (int p = 0; p < ARCOS_MAXIN; p++)
+                if (p != i) others *= av[p];
+              const double sgn = sv[i] > 0.0 ? 1.0 : (sv[i] < 0.0 ? -1.0 : 0.0);
+              const double d = rk * sgn * others;
+#pragma unroll
+              for (int s = 0; s < NS; s++)
+                if (s == sp[i]) out[q][s] += d;
             }
             // table entries: rate = v1 + (v2 - v1) (E - e1) / (e2 - e1) (reaction.c:142)
-            const TableNode *nd = A.nodes + M.r_node_off[r];
-            const int steps = M.r_steps[r];
             const double gr = rho * prod;
-            if (eabs >= nd[0].thr && eabs < nd[steps + 1].thr) {
-              const float lf = __log10f ((float) eabs);
-              const float pf = (lf - (float) M.r_e_min[r]) * M.r_inv_step_f[r];
-              int kk = (int) fminf (fmaxf (pf, 0.f), (float) steps);
-              for (int it = 0; it < 64 && kk > 0 && eabs < nd[kk].thr; it++) kk--;
-              for (int it = 0; it < 64 && kk < steps && eabs >= nd[kk + 1].thr; it++) kk++;
-              const double tt = (eabs - nd[kk].e1) * A.inv_de[M.r_node_off[r] + kk];
-              i_lo = M.r_node_off[r] + kk;
-              g_lo = gr * (1.0 - tt);
-              g_hi = gr * tt;
-              if (kk == steps) { g_lo += g_hi; g_hi = 0.0; }   // last node: v2 = v1
+            if (inr) {
+              const double tt = (e - n.e1) * A.inv_de[off + kk];
+              i_lo[q] = off + kk;
+              g_lo[q] = gr * (1.0 - tt);
+              g_hi[q] = gr * tt;
+              if (kk == steps) { g_lo[q] += g_hi[q]; g_hi[q] = 0.0; }   // last node: v2 = v1
+              else i_hi[q] = off + kk + 1;
             } else {
-              i_ex = A.n_nodes + 2 * r + (eabs >= nd[steps + 1].thr ? 1 : 0);
-              g_lo = gr;
+              i_lo[q] = A.n_nodes + 2 * r + (over ? 1 : 0);
+              g_lo[q] = gr;
             }
           }
-          warp_add (gtab, i_lo >= 0 ? i_lo : i_ex, g_lo);
-          warp_add (gtab, i_lo >= 0 ? i_lo + 1 : -1, g_hi);
+        }
+        if constexpr (CPT == 2) {               // the thread's two cells first, then the warp
+          const bool same = i_lo[0] == i_lo[1] && i_hi[0] == i_hi[1];
+          warp_add (gtab, i_lo[0], same ? g_lo[0] + g_lo[1] : g_lo[0]);
+          warp_add (gtab, i_hi[0], same ? g_hi[0] + g_hi[1] : g_hi[0]);
+          warp_add (gtab, same ? -1 : i_lo[1], g_lo[1]);
+          warp_add (gtab, same ? -1 : i_hi[1], g_hi[1]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < CPT; q++) {
+            warp_add (gtab, i_lo[q], g_lo[q]);
+            warp_add (gtab, i_hi[q], g_hi[q]);
+          }
         }
       }
-      if (own) {
-        const long long o = AO (c, j);
+    }
 #pragma unroll
-        for (int s = 0; s < NS; s++) {
-          double v = out[q][s];
-          if (A.mode == 2) {
-            v += __ldg (adj + (long long) (A.lam_idx + s) * asz + o) + __ldg (adj + (long long) (A.lams_idx + s) * asz + o);
-            if (!(sST[(s * SR + jj + 3) * SC + cc + 3] > 0.0)) v = 0.0;   // d max(0, n0)
-          }
-          adj[(long long) (A.out_idx + s) * asz + o] = v;
+    for (int q = 0; q < CPT; q++) {
+      const int jj = CPT * wq + q, j = j0 + jj, c = c0 + lane;
+      if (c >= nr || j >= nz) continue;
+      const long long o = AO (c, j);
+#pragma unroll
+      for (int s = 0; s < NS; s++) {
+        double v = out[q][s];
+        if (A.mode == 2) {
+          v += __ldg (adj + (long long) (A.lam_idx + s) * asz + o) + __ldg (adj + (long long) (A.lams_idx + s) * asz + o);
+          if (!(sST[(s * SR + jj + 3) * SC + lane + 3] > 0.0)) v = 0.0;   // d max(0, n0)
         }
+        adj[(long long) (A.out_idx + s) * asz + o] = v;
       }
     }
   }
@@ -462,7 +541,7 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
   __syncthreads ();
   if (t <= NS) {
     double v = 0.0;
-    for (int w = 0; w < NT / 32; w++) v += red[w][t];
+    for (int w = 0; w < NW; w++) v += red[w][t];
     A.g_part[(size_t) blockIdx.x * (NS + 1) + t] += v;
   }
   if (A.tab_smem)

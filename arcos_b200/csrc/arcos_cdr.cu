@@ -869,6 +869,20 @@ vjp_launch_m (int ns, const Model &M, const VjpArgs &A, int blocks, size_t smem,
   }
 }
 
+// Rows of a VJP tile.
+int
+vjp_tile_rows (int ns)
+{
+  switch (ns) {
+  case 1: return VjpTile<1>::VY;
+  case 2: return VjpTile<2>::VY;
+  case 3: return VjpTile<3>::VY;
+  case 4: return VjpTile<4>::VY;
+  case 5: return VjpTile<5>::VY;
+  default: return VjpTile<6>::VY;
+  }
+}
+
 // Shared memory of a VJP block without the table accumulator, in doubles.
 size_t
 vjp_base_doubles (int ns)
@@ -940,16 +954,18 @@ adj_alloc (Ctx *c, int nsteps, int ck)
     std::vector<AdjTile> tl;
     for (int p = 0; p < (int) c->pd_h.size (); p++) {
       const PatchDesc &P = c->pd_h[p];
-      for (int zb = 0; zb < P.nz; zb += VjpTile<1>::VY)
+      for (int zb = 0; zb < P.nz; zb += vjp_tile_rows (ns))
         for (int c0 = 0; c0 < P.nr; c0 += VjpTile<1>::VX) tl.push_back (AdjTile{p, c0, zb, 0});
     }
     c->adj_ntiles = (int) tl.size ();
     CK (cudaMalloc (&c->adj_tiles_d, sizeof (AdjTile) * tl.size ()));
     CK (cudaMemcpy (c->adj_tiles_d, tl.data (), sizeof (AdjTile) * tl.size (), cudaMemcpyHostToDevice));
     const size_t ng = c->nodes_h.size () + 2 * (size_t) c->M.nreact;
-    // the table accumulator joins the block's shared memory while it fits
+    // small tables (up to 4096 entries) accumulate in the block's shared
+    // memory; larger ones take warp-aggregated atomics in global memory, so
+    // that the table does not cost the kernel its resident blocks
     const size_t base = sizeof (double) * vjp_base_doubles (ns), limit = 227 * 1024;
-    c->adj_tab_smem = base + sizeof (double) * ng <= limit ? 1 : 0;
+    c->adj_tab_smem = (ng <= 4096 && base + sizeof (double) * ng <= limit) ? 1 : 0;
     c->adj_smem = base + (c->adj_tab_smem ? sizeof (double) * ng : 0);
     int occ = 0;
     cudaError_t e = vjp_launch_m (ns, c->M, VjpArgs{}, 0, c->adj_smem, 0, &occ);

@@ -150,14 +150,15 @@ table_pos_slow (const TableNode *__restrict__ nd, int steps, double eabs, int k)
   return k;
 }
 
-__device__ __forceinline__ double
-table_rate (const Model &M, const TableNode *__restrict__ nodes, int r, double eabs)
+// Node k of reaction r's table with nd[k].thr <= eabs < nd[k+1].thr, k in
+// [0, steps] (reaction.c:127-136): a single-precision estimate of the
+// position, then one exact correction each way (the estimate is never off by
+// more than one node for tables with e_step above ~1e-4); anything else
+// takes the exact search.
+__device__ __forceinline__ int
+table_index (const Model &M, const TableNode *__restrict__ nd, int r, double eabs)
 {
-  const TableNode *nd = nodes + M.r_node_off[r];
   const int steps = M.r_steps[r];
-  // single-precision estimate of the position, then one exact correction each
-  // way (the estimate is never off by more than one node for tables with
-  // e_step above ~1e-4); anything else takes the exact search
   const float lf = __log10f ((float) eabs);
   const float pf = (lf - (float) M.r_e_min[r]) * M.r_inv_step_f[r];
   int k = (int) fminf (fmaxf (pf, 0.f), (float) steps);
@@ -165,7 +166,15 @@ table_rate (const Model &M, const TableNode *__restrict__ nodes, int r, double e
   k += (k < steps && eabs >= nd[k + 1].thr) ? 1 : 0;
   if ((k > 0 && eabs < nd[k].thr) || (k < steps && eabs >= nd[k + 1].thr))
     k = table_pos_slow (nd, steps, eabs, k);
-  const TableNode n = nd[k];
+  return k;
+}
+
+__device__ __forceinline__ double
+table_rate (const Model &M, const TableNode *__restrict__ nodes, int r, double eabs)
+{
+  const TableNode *nd = nodes + M.r_node_off[r];
+  const int steps = M.r_steps[r];
+  const TableNode n = nd[table_index (M, nd, r, eabs)];
   double rate = n.val + n.slope * (eabs - n.e1);
   rate = (eabs >= nd[steps + 1].thr) ? M.r_over[r] : rate;   // log_e > e_min + e_step*steps
   rate = (eabs >= nd[0].thr) ? rate : M.r_under[r];          // log_e < e_min (or NaN)
