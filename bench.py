@@ -107,7 +107,32 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ CPU baseline ----
+class _CStdoutToStderr:
+    """Sends what C code prints on file descriptor 1 (the reference library's
+    progress lines) to stderr, so that stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        try:
+            C.CDLL(None).fflush(None)
+        except (OSError, AttributeError):
+            pass
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
 def cpu_baseline_sample(omp: bool, seconds: float = 12.0, max_steps: int = 10**9):
+    with _CStdoutToStderr():
+        return _cpu_baseline_sample(omp, seconds, max_steps)
+
+
+def _cpu_baseline_sample(omp: bool, seconds: float, max_steps: int):
     """Reference CPU implementation (oracle/_ref) on a 512 x 64 x 16 slab of
     the workload; returns (cell-species updates/s, threads, kind, steps)."""
     from arcos_b200 import workloads
@@ -146,6 +171,13 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    with _CStdoutToStderr():
+        line = _reference_line(args)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _reference_line(args):
     from oracle import bind
     omp = bind.ref_available(True)
     # each "step" is one RK2 step of the 512 x 64 x 16 slab
@@ -182,8 +214,7 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 # ---------------------------------------------------------------- device ----
@@ -231,6 +262,25 @@ def extra_amr(stream, steps: int = 10):
     out["batched_value"] = pb.cells * 2 / (out["batched_ms_per_step"] / 1e3)
     out["batched_over_per_patch"] = out["per_patch_ms_per_step"] / out["batched_ms_per_step"]
     return out
+
+
+def _time_sweep(tree, stream) -> float:
+    """Device time (CUDA events) of one reverse sweep through the C ABI
+    (arcos_adj_backward: the replayed sweep graph plus the reduction of the
+    mobility, diffusion and table gradients).  The initial-density gradients
+    stay on the device until arcos_adj_get_cotangent fetches them."""
+    import numpy as np
+    from arcos_b200._lib import check
+    ns = tree.model.no_species
+    gm, gd = np.zeros(ns), C.c_double(0.0)
+    gt = np.zeros(max(tree.L.arcos_adj_table_entries(tree.h), 1))
+    e0, e1 = _events(stream)
+    e0.record(stream)
+    check(tree.L.arcos_adj_backward(tree.h, gm.ctypes.data_as(C.POINTER(C.c_double)), C.byref(gd),
+                                    gt.ctypes.data_as(C.POINTER(C.c_double))))
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
 
 
 def extra_adjoint(stream, K: int = 64, ck: int = 8, ndir: int = 32):
@@ -291,11 +341,10 @@ def extra_adjoint(stream, K: int = 64, ck: int = 8, ndir: int = 32):
     g = adj.backward()                      # first call captures the sweep's CUDA graph
     adj.set_cotangent(0, 0, (ne - target) * vol)
     adj.set_cotangent(0, 1, np.zeros_like(ne))
-    e0.record(stream)
+    bwd_ms = _time_sweep(tree, stream)
+    adj.set_cotangent(0, 0, (ne - target) * vol)
+    adj.set_cotangent(0, 1, np.zeros_like(ne))
     g = adj.backward()
-    e1.record(stream)
-    e1.synchronize()
-    bwd_ms = e0.elapsed_time(e1)
     # finite differences
     eps, worst = 1e-6, 0.0
     for _ in range(ndir):
@@ -318,6 +367,7 @@ def extra_adjoint(stream, K: int = 64, ck: int = 8, ndir: int = 32):
     return {"workload": "256x512 grid, 2 species (ions immobile), 64 RK2 steps, checkpoints every 8, "
                         "gradients wrt n_e(0), n_i(0), mobility, diffusion, 256 table values",
             "forward_ms": fwd_ms, "forward_with_checkpoints_ms": fwd_ck_ms, "adjoint_ms": bwd_ms,
+            "adjoint_timed": "one arcos_adj_backward call, CUDA events",
             "adjoint_over_forward": bwd_ms / fwd_ms, "fd_directions": ndir, "fd_step": eps,
             "fd_max_rel_err": worst}
 
@@ -359,16 +409,13 @@ def extra_kinetic(stream, K: int = 20):
         adj.set_cotangent(g, 0, cell_volume(sp, pb.params.dr(0), pb.params.dz(0)))
         for s in range(1, ns):
             adj.set_cotangent(g, s, np.zeros(sp.shape))
-    e0.record(stream)
-    gr = adj.backward()
-    e1.record(stream)
-    e1.synchronize()
-    bwd = e0.elapsed_time(e1)
+    bwd = _time_sweep(tree, stream)
     tree.close()
     return {"workload": f"{len(pb.specs)} instances, {pb.cells} cells, {ns} species, "
                         f"{len(pb.model.reactions)} reactions (1000-entry tables)",
             "cells": pb.cells, "ms_per_step": ms, "value": pb.cells * ns / (ms / 1e3),
             "adjoint_steps": Ka, "adjoint_ms": bwd, "adjoint_over_forward": bwd / (ms * Ka),
+            "adjoint_timed": "one arcos_adj_backward call, CUDA events",
             "table_grad_norm": float(sum(np.linalg.norm(t) for t in gr.tables))}
 
 
