@@ -94,6 +94,8 @@ struct Ctx {
   long long *match_src_d[2] = {nullptr, nullptr}, *match_dst_d[2] = {nullptr, nullptr};
   double *match_tmp_d = nullptr;
   int n_match = 0;
+  double *xfer_d = nullptr;           // packed host image of one array (arcos_upload / download)
+  size_t xfer_bytes = 0;
   double *ext_d = nullptr;            // [ext_r (nfam*MAXPLANES) | ext_t | ext_z (nfam)]
   std::vector<double> famE;           // 3 per family
   arcos_field_fn fn = nullptr;
@@ -1083,6 +1085,26 @@ adj_check (Ctx *c)
   return ARCOS_OK;
 }
 
+// The packed transfer image: grown on demand, kept until the context ends.
+int
+xfer_reserve (Ctx *c, size_t bytes)
+{
+  if (c->xfer_bytes >= bytes) return ARCOS_OK;
+  CK (cudaStreamSynchronize (c->stream));
+  cudaFree (c->xfer_d);
+  c->xfer_d = nullptr;
+  c->xfer_bytes = 0;
+  CK (cudaMalloc (&c->xfer_d, bytes));
+  c->xfer_bytes = bytes;
+  return ARCOS_OK;
+}
+
+unsigned
+xfer_blocks (Ctx *c, long long rows)
+{
+  return (unsigned) std::min<long long> (rows, 16LL * c->num_sms);
+}
+
 }  // namespace
 
 // =============================== C ABI ==========================================
@@ -1157,6 +1179,7 @@ arcos_destroy (void *ctx)
   cudaFree (c->plist_d); cudaFree (c->kids_d); cudaFree (c->strips_d); cudaFree (c->ext_d);
   for (int s = 0; s < 2; s++) { cudaFree (c->match_src_d[s]); cudaFree (c->match_dst_d[s]); }
   cudaFree (c->match_tmp_d);
+  cudaFree (c->xfer_d);
   cudaFree (c->maps_d);
   if (c->own_stream) cudaStreamDestroy (c->own_stream);
   delete c;
@@ -1691,9 +1714,13 @@ arcos_upload (void *ctx, int grid, int set, int kind, int species, const double 
   if (grid < 0 || grid >= (int) c->pd_h.size () || set < 0 || set > 1 || !host || !kind_ok (kind, species, c->M.ns))
     return fail (ARCOS_ERR_ARG, "arcos_upload: bad argument");
   const PatchDesc &P = c->pd_h[grid];
-  const size_t w = sizeof (double) * (P.nr + 4);
-  CK (cudaMemcpy2DAsync (P.arr (set, kind, species), sizeof (double) * P.pitch, host, w, w,
-                         (size_t) (P.nz + 4) * P.planes, cudaMemcpyHostToDevice, c->stream));
+  const long long rows = (long long) (P.nz + 4) * P.planes;
+  if ((r = xfer_reserve (c, sizeof (double) * (size_t) (P.nr + 4) * rows))) return r;
+  CK (cudaMemcpyAsync (c->xfer_d, host, sizeof (double) * (size_t) (P.nr + 4) * rows, cudaMemcpyHostToDevice,
+                       c->stream));
+  k_unpack_rows<<<xfer_blocks (c, rows), 128, 0, c->stream>>> (c->xfer_d, P.arr (set, kind, species), P.nr + 4,
+                                                              rows, P.pitch);
+  CK (cudaGetLastError ());
   CK (cudaStreamSynchronize (c->stream));
   return ARCOS_OK;
 }
@@ -1707,9 +1734,13 @@ arcos_download (void *ctx, int grid, int set, int kind, int species, double *hos
   if (grid < 0 || grid >= (int) c->pd_h.size () || set < 0 || set > 1 || !host || !kind_ok (kind, species, c->M.ns))
     return fail (ARCOS_ERR_ARG, "arcos_download: bad argument");
   const PatchDesc &P = c->pd_h[grid];
-  const size_t w = sizeof (double) * (P.nr + 4);
-  CK (cudaMemcpy2DAsync (host, w, P.arr (set, kind, species), sizeof (double) * P.pitch, w,
-                         (size_t) (P.nz + 4) * P.planes, cudaMemcpyDeviceToHost, c->stream));
+  const long long rows = (long long) (P.nz + 4) * P.planes;
+  if ((r = xfer_reserve (c, sizeof (double) * (size_t) (P.nr + 4) * rows))) return r;
+  k_pack_rows<<<xfer_blocks (c, rows), 128, 0, c->stream>>> (P.arr (set, kind, species), c->xfer_d, P.nr + 4,
+                                                            rows, P.pitch);
+  CK (cudaGetLastError ());
+  CK (cudaMemcpyAsync (host, c->xfer_d, sizeof (double) * (size_t) (P.nr + 4) * rows, cudaMemcpyDeviceToHost,
+                       c->stream));
   CK (cudaStreamSynchronize (c->stream));
   return ARCOS_OK;
 }

@@ -8,6 +8,24 @@
 
 namespace arcos {
 
+// ---- host transfers: rows of w doubles, packed (the host rz_array layout)
+// <-> rows of `pitch` doubles (the device layout).  A host<->device copy moves
+// the packed image linearly and one of these kernels repitches it on the
+// device: a pitched DMA of ~4 KB rows runs well below the link's rate. ----
+__global__ void
+k_unpack_rows (const double *__restrict__ src, double *__restrict__ dst, int w, long long rows, int pitch)
+{
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x)
+    for (int x = threadIdx.x; x < w; x += blockDim.x) dst[r * pitch + x] = src[r * w + x];
+}
+
+__global__ void
+k_pack_rows (const double *__restrict__ src, double *__restrict__ dst, int w, long long rows, int pitch)
+{
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x)
+    for (int x = threadIdx.x; x < w; x += blockDim.x) dst[r * w + x] = src[r * pitch + x];
+}
+
 // ---- A13: cdr_nonegative (cdr.c:703-721): dens = MYMAX(0, dens) over the
 // whole arrays (ghosts included) of every species. ----
 __global__ void
