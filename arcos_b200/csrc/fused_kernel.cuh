@@ -533,8 +533,10 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
           if (wr) {
             outp[(long long) k * pitch] = n1;
             if (A.want_charge) chg[k] += (n1 * M.charge[s]) / T.nt;     // cdr.c:380-381
-            // max of the mobile densities; fmax drops NaN as the key reduction does
-            if (mob && fam_cur >= 0) dmax_local = fmax (dmax_local, clamp0 (n1));
+            // max of the mobile densities; a NaN never compares greater, so it
+            // is dropped as the key reduction does
+            const double n1c = clamp0 (n1);
+            if (mob && fam_cur >= 0 && n1c > dmax_local) dmax_local = n1c;
             neg_local = neg_local || n1 < 0.0;
           }
         }
