@@ -32,6 +32,15 @@ class ArcosParams(C.Structure):
                 ("extra_pois_levels", C.c_int), ("per_plane", C.c_int)]
 
 
+class RefineParams(C.Structure):
+    """``arcos_refine_params`` of include/arcos_cdr.h (the refinement
+    parameters of the reference's src/parameters.h)."""
+    _fields_ = [("threshold_eabs", C.c_double), ("level_eabs", C.c_int),
+                ("threshold_charge", C.c_double), ("threshold_dens", C.c_double),
+                ("threshold_edge", C.c_double), ("brick_dr", C.c_int), ("brick_dz", C.c_int),
+                ("max_level", C.c_int)]
+
+
 FIELD_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, DP, DP, DP, DP)
 
 _lib = None
@@ -97,6 +106,8 @@ def lib():
     L.arcos_adj_backward.argtypes = [VP, DP, DP, DP]
     L.arcos_adj_table_entries.argtypes = [VP]
     L.arcos_adj_table_offset.argtypes = [VP, C.c_int]
+    L.arcos_cdr_refine.argtypes = [VP, C.c_int, C.POINTER(RefineParams), C.c_int,
+                                   C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]
     _lib = L
     return L
 

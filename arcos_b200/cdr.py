@@ -36,7 +36,7 @@ from typing import Callable, List, Optional, Sequence
 
 import numpy as np
 
-from ._lib import DP, FIELD_FN, ArcosParams, check, lib
+from ._lib import DP, FIELD_FN, ArcosParams, RefineParams, check, lib
 from .grids import GridSpec
 from .model import KineticModel, Params
 
@@ -185,6 +185,27 @@ class CdrTree:
     def cdr_add_ext_field_r(self, set=SET_GRID): self._call("arcos_cdr_add_ext_field_r", set)
     def cdr_calc_eabs_r(self, set=SET_GRID): self._call("arcos_cdr_calc_eabs_r", set)
     def cdr_calc_charge_r(self, set=SET_GRID): self._call("arcos_cdr_calc_charge_r", set)
+
+    def cdr_refine(self, gid: int, threshold_eabs: float, level_eabs: int, threshold_charge: float,
+                   threshold_dens: float, threshold_edge: float, brick_dr: int = 8, brick_dz: int = 8,
+                   max_level: int = 4, contains_edge: bool = False) -> List[tuple]:
+        """cdr_refine (src/cdr.c:1630-1682) of grid ``gid``: the children
+        refine_in would create, in creation order, as (r0, z0, r1, z1,
+        contains_edge) in child-level coordinates.  Refine a family's root
+        before its other grids (they inherit its maxima)."""
+        rp = RefineParams(threshold_eabs, level_eabs, threshold_charge, threshold_dens,
+                          threshold_edge, brick_dr, brick_dz, max_level)
+        cap = 64
+        while True:
+            buf = (C.c_int * (5 * cap))()
+            n = C.c_int(0)
+            rc = self.L.arcos_cdr_refine(self.h, self.ids[gid], C.byref(rp), 1 if contains_edge else 0,
+                                         buf, cap, C.byref(n))
+            if rc != 0 and n.value > cap:
+                cap = n.value
+                continue
+            check(rc)
+            return [tuple(buf[5 * i: 5 * i + 5]) for i in range(n.value)]
     def react_apply_all(self, set=SET_GRID): self._call("arcos_react_apply_all", set)
     def cdr_advect_diffu_r(self, set=SET_GRID): self._call("arcos_cdr_advect_diffu_r", set)
     def cdr_calc_d_dens(self, set=SET_GRID): self._call("arcos_cdr_calc_d_dens", set)

@@ -16,6 +16,7 @@
 #include "fused_kernel.cuh"
 #include "adjoint_kernel.cuh"
 #include "aux_kernels.cuh"
+#include "refine_kernel.cuh"
 
 using namespace arcos;
 
@@ -96,6 +97,10 @@ struct Ctx {
   int n_match = 0;
   double *xfer_d = nullptr;           // packed host image of one array (arcos_upload / download)
   size_t xfer_bytes = 0;
+  unsigned short *refine_flags_d = nullptr;   // per-cell refinement masks of one grid
+  size_t refine_cells = 0;
+  unsigned long long *refine_keys_d = nullptr;
+  std::vector<std::vector<double>> refine_max;   // per grid: |charge| max, dens maxima (roots)
   double *ext_d = nullptr;            // [ext_r (nfam*MAXPLANES) | ext_t | ext_z (nfam)]
   std::vector<double> famE;           // 3 per family
   arcos_field_fn fn = nullptr;
@@ -1085,6 +1090,72 @@ adj_check (Ctx *c)
   return ARCOS_OK;
 }
 
+// The brick search of cdr_refine (src/cdr.c:1630-1682) over the per-cell
+// masks of k_refine_flags: needs_refinement (:1459-1563) with its border
+// recursion, any_needs_refinement (:1576-1591), brick_needs_refinement
+// (:1605-1620); the leading-edge flag travels in the reference's order.
+struct RefineReplay {
+  const unsigned short *f;
+  int r0, z0, r1, z1, nt, nmob;     // grid extent (absolute, this level)
+
+  unsigned mask (int ir, int iz, int it) const {
+    return f[((size_t) it * (z1 - z0) + (iz - z0)) * (size_t) (r1 - r0) + (ir - r0)];
+  }
+  bool needs (int ir, int iz, int it, bool &in_edge) const {
+    const unsigned b = mask (ir, iz, it);
+    if (b & 1u) { in_edge = false; return true; }
+    for (int k = 0; k < nmob; k++) {
+      if (b & (1u << (1 + 2 * k))) { in_edge = false; return true; }
+      if (in_edge && (b & (1u << (2 + 2 * k)))) return true;
+    }
+    if (ir == r0 + 1 && needs (ir - 1, iz, it, in_edge)) return true;
+    if (iz == z0 + 1 && needs (ir, iz - 1, it, in_edge)) return true;
+    if (ir == r1 - 2 && needs (ir + 1, iz, it, in_edge)) return true;
+    if (iz == z1 - 2 && needs (ir, iz + 1, it, in_edge)) return true;
+    return false;
+  }
+  bool any_needs (int ir, int iz, bool &in_edge) const {
+    bool ret = false;
+    for (int it = 0; it < nt; it++) {
+      if (needs (ir, iz, it, in_edge)) ret = true;
+      if (ret && !in_edge) return true;
+    }
+    return ret;
+  }
+  bool brick_needs (int br0, int bz0, int br1, int bz1, bool &in_edge) const {
+    bool ret = false;
+    for (int ir = br0; ir < br1; ir++)
+      for (int iz = bz1 - 1; iz >= bz0; iz--) {
+        ret = any_needs (ir, iz, in_edge) || ret;
+        if (ret && !in_edge) return true;
+      }
+    return ret;
+  }
+  // the children refine_in (:1690-1708) would add, in creation order
+  void refine (int bdr, int bdz, bool contains_edge, std::vector<int> &out) const {
+    for (int ir = r0; ir < r1; ir += bdr) {
+      const int irmax = std::min (r1, ir + bdr);
+      bool building = false, in_edge = contains_edge, first_edge = contains_edge;
+      int cz0 = -1, cz1 = -1;
+      auto add = [&] () {
+        const int v[5] = {ir << 1, cz0 << 1, irmax << 1, cz1 << 1, in_edge ? 1 : 0};
+        out.insert (out.end (), v, v + 5);
+      };
+      for (int iz = z0; iz < z1; iz += bdz) {
+        const int izmax = std::min (z1, iz + bdz);
+        if (brick_needs (ir, iz, irmax, izmax, first_edge)) {
+          cz1 = izmax;
+          if (!building) { cz0 = iz; building = true; }
+        } else if (building) {
+          building = false;
+          if (!first_edge) { add (); in_edge = false; }
+        }
+      }
+      if (building && !first_edge) add ();
+    }
+  }
+};
+
 // The packed transfer image: grown on demand, kept until the context ends.
 int
 xfer_reserve (Ctx *c, size_t bytes)
@@ -1092,6 +1163,8 @@ xfer_reserve (Ctx *c, size_t bytes)
   if (c->xfer_bytes >= bytes) return ARCOS_OK;
   CK (cudaStreamSynchronize (c->stream));
   cudaFree (c->xfer_d);
+  cudaFree (c->refine_flags_d);
+  cudaFree (c->refine_keys_d);
   c->xfer_d = nullptr;
   c->xfer_bytes = 0;
   CK (cudaMalloc (&c->xfer_d, bytes));
@@ -1855,6 +1928,81 @@ arcos_cdr_calc_eabs_r (void *ctx, int set)
   return for_patches (c, w, [&] (dim3 g, const int *pl) {
     k_eabs<<<g, 256, 0, c->stream>>> (c->pd_d, pl, set, c->st_d);
   });
+}
+
+int
+arcos_cdr_refine (void *ctx, int grid, const arcos_refine_params *rp, int contains_edge,
+                  int *rects, int max_rects, int *n_rects)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (!rp || !n_rects || (max_rects > 0 && !rects) || grid < 0 || grid >= (int) c->pd_h.size ()
+      || rp->brick_dr < 1 || rp->brick_dz < 1)
+    return fail (ARCOS_ERR_ARG, "arcos_cdr_refine: bad argument");
+  const PatchDesc &P = c->pd_h[grid];
+  *n_rects = 0;
+  if (P.level >= rp->max_level) return ARCOS_OK;             // cdr.c:1636
+  if (P.nr < 3 || P.nz < 3) return fail (ARCOS_ERR_ARG, "arcos_cdr_refine: grid narrower than 3 cells");
+  const int ns = c->M.ns;
+  if (c->refine_max.size () != c->pd_h.size ()) c->refine_max.assign (c->pd_h.size (), {});
+  const size_t cells = (size_t) P.nr * P.nz * P.ntheta;
+  if (c->refine_cells < cells) {
+    CK (cudaStreamSynchronize (c->stream));
+    cudaFree (c->refine_flags_d);
+    c->refine_flags_d = nullptr;
+    c->refine_cells = 0;
+    CK (cudaMalloc (&c->refine_flags_d, sizeof (unsigned short) * cells));
+    c->refine_cells = cells;
+  }
+  if (!c->refine_keys_d) CK (cudaMalloc (&c->refine_keys_d, sizeof (unsigned long long) * (1 + ARCOS_MAXS)));
+  RefineArgs A{};
+  A.patch = grid;
+  A.flags = c->refine_flags_d;
+  A.keys = c->refine_keys_d;
+  const unsigned blocks = (unsigned) std::max<size_t> (1, std::min<size_t> ((cells + 255) / 256, 8 * (size_t) c->num_sms));
+  // cdr_calc_maxs: a root computes its maxima, other grids inherit the root's
+  int root = grid;
+  while (c->pd_h[root].parent >= 0) root = c->pd_h[root].parent;
+  if (root == grid) {
+    CK (cudaMemsetAsync (c->refine_keys_d, 0, sizeof (unsigned long long) * (1 + ARCOS_MAXS), c->stream));
+    k_refine_max<<<blocks, 256, 0, c->stream>>> (c->M, c->pd_d, A);
+    CK (cudaGetLastError ());
+    unsigned long long keys[1 + ARCOS_MAXS];
+    CK (cudaMemcpyAsync (keys, c->refine_keys_d, sizeof (keys), cudaMemcpyDeviceToHost, c->stream));
+    CK (cudaStreamSynchronize (c->stream));
+    std::vector<double> m (1 + ns);
+    for (int i = 0; i <= ns; i++) m[i] = dkey_inv (keys[i]);
+    c->refine_max[grid] = m;
+  } else if (c->refine_max[root].empty ()) {
+    return fail (ARCOS_ERR_STATE, "arcos_cdr_refine: refine the family's root first (its maxima are inherited)");
+  }
+  const std::vector<double> &m = c->refine_max[root];
+  A.eabs_on = P.level < rp->level_eabs;
+  A.charge_on = m[0] > 1e-8;                                  // epsilon_charge, cdr.c:1470
+  A.thr_eabs = rp->threshold_eabs;
+  A.thr_charge = rp->threshold_charge;
+  A.thr_dens = rp->threshold_dens;
+  A.thr_edge = rp->threshold_edge;
+  A.max_charge = m[0];
+  for (int s = 0; s < ns; s++) A.max_dens[s] = m[1 + s];
+  k_refine_flags<<<blocks, 256, 0, c->stream>>> (c->M, c->pd_d, A);
+  CK (cudaGetLastError ());
+  std::vector<unsigned short> f (cells);
+  CK (cudaMemcpyAsync (f.data (), c->refine_flags_d, sizeof (unsigned short) * cells, cudaMemcpyDeviceToHost,
+                       c->stream));
+  CK (cudaStreamSynchronize (c->stream));
+  RefineReplay R;
+  R.f = f.data ();
+  R.r0 = P.r0; R.z0 = P.z0; R.r1 = P.r0 + P.nr; R.z1 = P.z0 + P.nz; R.nt = P.ntheta;
+  R.nmob = 0;
+  for (int s = 0; s < ns; s++) R.nmob += c->M.mobile[s] ? 1 : 0;
+  std::vector<int> out;
+  R.refine (rp->brick_dr, rp->brick_dz, contains_edge != 0, out);
+  *n_rects = (int) (out.size () / 5);
+  if (*n_rects > max_rects) return fail (ARCOS_ERR_ARG, "arcos_cdr_refine: more children than max_rects");
+  std::copy (out.begin (), out.end (), rects);
+  return ARCOS_OK;
 }
 
 // react_apply_all alone: d_dens = reactions (interior), no drift/diffusion.

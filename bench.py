@@ -419,6 +419,78 @@ def extra_kinetic(stream, K: int = 20):
             "table_grad_norm": float(sum(np.linalg.norm(t) for t in gr.tables))}
 
 
+# the reference's default refinement parameters (src/cstream.c:165-182)
+REFINE_DEFAULTS = dict(threshold_eabs=0.2, level_eabs=4, threshold_charge=0.004, threshold_dens=0.004,
+                       threshold_edge=1e4, brick_dr=8, brick_dz=8, max_level=3)
+
+
+def _refine_state(tree_like, pb, upload):
+    """Seeded state of the refinement row: the plain workload's densities
+    with the ions perturbed (so the charge has structure) and a smooth |E|
+    that exceeds the default threshold (0.2) only around its peak."""
+    import numpy as np
+    d0, d1 = pb.dens[0]
+    sp = pb.specs[0]
+    z = (np.arange(sp.nz + 4) - 2 + 0.5) / sp.nz
+    r = (np.arange(sp.nr + 4) - 2 + 0.5) / sp.nr
+    d1 = d1 * (1.0 + 0.2 * np.sin(6.0 * z))[None, :, None]
+    peak = np.exp(-(r[None, :] ** 2 + (z[:, None] - 0.6) ** 2) / (2 * 0.1 ** 2))
+    eabs = np.broadcast_to((0.1 + 0.3 * peak)[None], d0.shape).copy()
+    upload(d0, d1, eabs)
+
+
+def extra_refine(stream, calls: int = 5):
+    """Refinement criteria (cdr_refine, src/cdr.c:1630-1682) of the
+    512 x 1024 x 16 grid with the reference's default parameters: one
+    arcos_cdr_refine call (per-cell masks on the device, masks to the host,
+    the brick search on the host) against the reference's cdr_refine on a
+    512 x 64 x 16 slab on one host core, as cells per second."""
+    import numpy as np
+    from arcos_b200 import workloads
+    from arcos_b200.cdr import CdrTree
+    from oracle import bind
+    pb = workloads.plain(nr=NR, nz=NZ, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=0)
+    tree = CdrTree(pb.params, pb.model, pb.specs, stream=stream.cuda_stream)
+    tree.set_fixed_field(pb.fields)
+
+    def up(d0, d1, eabs):
+        tree.upload(0, "dens", d0, 0)
+        tree.upload(0, "dens", d1, 1)
+        tree.cdr_set_ext_bnd_r()
+        tree.cdr_calc_charge_r()
+        tree.upload(0, "eabs", eabs)
+    _refine_state(tree, pb, up)
+    kids = tree.cdr_refine(0, **REFINE_DEFAULTS)
+    stream.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        tree.cdr_refine(0, **REFINE_DEFAULTS)
+    dev_s = (time.perf_counter() - t0) / calls
+    cells = NR * NZ * NTHETA
+    tree.close()
+    out = {"workload": f"{NR}x{NZ}x{NTHETA} grid, seeded blobs, reference default refinement parameters",
+           "children": len(kids), "device_call_ms": dev_s * 1e3, "device_cells_per_s": cells / dev_s}
+    if bind.ref_available(False):
+        with _CStdoutToStderr():
+            spb = workloads.plain(nr=NR, nz=SAMPLE_NZ, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=0)
+            ref = bind.RefTree(spb.params, spb.model, spb.specs, field_mode=bind.FIELD_FIXED)
+
+            def rup(d0, d1, eabs):
+                ref.dens(0, 0)[...] = d0
+                ref.dens(0, 1)[...] = d1
+                ref.call("ref_set_ext_bnd_r")
+                ref.call("ref_calc_charge_r")
+                ref.array(0, "eabs")[...] = eabs
+            _refine_state(ref, spb, rup)
+            ref.cdr_refine(0, **REFINE_DEFAULTS)
+            t0 = time.perf_counter()
+            ref.cdr_refine(0, **REFINE_DEFAULTS)
+            ref_s = time.perf_counter() - t0
+        out["reference_cells_per_s"] = NR * SAMPLE_NZ * NTHETA / ref_s
+        out["reference_sample"] = f"one cdr_refine of a {NR}x{SAMPLE_NZ}x{NTHETA} slab, 1 core"
+    return out
+
+
 def run_device(args):
     import ctypes as C
 
@@ -563,7 +635,7 @@ def run_device(args):
     if rank == 0 and not args.no_extras:
         wanted = set(args.extras.split(","))
         for name, fn in (("amr_batched", extra_amr), ("adjoint", extra_adjoint),
-                         ("kinetic_batch", extra_kinetic)):
+                         ("kinetic_batch", extra_kinetic), ("refine", extra_refine)):
             if name not in wanted:
                 continue
             try:
@@ -604,7 +676,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-AMR, adjoint and kinetic-batch measurements")
-    ap.add_argument("--extras", default="amr_batched,adjoint,kinetic_batch",
+    ap.add_argument("--extras", default="amr_batched,adjoint,kinetic_batch,refine",
                     help="comma-separated subset of the extra measurements")
     ap.add_argument("--exact", action="store_true", help="bit-exact flux limiter")
     ap.add_argument("--tile", type=int, default=None,

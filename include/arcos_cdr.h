@@ -138,6 +138,35 @@ int arcos_cdr_match_r (void *ctx, int set);                 /* cdr.c:1763-1882 *
 int arcos_prepare_grid (void *ctx, int set);                /* cdr.c:1334-1351 */
 int arcos_cdr_add_ext_field_r (void *ctx, int set);         /* cdr.c:595-625 */
 int arcos_cdr_calc_eabs_r (void *ctx, int set);             /* cdr.c:668-695 */
+
+/* Refinement criteria (the refinement parameters of src/parameters.h:31-56;
+ * sprite-dependent thresholds are not supported). */
+typedef struct {
+  double threshold_eabs;     /* ref_threshold_eabs */
+  int level_eabs;            /* ref_level_eabs */
+  double threshold_charge;   /* ref_threshold_charge */
+  double threshold_dens;     /* ref_threshold_dens */
+  double threshold_edge;     /* ref_threshold_edge */
+  int brick_dr, brick_dz;    /* cdr_brick_dr, cdr_brick_dz */
+  int max_level;             /* cdr_max_level */
+} arcos_refine_params;
+
+/* cdr_refine (src/cdr.c:1630-1682) on grid `grid` (set 0), with
+ * needs_refinement (:1459-1563), curv_at (:1428-1453) and cdr_calc_maxs
+ * (:1383-1417): the per-cell tests run on the device, the brick search on
+ * the host.  Instead of adding children to a tree it returns the rectangles
+ * refine_in (:1690-1708) would create, in creation order, five ints each:
+ * r0, z0, r1, z1 (child level coordinates) and contains_edge.  A root grid
+ * computes the maxima of |charge| and of every density; another grid uses
+ * those of its root's last call, as the reference's children inherit them
+ * from their parents.  The caller keeps charge, eabs and the density ghosts
+ * current (arcos_cdr_calc_charge_r, arcos_cdr_calc_eabs_r, the ghost fill),
+ * as the reference's cdr_refine_r does.  Grids narrower than three cells
+ * in r or z return ARCOS_ERR_ARG (the reference's border recursion does not
+ * end there); more than max_rects children return ARCOS_ERR_ARG with
+ * *n_rects set to the number needed. */
+int arcos_cdr_refine (void *ctx, int grid, const arcos_refine_params *rp, int contains_edge,
+                      int *rects, int max_rects, int *n_rects);
 int arcos_cdr_calc_charge_r (void *ctx, int set);           /* cdr.c:361-389 */
 int arcos_react_apply_all (void *ctx, int set);             /* reaction.c:192-211 */
 int arcos_cdr_advect_diffu_r (void *ctx, int set);          /* cdr.c:900-955 */

@@ -115,6 +115,9 @@ def ref_lib(omp: bool = False):
                                        C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                        C.c_int, C.c_int]
         lib.ref_set_field_mode.argtypes = [C.c_int, C.c_int]
+        lib.ref_set_refine_params.argtypes = [C.c_double, C.c_int, C.c_double, C.c_double,
+                                              C.c_double, C.c_int, C.c_int, C.c_int]
+        lib.ref_cdr_refine.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int]
         _ref = lib
     return _ref
 
@@ -313,6 +316,20 @@ class RefTree(_TreeBase):
 
     def courant(self):
         return self.lib.ref_courant(self.gids[0])
+
+    def cdr_refine(self, gid: int, threshold_eabs: float, level_eabs: int, threshold_charge: float,
+                   threshold_dens: float, threshold_edge: float, brick_dr: int = 8, brick_dz: int = 8,
+                   max_level: int = 4, contains_edge: bool = False):
+        """The reference's cdr_refine (src/cdr.c:1630-1682) on grid ``gid``:
+        the children it creates, in creation order, as (r0, z0, r1, z1,
+        contains_edge); the tree is left unchanged."""
+        self.lib.ref_set_refine_params(threshold_eabs, level_eabs, threshold_charge, threshold_dens,
+                                       threshold_edge, brick_dr, brick_dz, max_level)
+        cap = 4096
+        buf = (C.c_int * (5 * cap))()
+        n = self.lib.ref_cdr_refine(self.gids[gid], int(contains_edge), buf, cap)
+        assert n <= cap
+        return [tuple(buf[5 * i: 5 * i + 5]) for i in range(n)]
 
 
 def poisson_field(nr: int, nz: int, dr: float, dz: float, charge: np.ndarray):

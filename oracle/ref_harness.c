@@ -300,6 +300,53 @@ ref_set_fixed_field (int gid, const double *er, const double *ez, const double *
 }
 
 /* ---- entry points into the reference ---- */
+/* Refinement (cdr_refine, src/cdr.c:1630-1682): the parameters of
+ * src/parameters.h, and one call that returns the children it created, in
+ * creation order, as (r0, z0, r1, z1, contains_edge), then detaches and
+ * frees them so the tree is left as it was. */
+void
+ref_set_refine_params (double thr_eabs, int level_eabs, double thr_charge, double thr_dens,
+                       double thr_edge, int brick_dr, int brick_dz, int max_level)
+{
+  ref_threshold_eabs = thr_eabs;
+  ref_level_eabs = level_eabs;
+  ref_threshold_charge = thr_charge;
+  ref_threshold_dens = thr_dens;
+  ref_threshold_edge = thr_edge;
+  cdr_brick_dr = brick_dr;
+  cdr_brick_dz = brick_dz;
+  cdr_max_level = max_level;
+}
+
+int
+ref_cdr_refine (int gid, int contains_edge, int *out, int max_out)
+{
+  cdr_grid_t *g = grids[gid], *old_first = g->first_child, *ch, *next;
+  cdr_grid_t *made[4096];
+  int n = 0, i;
+  g->contains_edge = contains_edge;
+  cdr_refine (g);
+  /* add_child prepends: the new children precede the old first child */
+  for (ch = g->first_child; ch && ch != old_first; ch = ch->next) {
+    if (n < 4096) made[n] = ch;
+    n++;
+  }
+  for (i = 0; i < n && i < 4096; i++) {
+    cdr_grid_t *c = made[n - 1 - i];
+    if (i < max_out) {
+      out[5 * i + 0] = c->r0; out[5 * i + 1] = c->z0;
+      out[5 * i + 2] = c->r1; out[5 * i + 3] = c->z1;
+      out[5 * i + 4] = c->contains_edge;
+    }
+  }
+  for (ch = g->first_child; ch && ch != old_first; ch = next) {
+    next = ch->next;
+    cdr_free (ch);
+  }
+  g->first_child = old_first;
+  return n;
+}
+
 double ref_cdr_rk2 (int gid, double h, double t) { return cdr_rk2 (grids[gid], h, t); }
 void ref_calc_charge_r (int gid) { cdr_calc_charge_r (grids[gid]); }
 void ref_nonegative_r (int gid) { cdr_nonegative_r (grids[gid]); }
