@@ -100,6 +100,10 @@ struct Ctx {
   unsigned short *refine_flags_d = nullptr;   // per-cell refinement masks of one grid
   size_t refine_cells = 0;
   unsigned long long *refine_keys_d = nullptr;
+  unsigned char *refine_active_d = nullptr;   // per brick: the search can have an effect
+  size_t refine_bricks = 0;
+  unsigned short *refine_flags_h = nullptr;   // pinned copy of the masks
+  size_t refine_flags_h_cells = 0;
   std::vector<std::vector<double>> refine_max;   // per grid: |charge| max, dens maxima (roots)
   double *ext_d = nullptr;            // [ext_r (nfam*MAXPLANES) | ext_t | ext_z (nfam)]
   std::vector<double> famE;           // 3 per family
@@ -1096,6 +1100,7 @@ adj_check (Ctx *c)
 // (:1605-1620); the leading-edge flag travels in the reference's order.
 struct RefineReplay {
   const unsigned short *f;
+  const unsigned char *active;      // per brick (row-major over brick rows), or null: all
   int r0, z0, r1, z1, nt, nmob;     // grid extent (absolute, this level)
 
   unsigned mask (int ir, int iz, int it) const {
@@ -1143,7 +1148,9 @@ struct RefineReplay {
       };
       for (int iz = z0; iz < z1; iz += bdz) {
         const int izmax = std::min (z1, iz + bdz);
-        if (brick_needs (ir, iz, irmax, izmax, first_edge)) {
+        const size_t b = (size_t) ((iz - z0) / bdz) * (size_t) ((r1 - r0 + bdr - 1) / bdr) + (size_t) ((ir - r0) / bdr);
+        const bool live = !active || active[b];
+        if (live && brick_needs (ir, iz, irmax, izmax, first_edge)) {
           cz1 = izmax;
           if (!building) { cz0 = iz; building = true; }
         } else if (building) {
@@ -1165,6 +1172,8 @@ xfer_reserve (Ctx *c, size_t bytes)
   cudaFree (c->xfer_d);
   cudaFree (c->refine_flags_d);
   cudaFree (c->refine_keys_d);
+  cudaFree (c->refine_active_d);
+  cudaFreeHost (c->refine_flags_h);
   c->xfer_d = nullptr;
   c->xfer_bytes = 0;
   CK (cudaMalloc (&c->xfer_d, bytes));
@@ -1988,12 +1997,35 @@ arcos_cdr_refine (void *ctx, int grid, const arcos_refine_params *rp, int contai
   for (int s = 0; s < ns; s++) A.max_dens[s] = m[1 + s];
   k_refine_flags<<<blocks, 256, 0, c->stream>>> (c->M, c->pd_d, A);
   CK (cudaGetLastError ());
-  std::vector<unsigned short> f (cells);
-  CK (cudaMemcpyAsync (f.data (), c->refine_flags_d, sizeof (unsigned short) * cells, cudaMemcpyDeviceToHost,
+  const size_t nbricks = (size_t) ((P.nr + rp->brick_dr - 1) / rp->brick_dr) * ((P.nz + rp->brick_dz - 1) / rp->brick_dz);
+  if (c->refine_bricks < nbricks) {
+    CK (cudaStreamSynchronize (c->stream));
+    cudaFree (c->refine_active_d);
+    c->refine_active_d = nullptr;
+    c->refine_bricks = 0;
+    CK (cudaMalloc (&c->refine_active_d, nbricks));
+    c->refine_bricks = nbricks;
+  }
+  if (c->refine_flags_h_cells < cells) {
+    CK (cudaStreamSynchronize (c->stream));
+    cudaFreeHost (c->refine_flags_h);
+    c->refine_flags_h = nullptr;
+    c->refine_flags_h_cells = 0;
+    CK (cudaMallocHost (&c->refine_flags_h, sizeof (unsigned short) * cells));
+    c->refine_flags_h_cells = cells;
+  }
+  CK (cudaMemsetAsync (c->refine_active_d, 0, nbricks, c->stream));
+  k_refine_bricks<<<blocks, 256, 0, c->stream>>> (c->pd_d, grid, c->refine_flags_d, rp->brick_dr, rp->brick_dz,
+                                                  c->refine_active_d);
+  CK (cudaGetLastError ());
+  std::vector<unsigned char> active (nbricks);
+  CK (cudaMemcpyAsync (active.data (), c->refine_active_d, nbricks, cudaMemcpyDeviceToHost, c->stream));
+  CK (cudaMemcpyAsync (c->refine_flags_h, c->refine_flags_d, sizeof (unsigned short) * cells, cudaMemcpyDeviceToHost,
                        c->stream));
   CK (cudaStreamSynchronize (c->stream));
   RefineReplay R;
-  R.f = f.data ();
+  R.f = c->refine_flags_h;
+  R.active = active.data ();
   R.r0 = P.r0; R.z0 = P.z0; R.r1 = P.r0 + P.nr; R.z1 = P.z0 + P.nz; R.nt = P.ntheta;
   R.nmob = 0;
   for (int s = 0; s < ns; s++) R.nmob += c->M.mobile[s] ? 1 : 0;

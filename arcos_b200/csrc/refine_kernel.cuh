@@ -104,4 +104,31 @@ k_refine_flags (const __grid_constant__ Model M, const PatchDesc *__restrict__ p
   }
 }
 
+// Bricks whose search can have an effect: a brick is active when one of its
+// cells has a non-zero mask in its 3 x 3 neighbourhood (any plane).  The
+// search of an inactive brick reads only zero masks, so it answers "not
+// tainted" and leaves the edge flag alone: the host skips it.  The
+// neighbourhood covers the border recursion of needs_refinement, which steps
+// at most one cell in r and one in z towards the grid's edge.
+__global__ void
+k_refine_bricks (const PatchDesc *__restrict__ pd, int patch, const unsigned short *__restrict__ flags,
+                 int bdr, int bdz, unsigned char *__restrict__ active)
+{
+  const PatchDesc &P = pd[patch];
+  const int nr = P.nr, nz = P.nz;
+  const int nbc = (nr + bdr - 1) / bdr;
+  const long long n = (long long) nr * nz * P.ntheta;
+  for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
+    const int ar = (int) (i % nr), az = (int) ((i / nr) % nz);
+    const long long plane = i - (i % ((long long) nr * nz));
+    bool any = false;
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dr = -1; dr <= 1; dr++) {
+        const int r = ar + dr, z = az + dz;
+        if (r >= 0 && r < nr && z >= 0 && z < nz && flags[plane + (long long) z * nr + r]) any = true;
+      }
+    if (any) active[(az / bdz) * nbc + ar / bdr] = 1;    // every writer stores 1
+  }
+}
+
 }  // namespace arcos

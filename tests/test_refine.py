@@ -75,6 +75,8 @@ CASES = [
     (1e9, 0, 1e9, 0.05, 1e-2, 8, 8, True),
     (1e9, 0, 1e9, 0.01, 1e-4, 8, 8, True),
     (1e9, 0, 0.01, 0.02, 1e-3, 5, 7, True),
+    (1e9, 0, 1e9, 0.01, 1e-4, 1, 2, True),          # one-cell bricks: the border recursion crosses bricks
+    (1e9, 0, 0.02, 0.03, 1e9, 3, 1, False),
 ]
 
 
