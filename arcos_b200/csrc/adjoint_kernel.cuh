@@ -453,31 +453,50 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
             k = (e >= nd[0].thr) ? k : M.r_under[r];
             // inputs |n_in| from the staged state (clamped in mode 2)
             const double *stq = sST + (CPT * wq + q + 3) * SC + lane + 3;
-            double av[ARCOS_MAXIN], sv[ARCOS_MAXIN];
-            int sp[ARCOS_MAXIN];
-            double prod = 1.0;
-#pragma unroll
-            for (int i = 0; i < ARCOS_MAXIN; i++) {
-              const int si = i < nin ? M.r_in[r][i] : 0;
-              sp[i] = i < nin ? si : -1;
-              const double v = i < nin ? stq[si * (SR * SC)] : 1.0;
-              sv[i] = v;
-              av[i] = fabs (v);
-              prod *= av[i];
-            }
             // d/dn_s of k prod |n_in|: per input, k sign(n) prod of the others
             const double rk = rho * k;
-#pragma unroll
-            for (int i = 0; i < ARCOS_MAXIN; i++) {
-              double others = 1.0;
-#pragma unroll
-              for (int p = 0; p < ARCOS_MAXIN; p++)
-                if (p != i) others *= av[p];
-              const double sgn = sv[i] > 0.0 ? 1.0 : (sv[i] < 0.0 ? -1.0 : 0.0);
-              const double d = rk * sgn * others;
+            auto sgn = [] (double v) -> double { return v > 0.0 ? 1.0 : (v < 0.0 ? -1.0 : 0.0); };
+            double prod;
+            if (nin == 1 || nin == 2) {                 // one or two inputs: no generic loops
+              const int s0 = M.r_in[r][0], s1 = nin == 2 ? M.r_in[r][1] : s0;
+              const double v0 = stq[s0 * (SR * SC)];
+              const double v1 = nin == 2 ? stq[s1 * (SR * SC)] : 1.0;
+              const double a0 = fabs (v0), a1 = fabs (v1);
+              prod = a0 * a1;
+              const double d0 = rk * sgn (v0) * a1;
 #pragma unroll
               for (int s = 0; s < NS; s++)
-                if (s == sp[i]) out[q][s] += d;
+                if (s == s0) out[q][s] += d0;
+              if (nin == 2) {
+                const double d1 = rk * sgn (v1) * a0;
+#pragma unroll
+                for (int s = 0; s < NS; s++)
+                  if (s == s1) out[q][s] += d1;
+              }
+            } else {
+              double av[ARCOS_MAXIN], sv[ARCOS_MAXIN];
+              int sp[ARCOS_MAXIN];
+              prod = 1.0;
+#pragma unroll
+              for (int i = 0; i < ARCOS_MAXIN; i++) {
+                const int si = i < nin ? M.r_in[r][i] : 0;
+                sp[i] = i < nin ? si : -1;
+                const double v = i < nin ? stq[si * (SR * SC)] : 1.0;
+                sv[i] = v;
+                av[i] = fabs (v);
+                prod *= av[i];
+              }
+#pragma unroll
+              for (int i = 0; i < ARCOS_MAXIN; i++) {
+                double others = 1.0;
+#pragma unroll
+                for (int p = 0; p < ARCOS_MAXIN; p++)
+                  if (p != i) others *= av[p];
+                const double d = rk * sgn (sv[i]) * others;
+#pragma unroll
+                for (int s = 0; s < NS; s++)
+                  if (s == sp[i]) out[q][s] += d;
+              }
             }
             // table entries: rate = v1 + (v2 - v1) (E - e1) / (e2 - e1) (reaction.c:142)
             const double gr = rho * prod;
