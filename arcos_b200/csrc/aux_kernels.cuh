@@ -425,16 +425,18 @@ k_dmax (const Model M, const PatchDesc *pd, const int *plist, int set, DevState 
 {
   const PatchDesc &P = pd[plist[blockIdx.y]];
   if (P.level != 0) return;
-  const long long total = (long long) P.nr * P.nz * P.ntheta;
+  const int rows = P.nz * P.ntheta;
   unsigned long long km = 0;
-  for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long long) gridDim.x * blockDim.x) {
-    const int ir = (int) (i % P.nr), iz = (int) ((i / P.nr) % P.nz), it = (int) (i / P.nr / P.nz);
-    const long long o = P.off (ir, iz, it);
-    for (int s = 0; s < P.ns; s++) {
-      if (!M.mobile[s]) continue;
-      const double v = clamp0 (P.arr (set, K_DENS, s)[o]);
-      if (v == v) { const unsigned long long kk = dkey (v); km = kk > km ? kk : km; }
+  // blocks over the rows (z, theta), threads along r: no division per cell
+  for (int j = blockIdx.x; j < rows; j += gridDim.x) {
+    const int it = j / P.nz, iz = j - it * P.nz;
+    for (int ir = threadIdx.x; ir < P.nr; ir += blockDim.x) {
+      const long long o = P.off (ir, iz, it);
+      for (int s = 0; s < P.ns; s++) {
+        if (!M.mobile[s]) continue;
+        const double v = clamp0 (P.arr (set, K_DENS, s)[o]);
+        if (v == v) { const unsigned long long kk = dkey (v); km = kk > km ? kk : km; }
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) {

@@ -48,32 +48,41 @@ refine_curv (const PatchDesc &P, const double *__restrict__ a, int ir, int iz, i
 __global__ void
 k_refine_max (const __grid_constant__ Model M, const PatchDesc *__restrict__ pd, RefineArgs A)
 {
+  constexpr int RMAXS = 6;                      // the device kernels take 1..6 species
   const PatchDesc &P = pd[A.patch];
-  const long long n = (long long) P.nr * P.nz * P.ntheta;
-  unsigned long long kc = 0ULL, kd[ARCOS_MAXS];
-  for (int s = 0; s < ARCOS_MAXS; s++) kd[s] = 0ULL;
+  unsigned long long kc = 0ULL, kd[RMAXS];
+#pragma unroll
+  for (int s = 0; s < RMAXS; s++) kd[s] = 0ULL;
   const double *ch = P.arr (0, K_CHARGE);
-  for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
-    const int ir = (int) (i % P.nr), iz = (int) ((i / P.nr) % P.nz), it = (int) (i / ((long long) P.nr * P.nz));
-    const long long o = P.off (ir, iz, it);
-    const unsigned long long k = dkey (fabs (ch[o]));
-    kc = k > kc ? k : kc;
-    for (int s = 0; s < M.ns; s++) {
-      const unsigned long long q = dkey (P.arr (0, K_DENS, s)[o]);
-      kd[s] = q > kd[s] ? q : kd[s];
+  const int rows = P.nz * P.ntheta;
+  for (int j = blockIdx.x; j < rows; j += gridDim.x) {          // blocks over rows, threads along r
+    const int it = j / P.nz, iz = j - it * P.nz;
+    for (int ir = threadIdx.x; ir < P.nr; ir += blockDim.x) {
+      const long long o = P.off (ir, iz, it);
+      const unsigned long long k = dkey (fabs (ch[o]));
+      kc = k > kc ? k : kc;
+#pragma unroll
+      for (int s = 0; s < RMAXS; s++)
+        if (s < M.ns) {
+          const unsigned long long q = dkey (P.arr (0, K_DENS, s)[o]);
+          kd[s] = q > kd[s] ? q : kd[s];
+        }
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long v = __shfl_xor_sync (0xffffffffu, kc, o);
     kc = v > kc ? v : kc;
-    for (int s = 0; s < ARCOS_MAXS; s++) {
+#pragma unroll
+    for (int s = 0; s < RMAXS; s++) {
       const unsigned long long w = __shfl_xor_sync (0xffffffffu, kd[s], o);
       kd[s] = w > kd[s] ? w : kd[s];
     }
   }
   if ((threadIdx.x & 31) == 0) {
     atomicMax (A.keys, kc);
-    for (int s = 0; s < M.ns; s++) atomicMax (A.keys + 1 + s, kd[s]);
+#pragma unroll
+    for (int s = 0; s < RMAXS; s++)
+      if (s < M.ns) atomicMax (A.keys + 1 + s, kd[s]);
   }
 }
 
