@@ -16,9 +16,6 @@ from oracle import bind
 
 pytestmark = pytest.mark.gpu
 
-KINDS = ("dens", "charge", "eabs")
-
-
 def seeded_state(pb, rng):
     """Two offset Gaussian blobs per species (ions shifted, so the charge has
     structure), a smooth |E| with a peak, on every grid of the tree."""
