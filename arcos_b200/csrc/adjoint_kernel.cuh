@@ -210,7 +210,8 @@ struct VjpTile {
 // r = L_r and z = L_z).  Thread (lane, warp) owns column lane and rows
 // CPT warp .. CPT warp + CPT - 1 of the tile.
 template <int NS>
-__global__ void __launch_bounds__ (256)
+// two blocks per SM (32 x 16 tiles) or three (32 x 8 tiles), as shared memory allows
+__global__ void __launch_bounds__ (256, NS <= 3 ? 2 : 3)
 k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
 {
   using L = VjpTile<NS>;
