@@ -198,3 +198,47 @@ def test_fast_limiter_long_run(cuda_device):
     for s in range(2):
         a, b = dev.download(0, "dens", s), port.dens(0, s)
         assert rel_err(a, b) <= 1e-9, rel_err(a, b)
+
+
+@pytest.mark.parametrize("tile", [0, 1, 2])
+@pytest.mark.parametrize("ntheta", [1, 4])
+def test_fused_every_tile_shape(cuda_device, tile, ntheta):
+    """The fused step (division-free limiter) with each tile shape the
+    autotuner can pick, per step against the oracle at 1e-12, then four
+    steps replayed from the step graph."""
+    pb = workloads.plain(nr=40, nz=72, ntheta=ntheta, ion_mass=1.0, noise=1e-3, seed=21)
+    port = port_tree(pb)
+    dev = device_tree(pb, exact=False)
+    dev.set_tile(tile)
+    for _ in range(3):
+        hp = port.rk2(50.0)[0]
+        hd = dev.run(1, 50.0)[0][0]
+        assert abs(hd - hp) <= TOL * hp
+        for s in range(2):
+            a, b = dev.download(0, "dens", s), port.dens(0, s)
+            assert rel_err(a, b) <= TOL, (tile, s, rel_err(a, b))
+            dev.upload(0, "dens", b, s)
+    for _ in range(4):
+        port.rk2(50.0)
+    dev.run(4, 50.0)
+    for s in range(2):
+        assert rel_err(dev.download(0, "dens", s), port.dens(0, s)) <= 4 * TOL
+
+
+@pytest.mark.parametrize("tile", [0, 1, 2])
+def test_kinetic_batch_fused_every_tile_shape(cuda_device, tile):
+    """Six species, nine reactions, three families of different sizes on the
+    fused path with each tile shape, per step against the oracle at 1e-12."""
+    pb = workloads.kinetic_batch(n_inst=3, points=200, sizes_r=(24, 40), sizes_z=(32, 48), seed=1)
+    dev = device_tree(pb, exact=False)
+    dev.set_tile(tile)
+    ports = [port_tree(single_family(pb, i), E=pb.family_E[i]) for i in range(3)]
+    for _ in range(3):
+        hd = dev.run(1, 50.0)
+        for i, port in enumerate(ports):
+            hp = port.rk2(50.0)[0]
+            assert abs(hd[i][0] - hp) <= TOL * hp
+            for s in range(6):
+                a, b = dev.download(i, "dens", s), port.dens(0, s)
+                assert rel_err(a, b) <= TOL, (tile, i, s, rel_err(a, b))
+                dev.upload(i, "dens", b, s)
