@@ -99,6 +99,7 @@ struct VjpArgs {
   double *g_table;      // [nodes] then [under, over] per reaction
   int n_nodes;
   int tab_smem;         // accumulate the table gradients in shared memory (VjpTile::O_TAB)
+  int rates_idx;        // adjoint arrays of the per-cell reaction lookups (k_adj_rates), 3 per reaction
   double *g_part;       // [gridDim.x][ns + 1]: mobility gradients, then diffusion
   const double *colfac;
   double cm[ARCOS_MAXS], ddr[ARCOS_MAXS], ddz[ARCOS_MAXS];
@@ -142,6 +143,52 @@ k_adj_keep (const PatchDesc *__restrict__ pd, int i0, int is)
     double2 *dst = reinterpret_cast<double2 *> (P.adj + (long long) ((set ? is : i0) + s) * P.asz);
     for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride) dst[i] = src[i];
   }
+}
+
+// Per cell and reaction, the table lookup of react_apply (reaction.c:127-142)
+// for the fixed field of the sweep, stored for every transposed stage in
+// adjoint arrays rates_idx + 3 r + {0, 1, 2}: the rate k(|E|); the
+// interpolation weight tt = (|E| - e1) / (e2 - e1); and the table-gradient
+// entry: i_lo (|E| inside the table), i_lo + 0.5 (inside, on the last node,
+// where v2 = v1), or -(under/over entry) - 1 (outside).  |E| as the VJP's
+// reactions take it (cdr.c:681-692).
+__global__ void
+k_adj_rates (const __grid_constant__ Model M, const PatchDesc *__restrict__ pd, const TableNode *__restrict__ nodes,
+             const double *__restrict__ inv_de, int n_nodes, int rates_idx)
+{
+  const PatchDesc &P = pd[blockIdx.y];
+  const int nr = P.nr, nz = P.nz;
+  double *adj = P.adj;
+  const long long asz = P.asz;
+  const double *er = P.arr (0, K_ER), *ez = P.arr (0, K_EZ);
+  for (int j = blockIdx.x; j < nz; j += gridDim.x)
+    for (int c = threadIdx.x; c < nr; c += blockDim.x) {
+      const double e_r = 0.5 * (er[P.off (c, j, 0)] + er[P.off (c - 1, j, 0)]);
+      const double e_z = 0.5 * (ez[P.off (c, j, 0)] + ez[P.off (c, j - 1, 0)]);
+      const double e = sqrt (e_r * e_r + e_z * e_z);
+      const long long o = (long long) (c + 2) + (long long) (j + 2) * P.pitch;
+      for (int r = 0; r < M.nreact; r++) {
+        const int off = M.r_node_off[r], steps = M.r_steps[r];
+        const TableNode *nd = nodes + off;
+        const int kk = table_index (M, nd, r, e);
+        const TableNode n = nd[kk];
+        const bool over = e >= nd[steps + 1].thr, inr = e >= nd[0].thr && !over;
+        double k = n.val + n.slope * (e - n.e1);                       // table_rate
+        k = over ? M.r_over[r] : k;
+        k = (e >= nd[0].thr) ? k : M.r_under[r];
+        double tt = 0.0, cd;
+        if (inr) {
+          tt = (e - n.e1) * inv_de[off + kk];
+          cd = (double) (off + kk) + (kk == steps ? 0.5 : 0.0);
+        } else {
+          cd = -(double) (n_nodes + 2 * r + (over ? 1 : 0)) - 1.0;
+        }
+        double *rp = adj + (long long) (rates_idx + 3 * r) * asz + o;
+        rp[0] = k;
+        rp[asz] = tt;
+        rp[2 * asz] = cd;
+      }
+    }
 }
 
 // f(integral_constant<int, I>) for I = B .. E-1, unrolled at compile time.
@@ -416,26 +463,19 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
     // d_dens[s] += coef[s] rate.  Every lane joins the warp-wide table-gradient
     // reductions ----
     if (M.nreact > 0) {
-      double eabs[CPT], wc[CPT][NS];
+      double wc[CPT][NS];
       bool on[CPT];
 #pragma unroll
       for (int q = 0; q < CPT; q++) {
         const int jj = CPT * wq + q, j = j0 + jj, c = c0 + lane;
         const bool own = c < nr && j < nz;
-        eabs[q] = 1.0;
-        if (own) {
-          const double e_r = 0.5 * (sER[jj * EC + lane + 2] + sER[jj * EC + lane + 1]);     // cdr.c:681-682
-          const double e_z = 0.5 * (sEZ[(jj + 2) * VX + lane] + sEZ[(jj + 1) * VX + lane]); // cdr.c:683-684
-          eabs[q] = sqrt (e_r * e_r + e_z * e_z);
-        }
 #pragma unroll
         for (int s = 0; s < NS; s++) wc[q][s] = own ? sW[(s * WR + jj + 2) * WC + lane + 2] : 0.0;
         on[q] = own && ((double) (Pp->z0 + j) + 0.5) * Pp->dz < M.z_cutoff;
       }
 #pragma unroll 1
       for (int r = 0; r < M.nreact; r++) {
-        const int off = M.r_node_off[r], steps = M.r_steps[r], nin = M.r_nin[r];
-        const TableNode *nd = A.nodes + off;
+        const int nin = M.r_nin[r];
         int i_lo[CPT], i_hi[CPT];
         double g_lo[CPT], g_hi[CPT];
 #pragma unroll
@@ -445,13 +485,9 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
 #pragma unroll
           for (int s = 0; s < NS; s++) rho = __fma_rn ((double) M.r_coef[r][s], wc[q][s], rho);
           if (on[q] && rho != 0.0) {
-            const double e = eabs[q];
-            const int kk = table_index (M, nd, r, e);
-            const TableNode n = nd[kk];
-            const bool over = e >= nd[steps + 1].thr, inr = e >= nd[0].thr && !over;
-            double k = n.val + n.slope * (e - n.e1);                     // table_rate
-            k = over ? M.r_over[r] : k;
-            k = (e >= nd[0].thr) ? k : M.r_under[r];
+            // the lookup of k_adj_rates for this cell
+            const double *rp = adj + (long long) (A.rates_idx + 3 * r) * asz + AO (c0 + lane, j0 + CPT * wq + q);
+            const double k = __ldg (rp), tt = __ldg (rp + asz), cd = __ldg (rp + 2 * asz);
             // inputs |n_in| from the staged state (clamped in mode 2)
             const double *stq = sST + (CPT * wq + q + 3) * SC + lane + 3;
             // d/dn_s of k prod |n_in|: per input, k sign(n) prod of the others
@@ -501,15 +537,15 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
             }
             // table entries: rate = v1 + (v2 - v1) (E - e1) / (e2 - e1) (reaction.c:142)
             const double gr = rho * prod;
-            if (inr) {
-              const double tt = (e - n.e1) * A.inv_de[off + kk];
-              i_lo[q] = off + kk;
+            if (cd >= 0.0) {                            // |E| inside the table
+              const int il = (int) cd;
+              i_lo[q] = il;
               g_lo[q] = gr * (1.0 - tt);
               g_hi[q] = gr * tt;
-              if (kk == steps) { g_lo[q] += g_hi[q]; g_hi[q] = 0.0; }   // last node: v2 = v1
-              else i_hi[q] = off + kk + 1;
+              if (cd != (double) il) { g_lo[q] += g_hi[q]; g_hi[q] = 0.0; }   // last node: v2 = v1
+              else i_hi[q] = il + 1;
             } else {
-              i_lo[q] = A.n_nodes + 2 * r + (over ? 1 : 0);
+              i_lo[q] = (int) (-cd) - 1;
               g_lo[q] = gr;
             }
           }

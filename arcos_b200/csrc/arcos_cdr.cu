@@ -914,7 +914,8 @@ inline int adj_seg_n0 (Ctx *c, int j) { return 3 * c->M.ns + j * c->M.ns; }
 inline int adj_seg_ns (Ctx *c, int j) { return 3 * c->M.ns + (c->adj_ck + j) * c->M.ns; }
 inline int adj_ckpt (Ctx *c, int seg) { return 3 * c->M.ns + (2 * c->adj_ck + seg) * c->M.ns; }
 inline int adj_final (Ctx *c) { return 3 * c->M.ns + (2 * c->adj_ck + c->adj_nseg) * c->M.ns; }
-inline int adj_arrays (Ctx *c) { return adj_final (c) + c->M.ns; }
+inline int adj_rates (Ctx *c) { return adj_final (c) + c->M.ns; }          // 3 per reaction
+inline int adj_arrays (Ctx *c) { return adj_rates (c) + 3 * c->M.nreact; }
 
 // copies the densities of `set` to (to_adj) or from adjoint arrays idx .. idx+ns-1
 int
@@ -1045,6 +1046,7 @@ run_vjp (Ctx *c, int mode, int st_idx, int lam_idx, int lams_idx, int out_idx, i
   A.Ddz = D / dz;
   A.gdz = 1.0 / dz;
   A.tab_smem = c->adj_tab_smem;
+  A.rates_idx = adj_rates (c);
   if (c->M.ns < 1 || c->M.ns > 6) return fail (ARCOS_ERR_ARG, "adjoint: 1..6 species");
   cudaError_t e = vjp_launch_m (c->M.ns, c->M, A, c->adj_blocks, c->adj_smem, c->stream, nullptr);
   if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("vjp launch: ") + cudaGetErrorString (e));
@@ -1063,6 +1065,13 @@ adj_enqueue_sweep (Ctx *c)
   const size_t ng = c->nodes_h.size () + 2 * (size_t) c->M.nreact;
   CK (cudaMemsetAsync (c->adj_gtab_d, 0, sizeof (double) * std::max<size_t> (ng, 1), c->stream));
   CK (cudaMemsetAsync (c->adj_gpart_d, 0, sizeof (double) * (size_t) c->adj_blocks * (ns + 1), c->stream));
+  if (c->M.nreact > 0) {                       // the fixed field's table lookups, once per sweep
+    int nzm = 1;
+    for (auto &P : c->pd_h) nzm = std::max (nzm, P.nz);
+    k_adj_rates<<<dim3 ((unsigned) std::min (nzm, 4 * c->num_sms), (unsigned) c->pd_h.size ()), 128, 0, c->stream>>> (
+        c->M, c->pd_d, c->nodes_d, c->adj_invde_d, (int) c->nodes_h.size (), adj_rates (c));
+    CK (cudaGetLastError ());
+  }
   int lam = 0;
   for (int seg = c->adj_nseg - 1; seg >= 0; seg--) {
     const int k0 = seg * c->adj_ck, k1 = std::min (c->adj_nsteps, k0 + c->adj_ck);
