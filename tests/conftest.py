@@ -17,8 +17,11 @@ def pytest_configure(config):
     if not os.path.exists(port):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "port"], check=True)
     ref = os.path.join(ROOT, "oracle", "_ref", "libarcos_ref.so")
-    if not os.path.exists(ref) and os.path.exists("/root/reference/src/cdr.c"):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    if not os.path.exists(ref):
+        # oracle/Makefile knows where the reference sources are; without them
+        # (a machine that only has the prebuilt files) the build is skipped
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=False,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
 
 
 def gpu_available() -> bool:
