@@ -108,23 +108,32 @@ struct VjpArgs {
   double gdz;
 };
 
-// Adds g to entry idx of a table gradient (idx < 0 or g == 0: nothing); one
-// atomic per warp when every contributing lane targets the same entry.
+// Adds ga to entry ia and gb to entry ib of a table gradient (an index < 0
+// or a zero value: nothing), for a node and the next one: when every
+// contributing lane targets the same two entries, one warp sum each (both in
+// the same shuffle loop) and one atomic each; otherwise per-lane atomics.
 __device__ __forceinline__ void
-warp_add (double *base, int idx, double g)
+warp_add2 (double *base, int ia, double ga, int ib, double gb)
 {
-  const bool on = idx >= 0 && g != 0.0;
-  const unsigned act = __ballot_sync (0xffffffffu, on);
+  const bool on_a = ia >= 0 && ga != 0.0, on_b = ib >= 0 && gb != 0.0;
+  const unsigned act = __ballot_sync (0xffffffffu, on_a || on_b);
   if (!act) return;
   const int leader = __ffs (act) - 1;
-  const int i0 = __shfl_sync (0xffffffffu, idx, leader);
-  if (__all_sync (0xffffffffu, !on || idx == i0)) {
-    double v = on ? g : 0.0;
+  const int a0 = __shfl_sync (0xffffffffu, ia, leader), b0 = __shfl_sync (0xffffffffu, ib, leader);
+  if (__all_sync (0xffffffffu, (!on_a || ia == a0) && (!on_b || ib == b0))) {
+    double va = on_a ? ga : 0.0, vb = on_b ? gb : 0.0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync (0xffffffffu, v, o);
-    if ((int) (threadIdx.x & 31) == leader) atomicAdd (base + i0, v);
-  } else if (on) {
-    atomicAdd (base + idx, g);
+    for (int o = 16; o > 0; o >>= 1) {
+      va += __shfl_xor_sync (0xffffffffu, va, o);
+      vb += __shfl_xor_sync (0xffffffffu, vb, o);
+    }
+    if ((int) (threadIdx.x & 31) == leader) {
+      if (a0 >= 0 && va != 0.0) atomicAdd (base + a0, va);
+      if (b0 >= 0 && vb != 0.0) atomicAdd (base + b0, vb);
+    }
+  } else {
+    if (on_a) atomicAdd (base + ia, ga);
+    if (on_b) atomicAdd (base + ib, gb);
   }
 }
 
@@ -552,16 +561,11 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         }
         if constexpr (CPT == 2) {               // the thread's two cells first, then the warp
           const bool same = i_lo[0] == i_lo[1] && i_hi[0] == i_hi[1];
-          warp_add (gtab, i_lo[0], same ? g_lo[0] + g_lo[1] : g_lo[0]);
-          warp_add (gtab, i_hi[0], same ? g_hi[0] + g_hi[1] : g_hi[0]);
-          warp_add (gtab, same ? -1 : i_lo[1], g_lo[1]);
-          warp_add (gtab, same ? -1 : i_hi[1], g_hi[1]);
+          warp_add2 (gtab, i_lo[0], same ? g_lo[0] + g_lo[1] : g_lo[0], i_hi[0], same ? g_hi[0] + g_hi[1] : g_hi[0]);
+          warp_add2 (gtab, same ? -1 : i_lo[1], g_lo[1], same ? -1 : i_hi[1], g_hi[1]);
         } else {
 #pragma unroll
-          for (int q = 0; q < CPT; q++) {
-            warp_add (gtab, i_lo[q], g_lo[q]);
-            warp_add (gtab, i_hi[q], g_hi[q]);
-          }
+          for (int q = 0; q < CPT; q++) warp_add2 (gtab, i_lo[q], g_lo[q], i_hi[q], g_hi[q]);
         }
       }
     }
