@@ -92,10 +92,12 @@ __global__ void
 k_refine_flags (const __grid_constant__ Model M, const PatchDesc *__restrict__ pd, const __grid_constant__ RefineArgs A)
 {
   const PatchDesc &P = pd[A.patch];
-  const long long n = (long long) P.nr * P.nz * P.ntheta;
   const double *ch = P.arr (0, K_CHARGE), *ea = P.arr (0, K_EABS);
-  for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
-    const int ar = (int) (i % P.nr), az = (int) ((i / P.nr) % P.nz), it = (int) (i / ((long long) P.nr * P.nz));
+  const int rows = P.nz * P.ntheta;
+  for (int jr = blockIdx.x; jr < rows; jr += gridDim.x)          // blocks over rows, threads along r
+  for (int ar = threadIdx.x; ar < P.nr; ar += blockDim.x) {
+    const int it = jr / P.nz, az = jr - it * P.nz;
+    const long long i = (long long) jr * P.nr + ar;                // mask index [theta][z][r]
     const int ir = P.r0 + ar, iz = P.z0 + az;
     const long long o = P.off (ar, az, it);
     unsigned int b = 0;
@@ -126,10 +128,11 @@ k_refine_bricks (const PatchDesc *__restrict__ pd, int patch, const unsigned sho
   const PatchDesc &P = pd[patch];
   const int nr = P.nr, nz = P.nz;
   const int nbc = (nr + bdr - 1) / bdr;
-  const long long n = (long long) nr * nz * P.ntheta;
-  for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
-    const int ar = (int) (i % nr), az = (int) ((i / nr) % nz);
-    const long long plane = i - (i % ((long long) nr * nz));
+  const int rows = nz * P.ntheta;
+  for (int jr = blockIdx.x; jr < rows; jr += gridDim.x)          // blocks over rows, threads along r
+  for (int ar = threadIdx.x; ar < nr; ar += blockDim.x) {
+    const int it = jr / nz, az = jr - it * nz;
+    const long long plane = (long long) it * nr * nz;
     bool any = false;
     for (int dz = -1; dz <= 1; dz++)
       for (int dr = -1; dr <= 1; dr++) {
