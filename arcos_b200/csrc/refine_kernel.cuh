@@ -92,12 +92,10 @@ __global__ void
 k_refine_flags (const __grid_constant__ Model M, const PatchDesc *__restrict__ pd, const __grid_constant__ RefineArgs A)
 {
   const PatchDesc &P = pd[A.patch];
+  const long long n = (long long) P.nr * P.nz * P.ntheta;
   const double *ch = P.arr (0, K_CHARGE), *ea = P.arr (0, K_EABS);
-  const int rows = P.nz * P.ntheta;
-  for (int jr = blockIdx.x; jr < rows; jr += gridDim.x)          // blocks over rows, threads along r
-  for (int ar = threadIdx.x; ar < P.nr; ar += blockDim.x) {
-    const int it = jr / P.nz, az = jr - it * P.nz;
-    const long long i = (long long) jr * P.nr + ar;                // mask index [theta][z][r]
+  for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
+    const int ar = (int) (i % P.nr), az = (int) ((i / P.nr) % P.nz), it = (int) (i / ((long long) P.nr * P.nz));
     const int ir = P.r0 + ar, iz = P.z0 + az;
     const long long o = P.off (ar, az, it);
     unsigned int b = 0;
