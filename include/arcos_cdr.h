@@ -164,7 +164,10 @@ typedef struct {
  * as the reference's cdr_refine_r does.  Grids narrower than three cells
  * in r or z return ARCOS_ERR_ARG (the reference's border recursion does not
  * end there); more than max_rects children return ARCOS_ERR_ARG with
- * *n_rects set to the number needed. */
+ * *n_rects set to the number needed.  The masks live in buffers the context
+ * allocates on first use (device memory and a pinned host copy, 2 bytes per
+ * cell of the largest grid refined) and keeps until arcos_destroy.
+ * Synchronous on the context's stream. */
 int arcos_cdr_refine (void *ctx, int grid, const arcos_refine_params *rp, int contains_edge,
                       int *rects, int max_rects, int *n_rects);
 int arcos_cdr_calc_charge_r (void *ctx, int set);           /* cdr.c:361-389 */
