@@ -95,6 +95,7 @@ struct Ctx {
   long long *match_src_d[2] = {nullptr, nullptr}, *match_dst_d[2] = {nullptr, nullptr};
   double *match_tmp_d = nullptr;
   int n_match = 0;
+  std::vector<DevState> st_stage;     // host copy written to st_d by arcos_run (kept until the copy ran)
   double *xfer_d = nullptr;           // packed host image of one array (arcos_upload / download)
   size_t xfer_bytes = 0;
   unsigned short *refine_flags_d = nullptr;   // per-cell refinement masks of one grid
@@ -2170,7 +2171,21 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
   std::vector<DevState> st0;
   if ((r = read_states (c, st0))) return r;
   const int step0 = st0[0].step;
-  if ((r = set_h_attempt (c, h))) return r;
+  const bool fixed_fused = c->fused_ok && !c->fn;
+  if (fixed_fused) {
+    // set_h_attempt and reset_dmax (slot 0) in one stream-ordered write
+    c->st_stage = st0;
+    for (auto &s : c->st_stage) {
+      s.h_attempt = h;
+      s.dmax_key[s.step & 1] = dkey (-1.0);
+      s.neg[s.step & 1] = 1;                   // a run starts from a state nobody has checked
+      s.neg[(s.step + 1) & 1] = 0;
+    }
+    CK (cudaMemcpyAsync (c->st_d, c->st_stage.data (), sizeof (DevState) * c->nfam, cudaMemcpyHostToDevice,
+                         c->stream));
+  } else if ((r = set_h_attempt (c, h))) {
+    return r;
+  }
   if (!c->fused_ok && !c->fn && !c->per_patch && nsteps > 0) {
     // trees: one step (all its batched launches) captured once, replayed
     if (!c->graph_tree) {
@@ -2219,8 +2234,8 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
     if ((r = do_periodic (c, 0, 1))) return r;
   } else {
     // fixed field: h of the first step from the current state, then pairs of
-    // steps replayed from a CUDA graph (state 0 -> 1 -> 0)
-    if ((r = reset_dmax (c, 0))) return r;
+    // steps replayed from a CUDA graph (state 0 -> 1 -> 0); the dmax slot was
+    // reset with h_attempt above
     if ((r = do_dmax (c, 0, 0))) return r;
     k_cfl<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->M, c->st_d, c->nfam, 0);
     CKL ();
