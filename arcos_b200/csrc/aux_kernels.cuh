@@ -425,20 +425,25 @@ k_dmax (const Model M, const PatchDesc *pd, const int *plist, int set, DevState 
 {
   const PatchDesc &P = pd[plist[blockIdx.y]];
   if (P.level != 0) return;
-  const int rows = P.nz * P.ntheta;
-  unsigned long long km = 0;
+  const int nr = P.nr, nz = P.nz, ns = P.ns, rows = nz * P.ntheta;
+  const long long asz = P.asz;                 // the species arrays of a set are consecutive
+  const double *d0 = P.arr (set, K_DENS, 0);
+  // max over the clamped values, -0 taken as +0 (the ordered keys put +0
+  // above -0) and NaN never greater; -1 while nothing was seen
+  double vm = -1.0;
   // blocks over the rows (z, theta), threads along r: no division per cell
+#pragma unroll 2
   for (int j = blockIdx.x; j < rows; j += gridDim.x) {
-    const int it = j / P.nz, iz = j - it * P.nz;
-    for (int ir = threadIdx.x; ir < P.nr; ir += blockDim.x) {
-      const long long o = P.off (ir, iz, it);
-      for (int s = 0; s < P.ns; s++) {
+    const int it = j / nz, iz = j - it * nz;
+    const double *row = d0 + P.off (0, iz, it);
+    for (int ir = threadIdx.x; ir < nr; ir += blockDim.x)
+      for (int s = 0; s < ns; s++) {
         if (!M.mobile[s]) continue;
-        const double v = clamp0 (P.arr (set, K_DENS, s)[o]);
-        if (v == v) { const unsigned long long kk = dkey (v); km = kk > km ? kk : km; }
+        const double v = clamp0 (row[(long long) s * asz + ir]) + 0.0;
+        vm = v > vm ? v : vm;
       }
-    }
   }
+  unsigned long long km = vm >= 0.0 ? dkey (vm) : 0ULL;
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long y = __shfl_xor_sync (0xffffffffu, km, o);
     km = y > km ? y : km;
