@@ -76,7 +76,7 @@ class CdrTree:
     """One or more grid families resident on the current CUDA device."""
 
     def __init__(self, params: Params, model: KineticModel, specs: Sequence[GridSpec],
-                 per_patch: bool = False, tile: int = 0, stream: Optional[int] = None,
+                 per_patch: bool = False, tile: int = 2, stream: Optional[int] = None,
                  exact: bool = False):
         self.L = lib()
         self.params, self.model, self.specs = params, model, list(specs)

@@ -79,7 +79,7 @@ struct Ctx {
   WorkItem *items_d = nullptr;
   int n_items = 0;
   std::vector<int> item_off, item_cnt;
-  int tile_cfg = 1;                   // index into TILE_WY / TILE_RPW
+  int tile_cfg = 2;                   // index into TILE_WY / TILE_RPW (2: the fastest measured shape)
   int occ[2][2][4][N_TILE_CFG_MAX] = {};
   int stage_eabs = 0;                 // some set holds a non-zero E_theta
   int exact = 0;                      // 1: bit-exact flux limiter, 0: division-free form

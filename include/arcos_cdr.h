@@ -206,8 +206,8 @@ int arcos_set_per_patch (void *ctx, int on);
  * relative per-step agreement. */
 int arcos_set_exact (void *ctx, int on);
 /* Tile shape of the stencil kernel: 0 = 32x16 cells with 128 threads,
- * 1 = 32x32 cells with 256 threads, 2 = 32x16 cells with 256 threads.
- * Any time. */
+ * 1 = 32x32 cells with 256 threads, 2 (default) = 32x16 cells with 256
+ * threads.  Any time. */
 int arcos_set_tile (void *ctx, int cfg);
 /* 1 (default): stage stencil tiles in shared memory with TMA bulk tensor
  * copies; 0: with per-thread cp.async.  Same results either way. */
