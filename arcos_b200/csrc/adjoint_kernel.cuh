@@ -140,7 +140,7 @@ warp_add2 (double *base, int ia, double ga, int ib, double gb)
 // Keeps the state of a recomputed forward step for its transposed stages:
 // every species' density of set 0 (n0) and of set 1 (n*) of patch
 // blockIdx.y into its adjoint arrays i0 + s and is + s (whole arrays).
-__global__ void __launch_bounds__ (256)
+static __global__ void __launch_bounds__ (256)
 k_adj_keep (const PatchDesc *__restrict__ pd, int i0, int is)
 {
   const PatchDesc &P = pd[blockIdx.y];
@@ -161,7 +161,7 @@ k_adj_keep (const PatchDesc *__restrict__ pd, int i0, int is)
 // entry: i_lo (|E| inside the table), i_lo + 0.5 (inside, on the last node,
 // where v2 = v1), or -(under/over entry) - 1 (outside).  |E| as the VJP's
 // reactions take it (cdr.c:681-692).
-__global__ void
+static __global__ void
 k_adj_rates (const __grid_constant__ Model M, const PatchDesc *__restrict__ pd, const TableNode *__restrict__ nodes,
              const double *__restrict__ inv_de, int n_nodes, int rates_idx)
 {

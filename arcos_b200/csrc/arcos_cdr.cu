@@ -17,6 +17,7 @@
 #include "adjoint_kernel.cuh"
 #include "aux_kernels.cuh"
 #include "refine_kernel.cuh"
+#include "launch.cuh"
 
 using namespace arcos;
 
@@ -217,104 +218,20 @@ grid_blocks (long long work, int threads, int cap = 4096)
   return (int) b;
 }
 
-constexpr int NODES_SMEM_MAX = 4 * 1024 / (int) sizeof (TableNode);
-
-// Tile shapes the autotuner chooses from: (warps per block, rows per thread);
-// tiles are 32 columns wide and WY * RPW rows high.
-constexpr int N_TILE_CFG = 3;
-constexpr int TILE_WY[N_TILE_CFG] = {4, 8, 8};
-constexpr int TILE_RPW[N_TILE_CFG] = {4, 4, 2};
-
-template <int NS, int MODE, int WY, int RPW>
-size_t
-stage_smem_t (int n_nodes, int stage_eabs)
-{
-  using LY = TileLayout<NS, MODE, WY, RPW>;
-  size_t b = sizeof (double) * (size_t) ((stage_eabs ? LY::NA : LY::NA - 1) * LY::PLANE + LY::OPP);
-  if (n_nodes > 0 && n_nodes <= NODES_SMEM_MAX) b += sizeof (TableNode) * (size_t) n_nodes;
-  return b;
-}
-
-template <int NS, int MODE, int WY, int RPW, bool FAST>
-cudaError_t
-launch_stage_t (const Model &M, const StageArgs &A, int blocks, cudaStream_t s, int *occ)
-{
-  const size_t sm = stage_smem_t<NS, MODE, WY, RPW> (A.n_nodes, A.stage_eabs);
-  cudaFuncSetAttribute (k_stage<NS, MODE, WY, RPW, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
-  if (occ) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor (occ, k_stage<NS, MODE, WY, RPW, FAST>, 32 * WY, sm);
-    return cudaGetLastError ();
-  }
-  k_stage<NS, MODE, WY, RPW, FAST><<<blocks, 32 * WY, sm, s>>> (M, A);
-  return cudaGetLastError ();
-}
-
-template <int NS, int MODE>
-cudaError_t
-launch_stage_c (int cfg, const Model &M, const StageArgs &A, int blocks, cudaStream_t s, int *occ)
-{
-  const bool fast = !A.exact;
-  switch (cfg) {
-  case 0: return fast ? launch_stage_t<NS, MODE, 4, 4, true> (M, A, blocks, s, occ)
-                      : launch_stage_t<NS, MODE, 4, 4, false> (M, A, blocks, s, occ);
-  case 1: return fast ? launch_stage_t<NS, MODE, 8, 4, true> (M, A, blocks, s, occ)
-                      : launch_stage_t<NS, MODE, 8, 4, false> (M, A, blocks, s, occ);
-  default: return fast ? launch_stage_t<NS, MODE, 8, 2, true> (M, A, blocks, s, occ)
-                       : launch_stage_t<NS, MODE, 8, 2, false> (M, A, blocks, s, occ);
-  }
-}
-
-template <int MODE>
-cudaError_t
-launch_stage_m (int ns, int cfg, const Model &M, const StageArgs &A, int blocks, cudaStream_t s, int *occ)
-{
-  switch (ns) {
-  case 1: return launch_stage_c<1, MODE> (cfg, M, A, blocks, s, occ);
-  case 2: return launch_stage_c<2, MODE> (cfg, M, A, blocks, s, occ);
-  case 3: return launch_stage_c<3, MODE> (cfg, M, A, blocks, s, occ);
-  case 4: return launch_stage_c<4, MODE> (cfg, M, A, blocks, s, occ);
-  case 5: return launch_stage_c<5, MODE> (cfg, M, A, blocks, s, occ);
-  case 6: return launch_stage_c<6, MODE> (cfg, M, A, blocks, s, occ);
-  default: return cudaErrorInvalidValue;
-  }
-}
-
+// The stencil, fused and adjoint kernels are instantiated per species count
+// in launch_ns.cu (one translation unit per count); these dispatch to them.
 cudaError_t
 launch_stage (int mode, int ns, int cfg, const Model &M, const StageArgs &A, int blocks,
               cudaStream_t s, int *occ = nullptr)
 {
-  switch (mode) {
-  case M_DERIV: return launch_stage_m<M_DERIV> (ns, cfg, M, A, blocks, s, occ);
-  case M_S1: return launch_stage_m<M_S1> (ns, cfg, M, A, blocks, s, occ);
-  case M_S2: return launch_stage_m<M_S2> (ns, cfg, M, A, blocks, s, occ);
-  case M_AMR2: return launch_stage_m<M_AMR2> (ns, cfg, M, A, blocks, s, occ);
+  switch (ns) {
+  case 1: return launch_stage_ns<1> (mode, cfg, M, A, blocks, s, occ);
+  case 2: return launch_stage_ns<2> (mode, cfg, M, A, blocks, s, occ);
+  case 3: return launch_stage_ns<3> (mode, cfg, M, A, blocks, s, occ);
+  case 4: return launch_stage_ns<4> (mode, cfg, M, A, blocks, s, occ);
+  case 5: return launch_stage_ns<5> (mode, cfg, M, A, blocks, s, occ);
+  case 6: return launch_stage_ns<6> (mode, cfg, M, A, blocks, s, occ);
   default: return cudaErrorInvalidValue;
-  }
-}
-
-// ---- lean fused kernels (fast limiter, single-grid families) ----
-template <int NS, bool S2, int WY, int RPW>
-cudaError_t
-launch_fused_t (const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
-{
-  const size_t sm = sizeof (double) * 2 * fused_buffer_doubles<NS, WY, RPW> (A.stage_eabs);
-  cudaFuncSetAttribute (k_fused<NS, S2, WY, RPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
-  if (occ) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor (occ, k_fused<NS, S2, WY, RPW>, 32 * WY, sm);
-    return cudaGetLastError ();
-  }
-  k_fused<NS, S2, WY, RPW><<<blocks, 32 * WY, sm, s>>> (M, A);
-  return cudaGetLastError ();
-}
-
-template <int NS, bool S2>
-cudaError_t
-launch_fused_c (int cfg, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
-{
-  switch (cfg) {
-  case 0: return launch_fused_t<NS, S2, 4, 4> (M, A, blocks, s, occ);
-  case 1: return launch_fused_t<NS, S2, 8, 4> (M, A, blocks, s, occ);
-  default: return launch_fused_t<NS, S2, 8, 2> (M, A, blocks, s, occ);
   }
 }
 
@@ -323,12 +240,12 @@ cudaError_t
 launch_fused_m (int ns, int cfg, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
 {
   switch (ns) {
-  case 1: return launch_fused_c<1, S2> (cfg, M, A, blocks, s, occ);
-  case 2: return launch_fused_c<2, S2> (cfg, M, A, blocks, s, occ);
-  case 3: return launch_fused_c<3, S2> (cfg, M, A, blocks, s, occ);
-  case 4: return launch_fused_c<4, S2> (cfg, M, A, blocks, s, occ);
-  case 5: return launch_fused_c<5, S2> (cfg, M, A, blocks, s, occ);
-  case 6: return launch_fused_c<6, S2> (cfg, M, A, blocks, s, occ);
+  case 1: return launch_fused_ns<1> (S2, cfg, M, A, blocks, s, occ);
+  case 2: return launch_fused_ns<2> (S2, cfg, M, A, blocks, s, occ);
+  case 3: return launch_fused_ns<3> (S2, cfg, M, A, blocks, s, occ);
+  case 4: return launch_fused_ns<4> (S2, cfg, M, A, blocks, s, occ);
+  case 5: return launch_fused_ns<5> (S2, cfg, M, A, blocks, s, occ);
+  case 6: return launch_fused_ns<6> (S2, cfg, M, A, blocks, s, occ);
   default: return cudaErrorInvalidValue;
   }
 }
@@ -852,31 +769,16 @@ rk2_fused_launches (Ctx *c, int src, int fold)
 
 
 // ---- discrete adjoint -----------------------------------------------------------
-// Launches k_vjp<NS> (occ == nullptr), or sets its shared-memory limit and
-// returns its resident blocks per SM in *occ.
-template <int NS>
-cudaError_t
-vjp_launch (const Model &M, const VjpArgs &A, int blocks, size_t smem, cudaStream_t st, int *occ)
-{
-  if (occ) {
-    cudaError_t e = cudaFuncSetAttribute (k_vjp<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor (occ, k_vjp<NS>, VjpTile<NS>::NT, smem);
-  }
-  k_vjp<NS><<<blocks, VjpTile<NS>::NT, smem, st>>> (M, A);
-  return cudaGetLastError ();
-}
-
 cudaError_t
 vjp_launch_m (int ns, const Model &M, const VjpArgs &A, int blocks, size_t smem, cudaStream_t st, int *occ)
 {
   switch (ns) {
-  case 1: return vjp_launch<1> (M, A, blocks, smem, st, occ);
-  case 2: return vjp_launch<2> (M, A, blocks, smem, st, occ);
-  case 3: return vjp_launch<3> (M, A, blocks, smem, st, occ);
-  case 4: return vjp_launch<4> (M, A, blocks, smem, st, occ);
-  case 5: return vjp_launch<5> (M, A, blocks, smem, st, occ);
-  case 6: return vjp_launch<6> (M, A, blocks, smem, st, occ);
+  case 1: return launch_vjp_ns<1> (M, A, blocks, smem, st, occ);
+  case 2: return launch_vjp_ns<2> (M, A, blocks, smem, st, occ);
+  case 3: return launch_vjp_ns<3> (M, A, blocks, smem, st, occ);
+  case 4: return launch_vjp_ns<4> (M, A, blocks, smem, st, occ);
+  case 5: return launch_vjp_ns<5> (M, A, blocks, smem, st, occ);
+  case 6: return launch_vjp_ns<6> (M, A, blocks, smem, st, occ);
   default: return cudaErrorInvalidValue;
   }
 }
@@ -2708,30 +2610,61 @@ arcos_cdr_advect_vec_dev (double mass, double charge, const double *dens, double
 // ---- the narrow seam without allocations ----------------------------------
 // All device memory of this entry point is one file-scope array: a header
 // (patch descriptor, E_theta flags, tile list) and the four padded arrays
-// the stencil kernel reads (dens, d_dens, er, ez).  Its address is looked up
-// once per device; every call re-writes what it uses, nothing has to start
-// at zero except the E_theta flags, which each call clears.
+// the stencil kernel reads (dens, d_dens, er, ez).  Its address, the stencil
+// kernel's occupancy and the SM count are looked up once per device, at the
+// first call on that device; every call re-writes what it uses on the device
+// (k_noalloc_header takes the descriptor and the tile shape by value), and
+// nothing has to start at zero except the E_theta flags, which each call
+// clears.
 constexpr size_t NOALLOC_DOUBLES = (size_t) 2 << 20;        // 16 MiB
 constexpr size_t NOALLOC_HEADER = 8192;                       // doubles (64 KiB)
 static __device__ __align__ (256) double g_noalloc_scratch[NOALLOC_DOUBLES];
 constexpr int NOALLOC_MAXDEV = 64;
-static double *g_noalloc_ptr[NOALLOC_MAXDEV];
+struct NoallocDev {
+  double *ptr;                 // device address of g_noalloc_scratch
+  int blocks;                  // resident stencil blocks per SM x SMs
+};
+static NoallocDev g_noalloc[NOALLOC_MAXDEV];
+
+__global__ void
+k_noalloc_header (PatchDesc P, int tx, int ty, int n_items, char *head)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    *reinterpret_cast<PatchDesc *> (head) = P;
+    reinterpret_cast<int *> (head + 256)[0] = 0;          // E_theta flags of both sets
+    reinterpret_cast<int *> (head + 256)[1] = 0;
+  }
+  WorkItem *items = reinterpret_cast<WorkItem *> (head + 512);
+  const int ncol = (P.nr + tx - 1) / tx;
+  for (int i = t; i < n_items; i += gridDim.x * blockDim.x) {
+    const int zb = (i / ncol) * ty, c0 = (i % ncol) * tx;
+    items[i] = WorkItem{0, 0, c0, min (tx, P.nr - c0), zb, min (ty, P.nz - zb)};
+  }
+}
 
 static int
-noalloc_setup (double **out)
+noalloc_setup (const Model &M, const StageArgs &A, NoallocDev **out)
 {
   int dev = 0;
   cudaError_t e = cudaGetDevice (&dev);
   if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("cudaGetDevice: ") + cudaGetErrorString (e));
   if (dev < 0 || dev >= NOALLOC_MAXDEV) return fail (ARCOS_ERR_ARG, "device index above 63");
-  if (!g_noalloc_ptr[dev]) {
+  NoallocDev &d = g_noalloc[dev];
+  if (!d.ptr) {
     void *p = nullptr;
     e = cudaGetSymbolAddress (&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
       return fail (ARCOS_ERR_CUDA, std::string ("cudaGetSymbolAddress (scratch): ") + cudaGetErrorString (e));
-    g_noalloc_ptr[dev] = (double *) p;
+    int occ = 0, sms = 0;
+    e = launch_stage (M_DERIV, 1, 0, M, A, 0, 0, &occ);
+    if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("occupancy: ") + cudaGetErrorString (e));
+    e = cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("SM count: ") + cudaGetErrorString (e));
+    d.blocks = std::max (1, occ) * std::max (1, sms);
+    d.ptr = (double *) p;
   }
-  *out = g_noalloc_ptr[dev];
+  *out = &d;
   return ARCOS_OK;
 }
 
@@ -2753,9 +2686,22 @@ arcos_cdr_advect_vec_dev_noalloc (double mass, double charge, const double *dens
     return fail (ARCOS_ERR_ARG, "arcos_cdr_advect_vec_dev_noalloc: slab larger than the 16 MiB static "
                                 "scratch (at most 4 padded arrays of (nr+6 rounded to 4) x (nz+4) doubles "
                                 "plus the tile list); use arcos_cdr_advect_vec_dev");
-  double *scr = nullptr;
-  int r = noalloc_setup (&scr);
+  Model M{};
+  M.ns = 1; M.nreact = 0;
+  M.mobile[0] = 1; M.charge[0] = charge; M.mass[0] = mass;
+  M.diffusion_coeff = diffusion_coeff;
+  M.z_cutoff = 1e7;
+  M.bnd_sign[1] = M.bnd_sign[2] = M.bnd_sign[3] = 1;
+  M.per_plane = 1;
+  StageArgs A{};
+  A.nset = 0; A.dset = 0; A.accumulate = 1;
+  A.exact = 1;                                       // the Fortran kernel's arithmetic exactly
+  A.stage_eabs = 0;
+  A.maps = nullptr;                                  // cp.async staging
+  NoallocDev *d = nullptr;
+  int r = noalloc_setup (M, A, &d);
   if (r) return r;
+  double *scr = d->ptr;
   cudaStream_t st = (cudaStream_t) stream;
   // header: [PatchDesc @0 | etz flags @256 B | tiles @512 B], arrays after NOALLOC_HEADER doubles
   char *head = (char *) scr;
@@ -2768,42 +2714,20 @@ arcos_cdr_advect_vec_dev_noalloc (double mass, double charge, const double *dens
   P.dr = dr; P.dz = dz;                              // the slab's own spacing (cdr.c:947)
   P.base = scr + NOALLOC_HEADER;
   P.fam = 0;
-  static WorkItem items[(sizeof (double) * NOALLOC_HEADER - 512) / sizeof (WorkItem)];
-  int ni = 0;
-  for (int zb = 0; zb < nz; zb += ty)
-    for (int c0 = 0; c0 < nr; c0 += TX) items[ni++] = WorkItem{0, 0, c0, std::min (TX, nr - c0), zb, std::min (ty, nz - zb)};
-  CK (cudaMemcpyAsync (head, &P, sizeof (P), cudaMemcpyHostToDevice, st));
-  CK (cudaMemsetAsync (head + 256, 0, 2 * sizeof (int), st));
-  CK (cudaMemcpyAsync (head + 512, items, sizeof (WorkItem) * ni, cudaMemcpyHostToDevice, st));
+  const int ni = (int) n_items;
+  k_noalloc_header<<<(ni + 255) / 256, 256, 0, st>>> (P, TX, ty, ni, head);
+  cudaError_t e = cudaGetLastError ();
+  if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("header launch: ") + cudaGetErrorString (e));
   const size_t w = sizeof (double) * (nr + 4), hgt = (size_t) (nz + 4), dp = sizeof (double) * pitch;
   CK (cudaMemcpy2DAsync (P.arr (0, K_DENS, 0), dp, dens, w, w, hgt, cudaMemcpyDeviceToDevice, st));
   CK (cudaMemcpy2DAsync (P.arr (0, K_DDENS, 0), dp, d_dens, w, w, hgt, cudaMemcpyDeviceToDevice, st));
   CK (cudaMemcpy2DAsync (P.arr (0, K_ER), dp, er, w, w, hgt, cudaMemcpyDeviceToDevice, st));
   CK (cudaMemcpy2DAsync (P.arr (0, K_EZ), dp, ez, w, w, hgt, cudaMemcpyDeviceToDevice, st));
-  Model M{};
-  M.ns = 1; M.nreact = 0;
-  M.mobile[0] = 1; M.charge[0] = charge; M.mass[0] = mass;
-  M.diffusion_coeff = diffusion_coeff;
-  M.z_cutoff = 1e7;
-  M.bnd_sign[1] = M.bnd_sign[2] = M.bnd_sign[3] = 1;
-  M.per_plane = 1;
-  StageArgs A{};
   A.patches = (const PatchDesc *) head;
   A.items = (const WorkItem *) (head + 512);
   A.n_items = ni;
-  A.nset = 0; A.dset = 0; A.accumulate = 1;
   A.etz = (const int *) (head + 256);
-  A.exact = 1;                                       // the Fortran kernel's arithmetic exactly
-  A.stage_eabs = 0;
-  A.maps = nullptr;                                  // cp.async staging
-  int occ = 0;
-  cudaError_t e = launch_stage (M_DERIV, 1, 0, M, A, 0, 0, &occ);
-  if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("occupancy: ") + cudaGetErrorString (e));
-  int dev = 0, sms = 148;
-  cudaGetDevice (&dev);
-  cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int blocks = std::min (ni, std::max (1, occ) * sms);
-  e = launch_stage (M_DERIV, 1, 0, M, A, blocks, st);
+  e = launch_stage (M_DERIV, 1, 0, M, A, std::min (ni, d->blocks), st);
   if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("stage launch: ") + cudaGetErrorString (e));
   CK (cudaMemcpy2DAsync (d_dens, w, P.arr (0, K_DDENS, 0), dp, w, hgt, cudaMemcpyDeviceToDevice, st));
   return ARCOS_OK;

@@ -142,7 +142,7 @@ face_z_fast (double nLL, double nL, double nR, double nRR, double v, double dd)
 // the table position the reference derives from log10/floor is recovered by
 // comparing |E| with exact per-node thresholds (precomputed on the host with
 // the same log10), starting from a single-precision estimate.
-__device__ __noinline__ int
+static __device__ __noinline__ int
 table_pos_slow (const TableNode *__restrict__ nd, int steps, double eabs, int k)
 {
   while (k > 0 && eabs < nd[k].thr) k--;

@@ -42,7 +42,11 @@ class ReactTable:
 
 def react_table_read(path: str | os.PathLike) -> ReactTable:
     """Parse a table file with the semantics of react_table.c:73-111
-    (``atof``/``atoi`` on successive lines after ``START``)."""
+    (``atof``/``atoi`` on successive lines after ``START``).  Where the
+    reference exits (missing file: FileNotFoundError here) or reads garbage
+    (no START line: it loops forever; a truncated file: it repeats the last
+    line; fewer than 2 points or e_step <= 0: a table the lookup cannot use)
+    this reader raises."""
     with open(path, "r") as fp:
         lines = fp.read().splitlines()
     i = 0
@@ -65,11 +69,17 @@ def react_table_read(path: str | os.PathLike) -> ReactTable:
             return 0.0
 
     vals = lines[i + 1:]
+    if len(vals) < 5:
+        raise ValueError(f"{path}: the header after START needs 5 lines, found {len(vals)}")
     e_min = atof(vals[0])
     e_step = atof(vals[1])
     steps = int(atof(vals[2])) - 1
     underflow = atof(vals[3])
     overflow = atof(vals[4])
+    if steps < 1:
+        raise ValueError(f"{path}: a table needs at least 2 points, found {steps + 1}")
+    if not (e_step > 0):
+        raise ValueError(f"{path}: e_step must be positive, found {e_step}")
     values = np.array([atof(v) for v in vals[5:5 + steps + 1]], dtype=np.float64)
     if values.size != steps + 1:
         raise ValueError(f"{path}: expected {steps + 1} values, found {values.size}")

@@ -72,10 +72,53 @@ def uniform_field(spec: GridSpec):
     return (spec.zeros(), spec.zeros(), None)
 
 
+def wavy_field(spec: GridSpec, params: Params, seed: int = 0, e_lo: float = 0.02,
+               e_hi: float = 30.0, wavelength: Tuple[float, float] = (14.0, 40.0),
+               cancel_applied: bool = True):
+    """A smooth, non-uniform fixed field: the field solve's part (er, ez,
+    None) in rz layout on the staggered points (er at r faces (ir + 1) dr and
+    cell-centre z, ez at cell-centre r and z faces (iz + 1) dz; grid.h:40,43).
+
+    Each component is a product of sines with seeded phases and wavelengths
+    drawn from ``wavelength`` (in cells of the grid's level), so both
+    components change sign inside 32-column and 16-row tiles, and an envelope
+    that grows log-uniformly from ``e_lo`` at z = 0 to ``e_hi`` at z = L_z, so
+    |E| sweeps a whole reaction table: underflow near z = 0, overflow near
+    z = L_z.  With ``cancel_applied`` the applied E0 is subtracted, so the
+    total field (after cdr_add_ext_field adds E0 back) is the wave itself.
+    In 3-D each plane is scaled by 1 + 0.3 cos(theta)."""
+    rng = np.random.default_rng(seed)
+    dr, dz = params.dr(spec.level), params.dz(spec.level)
+    ir = np.arange(spec.r0 - 2, spec.r1 + 2, dtype=np.float64)
+    iz = np.arange(spec.z0 - 2, spec.z1 + 2, dtype=np.float64)
+    lo, hi = wavelength
+    k = [2 * math.pi / (float(rng.uniform(lo, hi))) for _ in range(6)]
+    ph = [float(rng.uniform(0, 2 * math.pi)) for _ in range(6)]
+
+    def env(zc):
+        return e_lo * (e_hi / e_lo) ** np.clip(zc / params.L_z, 0.0, 1.0)
+
+    # er: r faces, z centres; ez: r centres, z faces (positions in cells of this level)
+    rf, zc = np.meshgrid(ir + 1.0, iz + 0.5)
+    rc, zf = np.meshgrid(ir + 0.5, iz + 1.0)
+    wr = np.sin(k[0] * rf + ph[0]) * np.cos(k[1] * zc + ph[1]) + 0.4 * np.sin(k[2] * rf + ph[2])
+    wz = np.cos(k[3] * rc + ph[3]) * np.sin(k[4] * zf + ph[4]) + 0.4 * np.cos(k[5] * zf + ph[5])
+    er2 = env(zc * dz) * wr
+    ez2 = env(zf * dz) * wz
+    er, ez = spec.zeros(), spec.zeros()
+    for p in range(spec.planes):
+        th = (p + spec.theta0) * params.dtheta
+        mod = 1.0 + 0.3 * math.cos(th) if spec.ntheta > 1 else 1.0
+        er[p] = er2 * mod - (params.E0_x if cancel_applied else 0.0)
+        ez[p] = ez2 * mod - (params.E0_z if cancel_applied else 0.0)
+    return (er, ez, None)
+
+
 def plain(nr: int = 128, nz: int = 256, ntheta: int = 1, L_r: float = 2.0, L_z: float = 4.0,
           ion_mass: float = 1.0, seed: int = 0, noise: float = 0.0, table_points: int = 256,
-          nu: float = 0.5, attempt_dt: float = 50.0) -> Problem:
-    """Single uniform grid with the minimal model and a uniform Ez = -1."""
+          nu: float = 0.5, attempt_dt: float = 50.0, field: str = "uniform") -> Problem:
+    """Single uniform grid with the minimal model and a uniform Ez = -1
+    (``field="uniform"``), or the non-uniform ``wavy_field`` (``"wavy"``)."""
     params = Params(L_r=L_r, L_z=L_z, gridpoints_r=nr, gridpoints_z=nz, max_ntheta=ntheta,
                     E0_z=-1.0, nu_a=nu, nu_d=nu, nu_rt=nu, diffusion_coeff=0.1,
                     warn_min_timestep=1e-12, max_levels=4)
@@ -84,7 +127,13 @@ def plain(nr: int = 128, nz: int = 256, ntheta: int = 1, L_r: float = 2.0, L_z: 
     rng = np.random.default_rng(seed)
     dens = [[seed_dens(spec, params, rng, noise=noise, theta_mod=ntheta > 1)
              for _ in range(model.no_species)]]
-    return Problem(params, model, [spec], dens, [uniform_field(spec)])
+    if field == "wavy":
+        fields = [wavy_field(spec, params, seed=seed + 1000)]
+    elif field == "uniform":
+        fields = [uniform_field(spec)]
+    else:
+        raise ValueError(f"unknown field {field!r}")
+    return Problem(params, model, [spec], dens, fields)
 
 
 def amr(n_patches: int = 320, levels: int = 4, root_nr: int = 512, root_nz: int = 1024,
@@ -212,9 +261,12 @@ def kinetic_model(points: int = 1000, seed: int = 0) -> KineticModel:
 
 def kinetic_batch(n_inst: int = 32, seed: int = 0, points: int = 1000,
                   sizes_r: Sequence[int] = (64, 128, 256),
-                  sizes_z: Sequence[int] = (128, 256, 512)) -> Problem:
+                  sizes_z: Sequence[int] = (128, 256, 512), field: str = "uniform") -> Problem:
     """A batch of independent single-grid instances of uneven sizes, each its
-    own family with its own applied field Ez ~ U[-2, -0.5]."""
+    own family with its own applied field Ez ~ U[-2, -0.5].  With
+    ``field="wavy"`` each instance also gets a ``wavy_field`` (added to its
+    applied field) whose |E| sweeps [0.005, 80], beyond both ends of the
+    rate tables."""
     rng = np.random.default_rng(seed)
     model = kinetic_model(points=points, seed=seed + 1)
     params = Params(L_r=2.0, L_z=4.0, gridpoints_r=128, gridpoints_z=256, E0_z=-1.0,
@@ -233,6 +285,12 @@ def kinetic_batch(n_inst: int = 32, seed: int = 0, points: int = 1000,
             per.append(seed_dens(sp, params, rng, amp=amp, noise=1e-6,
                                  center_z=0.9 * nz * params.dz(0)))
         dens.append(per)
-        fields.append(uniform_field(sp))
+        if field == "wavy":
+            fields.append(wavy_field(sp, params, seed=seed * 1000 + i, e_lo=0.005, e_hi=80.0,
+                                     cancel_applied=False))
+        elif field == "uniform":
+            fields.append(uniform_field(sp))
+        else:
+            raise ValueError(f"unknown field {field!r}")
         famE.append((0.0, 0.0, float(rng.uniform(-2.0, -0.5))))
     return Problem(params, model, specs, dens, fields, famE)

@@ -4,8 +4,8 @@
  * int status (ARCOS_OK = 0); arcos_last_error() holds a message for the last
  * failure of the calling thread.  The reference reports failures with fatal()
  * -> exit(-1) and assert (include/cstream.h:47-51); this library returns
- * instead, and the legacy adapter of INTEGRATION.md turns a non-zero status
- * back into fatal().
+ * instead; a legacy adapter that keeps the reference's void entry points
+ * turns a non-zero status back into fatal().
  *
  * Host arrays use the reference rz_array layout (include/rz_array.h:11-22,
  * src/rz_array.c:23-96): r fastest, two ghost cells on each side, row stride
@@ -290,12 +290,15 @@ int arcos_cdr_advect_vec_dev (double mass, double charge, const double *dens,
  * caching allocator already holds the GPU's memory, or code that must not
  * take cudaMalloc's implicit device synchronisation): all device memory is
  * one static 16 MiB array inside the library (the slab's four padded arrays,
- * (nr+6 rounded up to 4) x (nz+4) doubles each, plus the tile list), whose
- * address is looked up on the first call for each device, with that device
- * current.  Larger slabs return ARCOS_ERR_ARG.  Asynchronous on `stream`;
- * the scratch is shared, so calls that overlap (two streams, two threads, or
- * two devices' calls racing on the per-device lookup) race; make the first
- * call on a device before any stream capture, since it does the lookup. */
+ * (nr+6 rounded up to 4) x (nz+4) doubles each, plus the tile list).  The
+ * first call on each device, with that device current, looks up the array's
+ * address and the stencil kernel's occupancy; make that first call before
+ * any stream capture begins.  Every call writes its descriptor and tile list
+ * into the array with a small kernel, so no host buffer outlives the call.
+ * Larger slabs return ARCOS_ERR_ARG.  Asynchronous on `stream`; the scratch
+ * is shared and keeps the last call's contents, so calls that overlap on the
+ * GPU (two streams, two threads) race, and so do first calls made from two
+ * threads at once (the per-device lookup table is not locked). */
 int arcos_cdr_advect_vec_dev_noalloc (double mass, double charge, const double *dens,
                                       double *d_dens, const double *er, const double *ez,
                                       double diffusion_coeff, double dr, double dz,

@@ -67,7 +67,6 @@ PortGrid._fields_ = [("r0", C.c_int), ("z0", C.c_int), ("r1", C.c_int), ("z1", C
                      ("fixed_er", DP), ("fixed_ez", DP), ("fixed_et", DP), ("owns", C.c_int)]
 
 _port = None
-_ref = None
 
 
 def port_lib():
@@ -89,14 +88,36 @@ def port_lib():
     return _port
 
 
-def ref_available(omp: bool = False) -> bool:
-    return os.path.exists(REF_OMP_SO if omp else REF_SO)
+# Builds of the reference (oracle/Makefile), by variant:
+#   "plain"   the reference C + the restated Fortran kernel (the oracle itself)
+#   "omp"     the same with OpenMP (timing on all host cores)
+#   "bigtab"  "plain" with react_table's MAX_TABLE_SIZE raised to 1024
+#   "dropin"  the reference C without its Fortran wrapper, linked against the
+#             device library: cdr.c:945 calls the device's arcos_cdr_advect_vec
+#   "adapter" "dropin" plus the cdr_grid_t adapter, whose cdr_rk2 replaces the
+#             reference's (renamed cdr_rk2_host) and runs the step on the device
+REF_VARIANTS = {"plain": REF_SO, "omp": REF_OMP_SO,
+                "bigtab": os.path.join(HERE, "_ref", "libarcos_ref_bigtab.so"),
+                "dropin": os.path.join(HERE, "_ref", "libarcos_ref_dropin.so"),
+                "adapter": os.path.join(HERE, "_ref", "libarcos_ref_adapter.so")}
+_refs = {}
 
 
-def ref_lib(omp: bool = False):
-    global _ref
-    path = REF_OMP_SO if omp else REF_SO
-    if _ref is None or getattr(_ref, "_path", None) != path:
+def _variant(omp) -> str:
+    if isinstance(omp, str):
+        return omp
+    return "omp" if omp else "plain"
+
+
+def ref_available(omp=False) -> bool:
+    return os.path.exists(REF_VARIANTS[_variant(omp)])
+
+
+def ref_lib(omp=False):
+    """The reference build ``omp`` (a variant name, or a bool for omp/plain).
+    Each build keeps its own process globals (loaded RTLD_LOCAL)."""
+    path = REF_VARIANTS[_variant(omp)]
+    if path not in _refs:
         if not os.path.exists(path):
             raise RuntimeError(f"reference oracle library missing: {path}")
         lib = C.CDLL(path, mode=C.RTLD_LOCAL)
@@ -118,8 +139,8 @@ def ref_lib(omp: bool = False):
         lib.ref_set_refine_params.argtypes = [C.c_double, C.c_int, C.c_double, C.c_double,
                                               C.c_double, C.c_int, C.c_int, C.c_int]
         lib.ref_cdr_refine.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int]
-        _ref = lib
-    return _ref
+        _refs[path] = lib
+    return _refs[path]
 
 
 FIELD_ZERO, FIELD_FIXED, FIELD_POISSON = 0, 1, 2
@@ -253,7 +274,7 @@ class RefTree(_TreeBase):
     state in process globals, so only one RefTree is live at a time."""
 
     def __init__(self, params: Params, model: KineticModel, specs: Sequence[GridSpec],
-                 field_mode: int = FIELD_ZERO, omp: bool = False):
+                 field_mode: int = FIELD_ZERO, omp=False):
         super().__init__(params, model, specs)
         lib = ref_lib(omp)
         self.lib = lib
@@ -277,8 +298,9 @@ class RefTree(_TreeBase):
             for i, x in enumerate(re.outputs):
                 outs[r * MAXOUT + i] = x
             path = os.path.join(self._tmp.name, f"r{r}.reaction")
-            if re.table.points > 500:
-                raise ValueError("the reference stores at most 500 table points (react_table.h:5)")
+            if re.table.points > 500 and _variant(omp) != "bigtab":
+                raise ValueError("the reference stores at most 500 table points (react_table.h:5); "
+                                 "use the 'bigtab' build")
             write_react_table(path, re.table, "table written for the reference oracle")
             names += path.encode() + b"\0"
         lib.ref_set_reactions(nr, nin, ins, nout, outs, C.c_char_p(names + b"\0"))

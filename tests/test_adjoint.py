@@ -25,8 +25,8 @@ EPS = 1e-6
 TOL = 1e-6
 
 
-def problem(nr, nz, seed=0, ion_mass=0.0):
-    pb = workloads.plain(nr=nr, nz=nz, ion_mass=ion_mass, noise=1e-3, seed=seed)
+def problem(nr, nz, seed=0, ion_mass=0.0, field="uniform"):
+    pb = workloads.plain(nr=nr, nz=nz, ion_mass=ion_mass, noise=1e-3, seed=seed, field=field)
     return pb
 
 
@@ -96,15 +96,14 @@ def objective(ne, target, vol):
     return 0.5 * float(np.sum((ne - target) ** 2 * vol))
 
 
-def device_setup(nr, nz, K, ck, seed=0):
-    pb = problem(nr, nz, seed=seed)
+def device_setup(nr, nz, K, ck, seed=0, field="uniform"):
+    pb = problem(nr, nz, seed=seed, field=field)
     tree = CdrTree(pb.params, pb.model, pb.specs)
     tree.set_fixed_field(pb.fields)
     adj = Adjoint(tree)
     base = Params(pb)
     apply_device(tree, pb, base)
     # target: forward run from a perturbed seed (amplitude x1.1, radius x0.9)
-    tgt = problem(nr, nz, seed=seed)
     spec = pb.specs[0]
     rng = np.random.default_rng(seed + 100)
     tgt_e = workloads.seed_dens(spec, pb.params, rng, amp=0.11, sigma=0.09, noise=1e-3)
@@ -140,10 +139,13 @@ def device_J(tree, adj, pb, q, hs, K, ck, target, vol):
     return objective(device_ne(tree, adj, pb, q, hs, K, ck), target, vol)
 
 
+@pytest.mark.parametrize("field", ["uniform", "wavy"])
 @pytest.mark.parametrize("which", [("dens",), ("mu",), ("D",), ("table",), ("dens", "mu", "D", "table")])
-def test_adjoint_matches_device_fd(cuda_device, which):
+def test_adjoint_matches_device_fd(cuda_device, which, field):
+    """Uniform applied field, and the non-uniform wavy field (radial drift,
+    sign changes of the velocity inside a warp, |E| over the whole table)."""
     K, ck = 16, 4
-    pb, tree, adj, base, hs, target, vol = device_setup(32, 64, K, ck, seed=1)
+    pb, tree, adj, base, hs, target, vol = device_setup(32, 64, K, ck, seed=1, field=field)
     grads, J0 = device_grads(tree, adj, target, vol)
     assert J0 > 0
     rng = np.random.default_rng(7)
@@ -161,10 +163,11 @@ def test_adjoint_matches_device_fd(cuda_device, which):
         assert abs(fd - pr) <= TOL * max(abs(fd), 1e-300), (which, fd, pr)
 
 
-def test_adjoint_matches_oracle_fd(cuda_device):
+@pytest.mark.parametrize("field", ["uniform", "wavy"])
+def test_adjoint_matches_oracle_fd(cuda_device, field):
     """FD of the CPU oracle's frozen-step forward against the device adjoint."""
     K, ck, nr, nz = 8, 4, 24, 48
-    pb, tree, adj, base, hs, target, vol = device_setup(nr, nz, K, ck, seed=2)
+    pb, tree, adj, base, hs, target, vol = device_setup(nr, nz, K, ck, seed=2, field=field)
     grads, _ = device_grads(tree, adj, target, vol)
 
     def oracle_ne(q):
@@ -209,13 +212,15 @@ def test_frozen_forward_reproduces_cfl_run(cuda_device):
         assert np.array_equal(tree.download(0, "dens", s)[0, 2:-2, 2:-2], a[s][0, 2:-2, 2:-2])
 
 
-def test_kinetic_batch_adjoint_matches_fd(cuda_device):
+@pytest.mark.parametrize("field", ["uniform", "wavy"])
+def test_kinetic_batch_adjoint_matches_fd(cuda_device, field):
     """Three families of different sizes, six species (ions mobile), nine
     reactions with one- and two-input terms: the adjoint of the total electron
     number at T with respect to the initial densities of every species and
     every table value, against central differences of the frozen-step
     forward.  Two checkpoint segments."""
-    pb = workloads.kinetic_batch(n_inst=3, points=200, sizes_r=(24, 40), sizes_z=(32, 48), seed=1)
+    pb = workloads.kinetic_batch(n_inst=3, points=200, sizes_r=(24, 40), sizes_z=(32, 48), seed=1,
+                                 field=field)
     ns = pb.model.no_species
     tree = CdrTree(pb.params, pb.model, pb.specs)
     for f, E in enumerate(pb.family_E):

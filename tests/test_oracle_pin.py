@@ -21,12 +21,12 @@ from parity_util import max_ulp, port_tree, single_family
 needs_ref = pytest.mark.skipif(not bind.ref_available(), reason="reference build absent")
 
 
-def ref_tree(pb, field_mode=bind.FIELD_FIXED, E=None):
+def ref_tree(pb, field_mode=bind.FIELD_FIXED, E=None, variant="plain"):
     import copy
     params = copy.deepcopy(pb.params)
     if E is not None:
         params.E0_x, params.E0_y, params.E0_z = E
-    t = bind.RefTree(params, pb.model, pb.specs, field_mode=field_mode)
+    t = bind.RefTree(params, pb.model, pb.specs, field_mode=field_mode, omp=variant)
     for g, per in enumerate(pb.dens):
         for s, a in enumerate(per):
             t.dens(g, s)[...] = a
@@ -129,6 +129,67 @@ def test_kinetic_model():
         for _ in range(3):
             assert port.rk2(50.0)[0] == ref.rk2(50.0)
         assert_same(port, ref, sub, ("dens", "d_dens"))
+
+
+@needs_ref
+@pytest.mark.parametrize("ion_mass", [0.0, 1.0])
+def test_plain_2d_wavy_field(ion_mass):
+    """Non-uniform field (both components change sign, |E| from table
+    underflow to overflow): radial drift and the lookup at every node."""
+    pb = workloads.plain(nr=40, nz=72, ion_mass=ion_mass, noise=1e-3, seed=13, field="wavy")
+    port, ref = port_tree(pb), ref_tree(pb)
+    for _ in range(5):
+        hp, st = port.rk2(50.0)
+        assert st == 0 and hp == ref.rk2(50.0)
+    assert_same(port, ref, pb, ("dens", "d_dens"))
+
+
+@needs_ref
+def test_theta_ref_exact_wavy_field():
+    pb = workloads.plain(nr=20, nz=36, ntheta=4, ion_mass=1.0, noise=1e-6, seed=3, field="wavy")
+    pb.params.per_plane = False
+    port, ref = port_tree(pb, per_plane=False), ref_tree(pb)
+    for _ in range(3):
+        assert port.rk2(50.0)[0] == ref.rk2(50.0)
+    assert_same(port, ref, pb, ("dens", "d_dens"))
+
+
+@needs_ref
+def test_kinetic_model_wavy_field():
+    pb = workloads.kinetic_batch(n_inst=2, points=300, sizes_r=(24,), sizes_z=(40,), seed=8,
+                                 field="wavy")
+    for i in range(2):
+        sub = single_family(pb, i)
+        port = port_tree(sub, E=pb.family_E[i])
+        ref = ref_tree(sub, E=pb.family_E[i])
+        for _ in range(3):
+            assert port.rk2(50.0)[0] == ref.rk2(50.0)
+        assert_same(port, ref, sub, ("dens", "d_dens"))
+
+
+@pytest.mark.skipif(not bind.ref_available("bigtab"), reason="reference build absent")
+@pytest.mark.parametrize("field", ["uniform", "wavy"])
+def test_kinetic_model_1000_point_tables(field):
+    """The kinetic batch's 1000-point tables, against the reference built
+    with a 1024-entry MAX_TABLE_SIZE (oracle/react_table_1024.h): 9
+    reactions, 6 species, |E| over the whole table (and beyond it)."""
+    pb = workloads.kinetic_batch(n_inst=2, points=1000, sizes_r=(24,), sizes_z=(40,), seed=8,
+                                 field=field)
+    for i in range(2):
+        sub = single_family(pb, i)
+        port = port_tree(sub, E=pb.family_E[i])
+        ref = ref_tree(sub, E=pb.family_E[i], variant="bigtab")
+        for _ in range(3):
+            assert port.rk2(50.0)[0] == ref.rk2(50.0)
+        assert_same(port, ref, sub, ("dens", "d_dens"))
+
+
+def test_plain_reference_refuses_tables_above_500_points():
+    pb = workloads.kinetic_batch(n_inst=1, points=1000, sizes_r=(24,), sizes_z=(40,), seed=8)
+    if not bind.ref_available("plain"):
+        pytest.skip("reference build absent")
+    with pytest.raises(ValueError, match="500"):
+        ref_tree(single_family(pb, 0), E=pb.family_E[0])
 
 
 @needs_ref

@@ -1,13 +1,16 @@
 """The allocation-free narrow seam (arcos_cdr_advect_vec_dev_noalloc) against
 the allocating one (arcos_cdr_advect_vec_dev), two calls in a row with
-different slabs and parameters; results must be bit-identical.  Collected
-last so it also runs after every other test has used the library."""
+different slabs and parameters, and against the CPU oracle's restatement of
+the Fortran kernel (port_advect_vec); results must be bit-identical.
+Collected last so it also runs after every other test has used the
+library."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
 from arcos_b200._lib import ARCOS_OK, lib
+from oracle import bind
 
 pytestmark = pytest.mark.gpu
 
@@ -52,6 +55,12 @@ def test_noalloc_matches_allocating_seam(cuda_device):
         a, b = out_a.cpu().numpy(), out_b.cpu().numpy()
         assert not np.array_equal(a, d0)
         assert np.array_equal(a, b)
+        # the oracle on the same slab (arcos_f90/src/cdr_advect_diffu_vec.f90:45-132)
+        d_port = d0.copy()
+        P = bind._dp
+        bind.port_lib().port_advect_vec(mass, charge, P(dens), P(d_port), P(er), P(ez), D, h, h,
+                                        r0, r1, z0, z1)
+        assert np.array_equal(b, d_port)
 
 
 def test_noalloc_rejects_oversize_slab(cuda_device):
