@@ -73,6 +73,8 @@ def lib():
     L.arcos_download.argtypes = [VP, C.c_int, C.c_int, C.c_int, C.c_int, DP]
     L.arcos_set_field.argtypes = [VP, C.c_int, C.c_int, DP, DP, DP]
     L.arcos_set_field_fn.argtypes = [VP, FIELD_FN, VP]
+    L.arcos_set_field_poisson.argtypes = [VP, C.c_int]
+    L.arcos_solve_field.argtypes = [VP, C.c_int]
     for name in ("arcos_cdr_nonegative_r", "arcos_cdr_set_ext_bnd_r", "arcos_cdr_set_periodic_r",
                  "arcos_cdr_restrict_r", "arcos_cdr_set_bnd_r", "arcos_cdr_match_r",
                  "arcos_prepare_grid", "arcos_cdr_add_ext_field_r", "arcos_cdr_calc_eabs_r",

@@ -1,8 +1,10 @@
 """Tile-shape autotuner for the stencil kernel.
 
-The stage kernel works on tiles of 32 columns by WY*RPW rows; which shape is
-fastest depends on the grid sizes (tile count against SM count, halo share)
-and on the number of species.  The tuner times a few device-timed steps with
+Shapes 0-2 are the tiled fused kernel (tiles of 32 columns by WY*RPW rows,
+one block per tile); shapes 3-5 the marching kernel (one warp per 31-column
+strip and segment of 16, 32 or 64 rows).  Which is fastest depends on the
+grid sizes (work units against SM count, halo share) and on the number of
+species.  The tuner times a few device-timed steps with
 each shape on the caller's own problem and keeps the fastest.  Timing runs
 advance the simulation (the state moves on by the tuning steps).
 """
@@ -12,9 +14,12 @@ from typing import Dict, Optional
 
 from ._lib import check
 
-N_TILE_SHAPES = 3
-TILE_SHAPES = {0: "32 x 16 cells, 128 threads", 1: "32 x 32 cells, 256 threads",
-               2: "32 x 16 cells, 256 threads"}
+N_TILE_SHAPES = 6
+TILE_SHAPES = {0: "tiles of 32 x 16 cells, 128 threads", 1: "tiles of 32 x 32 cells, 256 threads",
+               2: "tiles of 32 x 16 cells, 256 threads",
+               3: "marching warps, 31-column strips, segments of 16 rows",
+               4: "marching warps, 31-column strips, segments of 32 rows",
+               5: "marching warps, 31-column strips, segments of 64 rows"}
 
 
 def autotune_tiles(tree, steps: int = 6, h: float = 50.0, stream=None) -> Dict[int, float]:

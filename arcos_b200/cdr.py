@@ -15,7 +15,8 @@ cdr_restrict_r     :2050-2097  cdr_restrict_r(set)
 cdr_set_bnd_r      :1888-1948  cdr_set_bnd_r(set)
 cdr_match_r        :1763-1882  cdr_match_r(set)
 prepare_grid       :1334-1351  prepare_grid(set)
-cdr_calc_field_r   :532-580    set_field(...) / field_post(set) / field callback
+cdr_calc_field_r   :532-580    set_field(...) / field_post(set) / field callback /
+                               set_field_poisson (the solve on the device)
 cdr_calc_charge_r  :361-389    cdr_calc_charge_r(set)
 react_apply_all    reaction.c:192-211   react_apply_all(set)
 cdr_advect_diffu_r :900-955    cdr_advect_diffu_r(set)
@@ -169,6 +170,15 @@ class CdrTree:
 
         self._field_cb = FIELD_FN(cb)
         check(self.L.arcos_set_field_fn(self.h, self._field_cb, None))
+
+    def set_field_poisson(self, on: bool = True):
+        """Solve the field of every stage on the device (pois_solve_a,
+        poisson.c:763, one 2-D grid): no host round trip per stage."""
+        check(self.L.arcos_set_field_poisson(self.h, 1 if on else 0))
+
+    def solve_field(self, set: int = SET_GRID):
+        """One device field solve of ``set`` from its current charge."""
+        check(self.L.arcos_solve_field(self.h, set))
 
     # ---- reference entry points ----
     def _call(self, name: str, set: int):

@@ -17,7 +17,9 @@
 #include "adjoint_kernel.cuh"
 #include "aux_kernels.cuh"
 #include "refine_kernel.cuh"
+#include "poisson_kernel.cuh"
 #include "launch.cuh"
+#include "march_kernel.cuh"
 
 using namespace arcos;
 
@@ -80,7 +82,12 @@ struct Ctx {
   WorkItem *items_d = nullptr;
   int n_items = 0;
   std::vector<int> item_off, item_cnt;
-  int tile_cfg = 2;                   // index into TILE_WY / TILE_RPW (2: the fastest measured shape)
+  int tile_cfg = 2;                   // 0..2: TILE_WY / TILE_RPW shapes of k_stage / k_fused;
+                                      // 3..5: k_march with segments of MARCH_H[cfg - 3] rows
+                                      // (k_stage then uses shape 2)
+  MarchUnit *units_d = nullptr;       // k_march work units
+  int n_units = 0;
+  CUtensorMap *rmaps_d = nullptr;     // k_march: one-row boxes [patch][set][array]
   int occ[2][2][4][N_TILE_CFG_MAX] = {};
   int stage_eabs = 0;                 // some set holds a non-zero E_theta
   int exact = 0;                      // 1: bit-exact flux limiter, 0: division-free form
@@ -110,6 +117,10 @@ struct Ctx {
   double *ext_d = nullptr;            // [ext_r (nfam*MAXPLANES) | ext_t | ext_z (nfam)]
   std::vector<double> famE;           // 3 per family
   arcos_field_fn fn = nullptr;
+  bool pois = false;                  // field of each stage from the device Poisson solve
+  double *pois_d = nullptr;           // its coefficients and scratch
+  PoisArgs pois_args{};
+  cudaGraphExec_t graph_inloop = nullptr;   // one step with the device field solve
   void *user = nullptr;
   bool field_set[2] = {false, false};
   bool per_patch = false;             // launch every kernel once per patch
@@ -139,6 +150,37 @@ struct Ctx {
   cudaGraphExec_t adj_graph = nullptr;   // the whole reverse sweep
   int occ_fused[2][2][N_TILE_CFG_MAX] = {};   // [stage_eabs][stage 2][tile]
 };
+
+// The field is solved between the stages (host callback or device Poisson).
+inline bool
+inloop (const Ctx *c)
+{
+  return c->fn != nullptr || c->pois;
+}
+
+// Every captured graph depends on the launch configuration: drop them when
+// it changes.
+void
+drop_graphs (Ctx *c)
+{
+  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
+  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
+  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
+  if (c->graph_inloop) { cudaGraphExecDestroy (c->graph_inloop); c->graph_inloop = nullptr; }
+}
+
+// Tile shape of k_stage / k_fused (the march shapes keep k_stage at shape 2).
+inline int
+stage_cfg (const Ctx *c)
+{
+  return c->tile_cfg < N_TILE_CFG ? c->tile_cfg : 2;
+}
+
+inline bool
+march_on (const Ctx *c)
+{
+  return c->tile_cfg >= N_TILE_CFG && c->units_d && c->rmaps_d;
+}
 
 // ---- reaction-table thresholds ----------------------------------------------
 // The reference's classification of |E| (reaction.c:127-136):
@@ -235,6 +277,20 @@ launch_stage (int mode, int ns, int cfg, const Model &M, const StageArgs &A, int
   }
 }
 
+cudaError_t
+launch_march (int ns, bool s2, bool tree, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s)
+{
+  switch (ns) {
+  case 1: return launch_march_ns<1> (s2, tree, M, A, blocks, s);
+  case 2: return launch_march_ns<2> (s2, tree, M, A, blocks, s);
+  case 3: return launch_march_ns<3> (s2, tree, M, A, blocks, s);
+  case 4: return launch_march_ns<4> (s2, tree, M, A, blocks, s);
+  case 5: return launch_march_ns<5> (s2, tree, M, A, blocks, s);
+  case 6: return launch_march_ns<6> (s2, tree, M, A, blocks, s);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
 template <bool S2>
 cudaError_t
 launch_fused_m (int ns, int cfg, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
@@ -253,14 +309,14 @@ launch_fused_m (int ns, int cfg, const Model &M, const FusedArgs &A, int blocks,
 int
 stage_blocks (Ctx *c, int mode, int n_items)
 {
-  int &o = c->occ[c->stage_eabs][c->exact][mode][c->tile_cfg];
+  int &o = c->occ[c->stage_eabs][c->exact][mode][stage_cfg (c)];
   if (o == 0) {
     StageArgs A{};
     A.exact = c->exact;
     A.stage_eabs = c->stage_eabs;
     A.n_nodes = (int) c->nodes_h.size ();
     int b = 0;
-    launch_stage (mode, c->M.ns, c->tile_cfg, c->M, A, 0, 0, &b);
+    launch_stage (mode, c->M.ns, stage_cfg (c), c->M, A, 0, 0, &b);
     o = b > 0 ? b : 1;
   }
   const int cap = c->num_sms * o;
@@ -321,8 +377,9 @@ upload_lean_nodes (Ctx *c)
 bool
 lean_ok (Ctx *c)
 {
+  // the lean kernels apply the flux on every theta plane (per_plane)
   return c->fused_ok && c->lean_tables && !c->exact && c->use_tma && c->maps_d && c->colfac_d
-         && c->lean_nodes_d && !c->fn && !c->per_patch;
+         && c->lean_nodes_d && !inloop (c) && !c->per_patch && (c->p.per_plane || c->p.max_ntheta == 1);
 }
 
 FusedArgs
@@ -341,6 +398,10 @@ fused_args (Ctx *c)
   A.stage_eabs = c->stage_eabs;
   A.maps = c->maps_d;
   A.maps_per_patch = c->maps_per_patch;
+  A.units = c->units_d;
+  A.n_units = c->n_units;
+  A.rmaps = c->rmaps_d;
+  A.rmaps_per_patch = c->maps_per_patch;
   A.colfac = c->colfac_d;
   // reaction program: node 0 of reaction r sits after r + 1 sentinels
   const Model &M = c->M;
@@ -379,17 +440,26 @@ run_fused (Ctx *c, bool s2, int fold, int fam_state = 1, int frozen_k = -1)
     A.h_stride = c->adj_nsteps;
     A.h_k = frozen_k;
   }
-  int &o = c->occ_fused[c->stage_eabs][s2 ? 1 : 0][c->tile_cfg];
+  if (march_on (c)) {
+    // one warp per unit; blocks are independent of one another
+    const int blocks = (c->n_units + MARCH_WPB - 1) / MARCH_WPB;
+    if (blocks <= 0) return ARCOS_OK;
+    cudaError_t e = launch_march (c->M.ns, s2, !c->fused_ok, c->M, A, blocks, c->stream);
+    if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("march launch: ") + cudaGetErrorString (e));
+    return ARCOS_OK;
+  }
+  const int cfg = stage_cfg (c);
+  int &o = c->occ_fused[c->stage_eabs][s2 ? 1 : 0][cfg];
   if (o == 0) {
     int b = 0;
-    if (s2) launch_fused_m<true> (c->M.ns, c->tile_cfg, c->M, A, 0, 0, &b);
-    else launch_fused_m<false> (c->M.ns, c->tile_cfg, c->M, A, 0, 0, &b);
+    if (s2) launch_fused_m<true> (c->M.ns, cfg, c->M, A, 0, 0, &b);
+    else launch_fused_m<false> (c->M.ns, cfg, c->M, A, 0, 0, &b);
     o = b > 0 ? b : 1;
   }
   const int blocks = std::min (c->n_items, c->num_sms * o);
   if (blocks <= 0) return ARCOS_OK;
-  cudaError_t e = s2 ? launch_fused_m<true> (c->M.ns, c->tile_cfg, c->M, A, blocks, c->stream, nullptr)
-                     : launch_fused_m<false> (c->M.ns, c->tile_cfg, c->M, A, blocks, c->stream, nullptr);
+  cudaError_t e = s2 ? launch_fused_m<true> (c->M.ns, cfg, c->M, A, blocks, c->stream, nullptr)
+                     : launch_fused_m<false> (c->M.ns, cfg, c->M, A, blocks, c->stream, nullptr);
   if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("fused launch: ") + cudaGetErrorString (e));
   return ARCOS_OK;
 }
@@ -402,7 +472,7 @@ run_stage (Ctx *c, StageArgs A, int mode)
   if (!c->per_patch) {
     const int blocks = stage_blocks (c, mode, A.n_items);
     if (blocks <= 0) return ARCOS_OK;
-    cudaError_t e = launch_stage (mode, c->M.ns, c->tile_cfg, c->M, A, blocks, c->stream);
+    cudaError_t e = launch_stage (mode, c->M.ns, stage_cfg (c), c->M, A, blocks, c->stream);
     if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("stage launch: ") + cudaGetErrorString (e));
     return ARCOS_OK;
   }
@@ -412,7 +482,7 @@ run_stage (Ctx *c, StageArgs A, int mode)
     B.n_items = c->item_cnt[p];
     if (B.n_items == 0) continue;
     const int blocks = stage_blocks (c, mode, B.n_items);
-    cudaError_t e = launch_stage (mode, c->M.ns, c->tile_cfg, c->M, B, blocks, c->stream);
+    cudaError_t e = launch_stage (mode, c->M.ns, stage_cfg (c), c->M, B, blocks, c->stream);
     if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("stage launch: ") + cudaGetErrorString (e));
   }
   return ARCOS_OK;
@@ -571,9 +641,7 @@ refresh_stage_eabs (Ctx *c)
   for (int v : h) any |= v != 0;
   if (any != c->stage_eabs) {
     c->stage_eabs = any;
-    if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
-  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
-  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
+    drop_graphs (c);
   }
   return ARCOS_OK;
 }
@@ -584,21 +652,9 @@ int
 do_field_post (Ctx *c, int set)
 {
   const int np = (int) c->pd_h.size ();
-  // reset the per-set counters and maxima
-  {
-    std::vector<int> h (np * 2);
-    CK (cudaMemcpyAsync (h.data (), c->etz_d, sizeof (int) * np * 2, cudaMemcpyDeviceToHost, c->stream));
-    CK (cudaStreamSynchronize (c->stream));
-    for (int p = 0; p < np; p++) h[p * 2 + set] = 0;
-    CK (cudaMemcpyAsync (c->etz_d, h.data (), sizeof (int) * np * 2, cudaMemcpyHostToDevice, c->stream));
-    std::vector<DevState> st (c->nfam);
-    CK (cudaMemcpyAsync (st.data (), c->st_d, sizeof (DevState) * c->nfam, cudaMemcpyDeviceToHost, c->stream));
-    CK (cudaStreamSynchronize (c->stream));
-    for (auto &s : st)
-      for (int k = 0; k < 3; k++) s.emax_key[set][k] = dkey (-1.0);
-    CK (cudaMemcpyAsync (c->st_d, st.data (), sizeof (DevState) * c->nfam, cudaMemcpyHostToDevice, c->stream));
-    CK (cudaStreamSynchronize (c->stream));
-  }
+  // reset the per-set E_theta counters and field maxima (stream-ordered)
+  k_field_reset<<<(std::max (np, c->nfam) + 127) / 128, 128, 0, c->stream>>> (c->etz_d, np, set, c->st_d, c->nfam);
+  CKL ();
   long long w = 0;
   for (auto &P : c->pd_h) w = std::max (w, P.asz);
   const double *er = c->ext_d, *et = c->ext_d + c->nfam * ARCOS_MAXPLANES,
@@ -612,7 +668,8 @@ do_field_post (Ctx *c, int set)
   });
   if (r) return r;
   if ((r = do_periodic (c, set, 2))) return r;
-  return refresh_stage_eabs (c);
+  // the device field solve writes E_theta = 0 on 2-D grids: nothing to refresh
+  return c->pois ? ARCOS_OK : refresh_stage_eabs (c);
 }
 
 int
@@ -659,10 +716,28 @@ check_state_errors (Ctx *c)
   return ARCOS_OK;
 }
 
+// The device field solve (poisson_kernel.cuh) from the charge of set `set`
+// into its er, ez, etheta, then the rest of cdr_calc_field_r.
+int
+device_poisson (Ctx *c, int set)
+{
+  const PoisArgs &A = c->pois_args;
+  const int n = A.nr * A.nz;
+  const int b = std::min ((n + 255) / 256, 8 * c->num_sms);
+  k_pois_fwd<<<b, 256, 0, c->stream>>> (c->pd_d, 0, set, A);
+  k_pois_tri<<<(A.nz + 127) / 128, 128, 0, c->stream>>> (A);
+  k_pois_inv<<<b, 256, 0, c->stream>>> (A);
+  const long long len = (long long) (A.nz + 4) * c->pd_h[0].pitch;
+  k_pois_field<<<(int) std::min<long long> ((len + 255) / 256, 8 * c->num_sms), 256, 0, c->stream>>> (c->pd_d, 0, set, A);
+  CKL ();
+  return do_field_post (c, set);
+}
+
 // field callback for the root of family 0 (the reference solves the field on the tree root)
 int
 field_from_callback (Ctx *c, int stage, int set)
 {
+  if (c->pois) return device_poisson (c, set);
   const PatchDesc &P = c->pd_h[0];
   const size_t n = (size_t) (P.nr + 4) * (P.nz + 4) * P.planes;
   std::vector<double> ch (n), er (n, 0.0), ez (n, 0.0), et (n, 0.0);
@@ -726,7 +801,7 @@ rk2_general (Ctx *c)
   CKL ();
   if ((r = do_nonneg (c, 0))) return r;                 // cdr.c:1276
   if ((r = do_prepare (c, 0))) return r;                // cdr.c:1279
-  if (c->fn && (r = field_from_callback (c, 0, 0))) return r;   // cdr.c:1283
+  if (inloop (c) && (r = field_from_callback (c, 0, 0))) return r;   // cdr.c:1283
   A.nset = 0; A.dset = 0;
   if ((r = run_stage (c, A, M_DERIV))) return r;        // cdr.c:1288
   if ((r = do_dmax (c, 0, 0))) return r;                // cdr.c:1293
@@ -737,7 +812,7 @@ rk2_general (Ctx *c)
        }))) return r;                                   // cdr.c:1308
   if ((r = do_charge (c, 1))) return r;
   if ((r = do_prepare (c, 1))) return r;                // cdr.c:1311
-  if (c->fn && (r = field_from_callback (c, 1, 1))) return r;   // cdr.c:1313
+  if (inloop (c) && (r = field_from_callback (c, 1, 1))) return r;   // cdr.c:1313
   if ((r = run_stage (c, A, M_AMR2))) return r;         // cdr.c:1314-1317
   if ((r = do_charge (c, 0))) return r;
   if ((r = do_prepare (c, 0))) return r;                // cdr.c:1322
@@ -745,6 +820,79 @@ rk2_general (Ctx *c)
   CKL ();
   return ARCOS_OK;
 }
+
+// One step of single-grid families with the field solved in the loop
+// (cdr.c:1262-1327 with cdr_calc_field_r at both stages): the bit-exact
+// stage kernels, the field of each stage from the host callback or the
+// device solve.
+int
+rk2_inloop_step (Ctx *c)
+{
+  int r;
+  if ((r = field_from_callback (c, 0, 0))) return r;
+  k_run_reset<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->st_d, c->nfam);
+  CKL ();
+  if ((r = do_dmax (c, 0, 0))) return r;
+  k_cfl<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->M, c->st_d, c->nfam, 0);
+  CKL ();
+  StageArgs A = base_args (c);
+  A.src = 0;
+  if ((r = run_stage (c, A, M_S1))) return r;
+  long long w = 0;
+  for (auto &P : c->pd_h) w = std::max (w, P.asz);
+  if ((r = for_patches (c, w, [&] (dim3 g, const int *pl) {
+         k_charge_star<<<g, 256, 0, c->stream>>> (c->M, c->pd_d, pl, 0, c->st_d);
+       }))) return r;
+  if ((r = field_from_callback (c, 1, 1))) return r;
+  A.dst = 1; A.fam_state = 0; A.want_charge = 1;
+  if ((r = run_stage (c, A, M_S2))) return r;
+  // move the state back to set 0 (this path keeps it there)
+  for (auto &P : c->pd_h) {
+    CK (cudaMemcpyAsync (P.arr (0, K_DENS, 0), P.arr (1, K_DENS, 0), sizeof (double) * P.asz * P.ns, cudaMemcpyDeviceToDevice, c->stream));
+    CK (cudaMemcpyAsync (P.arr (0, K_CHARGE), P.arr (1, K_CHARGE), sizeof (double) * P.asz, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  k_step_end<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->st_d, c->nfam);
+  CKL ();
+  return ARCOS_OK;
+}
+
+// The lean form of the tree step (fixed field, division-free limiter): the
+// two stages are k_march over every tile of every patch, ghosts read from
+// memory after prepare_grid.  Stage 1 writes n* = n0 + h F(n0) into set 1
+// (cdr_update); stage 2 writes (n0 + n*)/2 + h/2 F(n*) into set 0, which
+// equals cdr_rk2_update's n0 + h/2 F(n0) + h/2 F(n*) up to rounding except
+// in parent cells covered by a child, where prepare_grid(inter) restricted
+// n*; those cells are restricted again by the next prepare_grid.  For the
+// same reason the closing prepare_grid of cdr_rk2 (cdr.c:1322) is left to
+// the next step's (after cdr_nonegative_r, which gives the same ghosts and
+// covered cells) and done once at the end of a run.  d_dens is not
+// materialised.
+bool
+lean_tree_ok (Ctx *c)
+{
+  return !c->fused_ok && march_on (c) && c->lean_tables && !c->exact && c->use_tma && c->lean_nodes_d
+         && !inloop (c) && !c->per_patch && (c->p.per_plane || c->p.max_ntheta == 1);
+}
+
+int
+rk2_lean_tree (Ctx *c)
+{
+  int r;
+  if ((r = do_nonneg (c, 0))) return r;                 // cdr.c:1276
+  if ((r = do_prepare (c, 0))) return r;                // cdr.c:1279
+  k_reset_dmax<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->st_d, c->nfam, 0);
+  CKL ();
+  if ((r = do_dmax (c, 0, 0))) return r;                // cdr.c:1293
+  k_cfl<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->M, c->st_d, c->nfam, 0);
+  CKL ();
+  if ((r = run_fused (c, false, 0, 0))) return r;       // cdr.c:1308 (n* into set 1)
+  if ((r = do_prepare (c, 1))) return r;                // cdr.c:1311
+  if ((r = run_fused (c, true, 0, 0))) return r;        // cdr.c:1314-1317
+  k_step_end<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->st_d, c->nfam);
+  CKL ();
+  return ARCOS_OK;
+}
+
 
 // The fused single-grid step: two launches, ghosts from the boundary
 // conditions, state moves from dens[src] to dens[1 - src].
@@ -763,7 +911,7 @@ rk2_fused_launches (Ctx *c, int src, int fold)
   if (r) return r;
   A.fam_state = 1;
   A.cfl_fold = fold;
-  A.want_charge = c->fn ? 1 : 0;
+  A.want_charge = inloop (c) ? 1 : 0;
   return run_stage (c, A, M_S2);
 }
 
@@ -1161,10 +1309,9 @@ arcos_destroy (void *ctx)
 {
   Ctx *c = (Ctx *) ctx;
   if (!c) return ARCOS_OK;
-  if (c->graph2) cudaGraphExecDestroy (c->graph2);
-  if (c->graph_tree) cudaGraphExecDestroy (c->graph_tree);
-  if (c->adj_graph) cudaGraphExecDestroy (c->adj_graph);
+  drop_graphs (c);
   cudaFree (c->colfac_d);
+  cudaFree (c->pois_d);
   cudaFree (c->lean_nodes_d);
   cudaFree (c->adj_pool); cudaFree (c->adj_hs_d); cudaFree (c->adj_gtab_d);
   cudaFree (c->adj_gpart_d); cudaFree (c->adj_invde_d); cudaFree (c->adj_tiles_d);
@@ -1175,6 +1322,8 @@ arcos_destroy (void *ctx)
   cudaFree (c->match_tmp_d);
   cudaFree (c->xfer_d);
   cudaFree (c->maps_d);
+  cudaFree (c->rmaps_d);
+  cudaFree (c->units_d);
   if (c->own_stream) cudaStreamDestroy (c->own_stream);
   delete c;
   return ARCOS_OK;
@@ -1186,9 +1335,7 @@ arcos_set_stream (void *ctx, void *stream)
   Ctx *c = (Ctx *) ctx;
   if (!c) return fail (ARCOS_ERR_ARG, "null context");
   c->stream = stream ? (cudaStream_t) stream : c->own_stream;
-  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
-  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
-  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
+  drop_graphs (c);
   return ARCOS_OK;
 }
 
@@ -1415,13 +1562,63 @@ build_maps (Ctx *c, int ty)
   return ARCOS_OK;
 }
 
+// k_march: one-row tensor maps (MARCH_RW columns, same arrays and origin as
+// build_maps) and the work units of single-grid families, per plane, per
+// segment of MARCH_H rows, per strip - the strips of one band of rows run
+// side by side and share their halo columns through L2.
+int
+build_march (Ctx *c)
+{
+  cudaFree (c->rmaps_d);
+  c->rmaps_d = nullptr;
+  cudaFree (c->units_d);
+  c->units_d = nullptr;
+  c->n_units = 0;
+  if (!c->maps_d || c->tile_cfg < N_TILE_CFG || c->per_patch) return ARCOS_OK;
+  const int np = (int) c->pd_h.size ();
+  const int per_set = 2 * c->M.ns + 5;
+  std::vector<CUtensorMap> maps ((size_t) np * c->maps_per_patch);
+  for (int p = 0; p < np; p++) {
+    const PatchDesc &P = c->pd_h[p];
+    const cuuint64_t dims[3] = {(cuuint64_t) P.pitch, (cuuint64_t) (P.nz + 4), (cuuint64_t) P.planes};
+    const cuuint64_t strides[2] = {(cuuint64_t) P.pitch * 8, (cuuint64_t) P.plane_stride * 8};
+    const cuuint32_t box[3] = {(cuuint32_t) MARCH_RW, 1, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    for (int set = 0; set < 2; set++)
+      for (int a = 0; a < per_set; a++) {
+        double *ptr = P.base + (long long) (set * per_set + a) * P.asz;
+        CUresult r = g_encode (&maps[(size_t) p * c->maps_per_patch + set * per_set + a],
+                               CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ptr, dims, strides, box, es,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+          return fail (ARCOS_ERR_CUDA, "cuTensorMapEncodeTiled (rows) failed (" + std::to_string ((int) r) + ")");
+      }
+  }
+  CK (cudaMalloc (&c->rmaps_d, sizeof (CUtensorMap) * maps.size ()));
+  CK (cudaMemcpy (c->rmaps_d, maps.data (), sizeof (CUtensorMap) * maps.size (), cudaMemcpyHostToDevice));
+  const int H = MARCH_H[c->tile_cfg - N_TILE_CFG];
+  std::vector<MarchUnit> units;
+  for (int i = 0; i < np; i++) {
+    const PatchDesc &P = c->pd_h[i];
+    for (int pl = 0; pl < P.ntheta; pl++)
+      for (int zb = 0; zb < P.nz; zb += H)
+        for (int c0 = 0; c0 < P.nr; c0 += MARCH_OUT)
+          units.push_back ({i, pl, c0, zb, std::min (H, P.nz - zb)});
+  }
+  c->n_units = (int) units.size ();
+  CK (cudaMalloc (&c->units_d, sizeof (MarchUnit) * units.size ()));
+  CK (cudaMemcpy (c->units_d, units.data (), sizeof (MarchUnit) * units.size (), cudaMemcpyHostToDevice));
+  return ARCOS_OK;
+}
+
 // Work list of the tile kernel: per patch, per real plane, tiles of 32 columns
 // by TY rows (TY from the tile shape).
 int
 build_items (Ctx *c)
 {
   const int np = (int) c->pd_h.size ();
-  const int ty = TILE_WY[c->tile_cfg] * TILE_RPW[c->tile_cfg];
+  const int ty = TILE_WY[stage_cfg (c)] * TILE_RPW[stage_cfg (c)];
   std::vector<WorkItem> items;
   c->item_off.assign (np, 0);
   c->item_cnt.assign (np, 0);
@@ -1439,10 +1636,9 @@ build_items (Ctx *c)
   c->items_d = nullptr;
   CK (cudaMalloc (&c->items_d, sizeof (WorkItem) * items.size ()));
   CK (cudaMemcpy (c->items_d, items.data (), sizeof (WorkItem) * items.size (), cudaMemcpyHostToDevice));
-  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
-  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
-  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
-  return build_maps (c, ty);
+  drop_graphs (c);
+  int r = build_maps (c, ty);
+  return r ? r : build_march (c);
 }
 
 }  // namespace
@@ -1652,6 +1848,7 @@ arcos_commit (void *ctx)
     CK (cudaMalloc (&c->colfac_d, sizeof (double) * cf.size ()));
     CK (cudaMemcpy (c->colfac_d, cf.data (), sizeof (double) * cf.size (), cudaMemcpyHostToDevice));
   }
+  if ((r_ = build_march (c))) return r_;
   CK (cudaStreamSynchronize (c->stream));
   return ARCOS_OK;
 }
@@ -1775,16 +1972,92 @@ arcos_field_post (void *ctx, int set)
   return ARCOS_OK;
 }
 
+// The field of every stage from the device solve of poisson_kernel.cuh
+// (single 2-D grid).  The transform matrix, norms, eigenvalues and
+// tridiagonal coefficients are evaluated here, in the host solver's
+// expressions, so the device field is bit-identical to the host's.
+int
+arcos_set_field_poisson (void *ctx, int on)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  drop_graphs (c);
+  if (!on) { c->pois = false; return ARCOS_OK; }
+  if (c->pd_h.size () != 1 || !c->fused_ok || c->pd_h[0].ntheta != 1)
+    return fail (ARCOS_ERR_ARG, "the device field solve takes one 2-D grid with every side external");
+  if (c->fn) return fail (ARCOS_ERR_STATE, "a field callback is set (arcos_set_field_fn (ctx, NULL, NULL) first)");
+  const PatchDesc &P = c->pd_h[0];
+  const int nr = P.nr, nz = P.nz;
+  const double dr = P.dr, dz = P.dz, pi = 3.14159265358979323846;
+  std::vector<double> St ((size_t) nz * nz), norm (nz, 0.0), lam (nz), ta (nr), tc (nr);
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < nz; j++) {
+      const double v = sin (pi * (k + 1) * (j + 0.5) / nz);
+      St[(size_t) j * nz + k] = v;
+      norm[k] += v * v;
+    }
+  for (int k = 0; k < nz; k++) {
+    const double sk = sin (pi * (k + 1) / (2.0 * nz));
+    lam[k] = -4.0 / (dz * dz) * sk * sk;
+  }
+  for (int i = 0; i < nr; i++) {
+    const double ri = (i + 0.5) * dr, rm = i * dr, rp = (i + 1) * dr;
+    ta[i] = rm / (ri * dr * dr);
+    tc[i] = rp / (ri * dr * dr);
+  }
+  const size_t nn = (size_t) nr * nz;
+  const size_t total = St.size () + 3 * (size_t) nz + 2 * (size_t) nr + 5 * nn;
+  cudaFree (c->pois_d);
+  c->pois_d = nullptr;
+  CK (cudaMalloc (&c->pois_d, sizeof (double) * total));
+  double *q = c->pois_d;
+  PoisArgs &A = c->pois_args;
+  A.nr = nr; A.nz = nz; A.dr = dr; A.dz = dz;
+  A.St = q; q += St.size ();
+  A.norm = q; q += nz;
+  A.lam = q; q += nz;
+  A.ta = q; q += nr;
+  A.tc = q; q += nr;
+  A.qh = q; q += nn;
+  A.ph = q; q += nn;
+  A.cp = q; q += nn;
+  A.dp = q; q += nn;
+  A.phi = q; q += nn;
+  CK (cudaMemcpy ((void *) A.St, St.data (), sizeof (double) * St.size (), cudaMemcpyHostToDevice));
+  CK (cudaMemcpy ((void *) A.norm, norm.data (), sizeof (double) * nz, cudaMemcpyHostToDevice));
+  CK (cudaMemcpy ((void *) A.lam, lam.data (), sizeof (double) * nz, cudaMemcpyHostToDevice));
+  CK (cudaMemcpy ((void *) A.ta, ta.data (), sizeof (double) * nr, cudaMemcpyHostToDevice));
+  CK (cudaMemcpy ((void *) A.tc, tc.data (), sizeof (double) * nr, cudaMemcpyHostToDevice));
+  c->pois = true;
+  return ARCOS_OK;
+}
+
+// One device field solve of set `set` (the charge must be current), for tests
+// and for callers that step the grid-level entry points themselves.
+int
+arcos_solve_field (void *ctx, int set)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (!c->pois || !c->pois_d) return fail (ARCOS_ERR_STATE, "arcos_set_field_poisson (ctx, 1) first");
+  if (set < 0 || set > 1) return fail (ARCOS_ERR_ARG, "bad set");
+  if ((r = device_poisson (c, set))) return r;
+  c->field_set[set] = true;
+  CK (cudaStreamSynchronize (c->stream));
+  return ARCOS_OK;
+}
+
 int
 arcos_set_field_fn (void *ctx, arcos_field_fn fn, void *user)
 {
   Ctx *c = (Ctx *) ctx;
   if (!c) return fail (ARCOS_ERR_ARG, "null context");
+  if (fn && c->pois) return fail (ARCOS_ERR_STATE, "the device field solve is on (arcos_set_field_poisson (ctx, 0) first)");
   c->fn = fn;
   c->user = user;
-  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
-  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
-  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
+  drop_graphs (c);
   return ARCOS_OK;
 }
 
@@ -1794,9 +2067,7 @@ arcos_set_per_patch (void *ctx, int on)
   Ctx *c = (Ctx *) ctx;
   if (!c) return fail (ARCOS_ERR_ARG, "null context");
   c->per_patch = on != 0;
-  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
-  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
-  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
+  drop_graphs (c);
   return ARCOS_OK;
 }
 
@@ -2049,7 +2320,7 @@ arcos_cdr_rk2 (void *ctx, double h, double t, double *h_used)
   (void) t;
   int r = chk_committed (c);
   if (r) return r;
-  if (!c->fn && !(c->field_set[0] && c->field_set[1]))
+  if (!inloop (c) && !(c->field_set[0] && c->field_set[1]))
     return fail (ARCOS_ERR_STATE, "no field: call arcos_set_field (+ arcos_field_post) for both sets, or arcos_set_field_fn");
   if ((r = set_h_attempt (c, h))) return r;
   if ((r = rk2_general (c))) return r;
@@ -2068,12 +2339,12 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
   int r = chk_committed (c);
   if (r) return r;
   if (nsteps < 0) return fail (ARCOS_ERR_ARG, "nsteps < 0");
-  if (!c->fn && !(c->field_set[0] && c->field_set[1]))
+  if (!inloop (c) && !(c->field_set[0] && c->field_set[1]))
     return fail (ARCOS_ERR_STATE, "no field: call arcos_set_field (+ arcos_field_post) for both sets, or arcos_set_field_fn");
   std::vector<DevState> st0;
   if ((r = read_states (c, st0))) return r;
   const int step0 = st0[0].step;
-  const bool fixed_fused = c->fused_ok && !c->fn;
+  const bool fixed_fused = c->fused_ok && !inloop (c);
   if (fixed_fused) {
     // set_h_attempt and reset_dmax (slot 0) in one stream-ordered write
     c->st_stage = st0;
@@ -2088,12 +2359,13 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
   } else if ((r = set_h_attempt (c, h))) {
     return r;
   }
-  if (!c->fused_ok && !c->fn && !c->per_patch && nsteps > 0) {
+  if (!c->fused_ok && !inloop (c) && !c->per_patch && nsteps > 0) {
     // trees: one step (all its batched launches) captured once, replayed
+    const bool lean = lean_tree_ok (c);
     if (!c->graph_tree) {
       cudaGraph_t gr;
       CK (cudaStreamBeginCapture (c->stream, cudaStreamCaptureModeThreadLocal));
-      int e = rk2_general (c);
+      int e = lean ? rk2_lean_tree (c) : rk2_general (c);
       cudaError_t ee = cudaStreamEndCapture (c->stream, &gr);
       if (e) return e;
       if (ee != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("graph capture: ") + cudaGetErrorString (ee));
@@ -2101,35 +2373,28 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
       cudaGraphDestroy (gr);
     }
     for (int k = 0; k < nsteps; k++) CK (cudaGraphLaunch (c->graph_tree, c->stream));
+    if (lean && (r = do_prepare (c, 0))) return r;      // cdr.c:1322, once
   } else if (!c->fused_ok) {
     for (int k = 0; k < nsteps; k++)
       if ((r = rk2_general (c))) return r;
-  } else if (c->fn) {
-    // field in the loop: the host solve sits between the stages
-    for (int k = 0; k < nsteps; k++) {
-      if ((r = field_from_callback (c, 0, 0))) return r;
-      if ((r = reset_dmax (c, 0))) return r;
-      if ((r = do_dmax (c, 0, 0))) return r;
-      k_cfl<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->M, c->st_d, c->nfam, 0);
-      CKL ();
-      StageArgs A = base_args (c);
-      A.src = 0;
-      if ((r = run_stage (c, A, M_S1))) return r;
-      long long w = 0;
-      for (auto &P : c->pd_h) w = std::max (w, P.asz);
-      if ((r = for_patches (c, w, [&] (dim3 g, const int *pl) {
-             k_charge_star<<<g, 256, 0, c->stream>>> (c->M, c->pd_d, pl, 0, c->st_d);
-           }))) return r;
-      if ((r = field_from_callback (c, 1, 1))) return r;
-      A.dst = 1; A.fam_state = 0; A.want_charge = 1;
-      if ((r = run_stage (c, A, M_S2))) return r;
-      // move the state back to set 0 (the callback path keeps it there)
-      for (auto &P : c->pd_h) {
-        CK (cudaMemcpyAsync (P.arr (0, K_DENS, 0), P.arr (1, K_DENS, 0), sizeof (double) * P.asz * P.ns, cudaMemcpyDeviceToDevice, c->stream));
-        CK (cudaMemcpyAsync (P.arr (0, K_CHARGE), P.arr (1, K_CHARGE), sizeof (double) * P.asz, cudaMemcpyDeviceToDevice, c->stream));
+  } else if (inloop (c)) {
+    // field in the loop: the solve sits between the stages.  With the device
+    // solve the whole step is stream-ordered and replayed from a graph.
+    if (c->pois && nsteps > 0) {
+      if (!c->graph_inloop) {
+        cudaGraph_t gr;
+        CK (cudaStreamBeginCapture (c->stream, cudaStreamCaptureModeThreadLocal));
+        int e = rk2_inloop_step (c);
+        cudaError_t ee = cudaStreamEndCapture (c->stream, &gr);
+        if (e) return e;
+        if (ee != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("graph capture: ") + cudaGetErrorString (ee));
+        CK (cudaGraphInstantiate (&c->graph_inloop, gr, 0));
+        cudaGraphDestroy (gr);
       }
-      k_step_end<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->st_d, c->nfam);
-      CKL ();
+      for (int k = 0; k < nsteps; k++) CK (cudaGraphLaunch (c->graph_inloop, c->stream));
+    } else {
+      for (int k = 0; k < nsteps; k++)
+        if ((r = rk2_inloop_step (c))) return r;
     }
     // ghosts of the final state as prepare_grid leaves them (cdr.c:1322)
     if ((r = do_ext_bnd (c, 0))) return r;
@@ -2214,8 +2479,11 @@ arcos_run_enqueue (void *ctx, int nsteps)
   Ctx *c = (Ctx *) ctx;
   int r = chk_committed (c);
   if (r) return r;
-  if (!c->graph2 || (nsteps & 1)) return fail (ARCOS_ERR_STATE, "call arcos_run_prepare; nsteps must be even");
+  if (!c->graph2) return fail (ARCOS_ERR_STATE, "call arcos_run_prepare first");
+  if ((nsteps & 1) && !lean_ok (c))
+    return fail (ARCOS_ERR_STATE, "nsteps must be even on this path (the state alternates between sets)");
   for (int k = 0; k < nsteps / 2; k++) CK (cudaGraphLaunch (c->graph2, c->stream));
+  if (nsteps & 1) return rk2_fused_launches (c, 0, 1);   // the lean step keeps the state in set 0
   return ARCOS_OK;
 }
 
@@ -2383,14 +2651,6 @@ arcos_adj_table_offset (void *ctx, int reaction)
 }
 
 // ---- model parameters after commit (the adjoint's inputs) ----
-static void
-drop_graphs (Ctx *c)
-{
-  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
-  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
-  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
-}
-
 int
 arcos_set_species_mass (void *ctx, int species, double mass)
 {
@@ -2468,9 +2728,7 @@ arcos_set_exact (void *ctx, int on)
   Ctx *c = (Ctx *) ctx;
   if (!c) return fail (ARCOS_ERR_ARG, "null context");
   c->exact = on ? 1 : 0;
-  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
-  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
-  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
+  drop_graphs (c);
   return ARCOS_OK;
 }
 
@@ -2482,7 +2740,7 @@ arcos_set_tile (void *ctx, int cfg)
 {
   Ctx *c = (Ctx *) ctx;
   if (!c) return fail (ARCOS_ERR_ARG, "null context");
-  if (cfg < 0 || cfg >= N_TILE_CFG) return fail (ARCOS_ERR_ARG, "tile shape out of range");
+  if (cfg < 0 || cfg >= N_TILE_CFG + N_MARCH_H) return fail (ARCOS_ERR_ARG, "tile shape out of range");
   c->tile_cfg = cfg;
   if (c->committed) return build_items (c);
   return ARCOS_OK;
@@ -2495,10 +2753,8 @@ arcos_set_tma (void *ctx, int on)
   Ctx *c = (Ctx *) ctx;
   if (!c) return fail (ARCOS_ERR_ARG, "null context");
   c->use_tma = on ? 1 : 0;
-  if (c->graph2) { cudaGraphExecDestroy (c->graph2); c->graph2 = nullptr; }
-  if (c->graph_tree) { cudaGraphExecDestroy (c->graph_tree); c->graph_tree = nullptr; }
-  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
-  if (c->committed) return build_maps (c, TILE_WY[c->tile_cfg] * TILE_RPW[c->tile_cfg]);
+  drop_graphs (c);
+  if (c->committed) return build_maps (c, TILE_WY[stage_cfg (c)] * TILE_RPW[stage_cfg (c)]);
   return ARCOS_OK;
 }
 

@@ -473,6 +473,29 @@ k_reset_dmax (DevState *st, int nfam, int slot_rel)
   if (f < nfam) st[f].dmax_key[(st[f].step + slot_rel) & 1] = dkey (-1.0);
 }
 
+// Start of a field-solve step, stream-ordered: the current dmax slot is
+// reset and the state counts as unchecked for the stage-1 clamp.
+__global__ void
+k_run_reset (DevState *st, int nfam)
+{
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nfam) return;
+  st[f].dmax_key[st[f].step & 1] = dkey (-1.0);
+  st[f].neg[st[f].step & 1] = 1u;
+  st[f].neg[(st[f].step + 1) & 1] = 0u;
+}
+
+// Before a set's field is post-processed: its E_theta counters and field
+// maxima start over.
+__global__ void
+k_field_reset (int *etz, int np, int set, DevState *st, int nfam)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < np) etz[i * 2 + set] = 0;
+  if (i < nfam)
+    for (int k = 0; k < 3; k++) st[i].emax_key[set][k] = dkey (-1.0);
+}
+
 // Ends a step of every family whose stage-2 kernel did not fold the CFL.
 __global__ void
 k_step_end (DevState *st, int nfam)

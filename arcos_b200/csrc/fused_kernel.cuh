@@ -33,6 +33,8 @@ namespace arcos {
 #define FUSED_MAXS 6
 #define FUSED_MAXR ARCOS_MAXR
 
+struct MarchUnit;
+
 struct FusedArgs {
   const PatchDesc *patches;
   const WorkItem *items;
@@ -49,6 +51,10 @@ struct FusedArgs {
   int stage_eabs;            // some patch has E_theta != 0
   const CUtensorMap *maps;   // [patch][set][array]
   int maps_per_patch;
+  const struct MarchUnit *units;   // k_march: work units (warp, plane, strip, segment)
+  int n_units;
+  const CUtensorMap *rmaps;  // k_march: one-row boxes [patch][set][array]
+  int rmaps_per_patch;
   const double *colfac;      // per column ir: ir / ((ir + 1/2) dr), (ir + 1) / ((ir + 1/2) dr)
   double cm[FUSED_MAXS];     // charge / mass (0 for immobile species: zero flux) (.f90:90)
   double ddr[FUSED_MAXS];    // (diffusion_coeff / mass) / dr (.f90:85,174)

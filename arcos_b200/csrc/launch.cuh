@@ -10,6 +10,7 @@
 #include "stage_kernel.cuh"
 #include "fused_kernel.cuh"
 #include "adjoint_kernel.cuh"
+#include "march_kernel.cuh"
 
 namespace arcos {
 
@@ -22,6 +23,10 @@ constexpr int N_TILE_CFG = 3;
 constexpr int TILE_WY[N_TILE_CFG] = {4, 8, 8};
 constexpr int TILE_RPW[N_TILE_CFG] = {4, 4, 2};
 
+// Segment heights of the marching kernel (tile shapes N_TILE_CFG ..).
+constexpr int N_MARCH_H = 3;
+constexpr int MARCH_H[N_MARCH_H] = {16, 32, 64};
+
 // Each launches (occ == nullptr) or returns the resident blocks per SM in
 // *occ (after setting the kernel's dynamic shared-memory limit).
 template <int NS>
@@ -30,6 +35,8 @@ cudaError_t launch_stage_ns (int mode, int cfg, const Model &M, const StageArgs 
 template <int NS>
 cudaError_t launch_fused_ns (bool s2, int cfg, const Model &M, const FusedArgs &A, int blocks,
                              cudaStream_t s, int *occ);
+template <int NS>
+cudaError_t launch_march_ns (bool s2, bool tree, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s);
 template <int NS>
 cudaError_t launch_vjp_ns (const Model &M, const VjpArgs &A, int blocks, size_t smem, cudaStream_t st,
                            int *occ);
@@ -40,7 +47,9 @@ cudaError_t launch_vjp_ns (const Model &M, const VjpArgs &A, int blocks, size_t 
   extern template cudaError_t launch_fused_ns<N> (bool, int, const Model &, const FusedArgs &, int,  \
                                                   cudaStream_t, int *);                              \
   extern template cudaError_t launch_vjp_ns<N> (const Model &, const VjpArgs &, int, size_t,         \
-                                                cudaStream_t, int *);
+                                                cudaStream_t, int *);                                \
+  extern template cudaError_t launch_march_ns<N> (bool, bool, const Model &, const FusedArgs &, int, \
+                                                  cudaStream_t);
 ARCOS_DECLARE_NS (1)
 ARCOS_DECLARE_NS (2)
 ARCOS_DECLARE_NS (3)

@@ -106,6 +106,25 @@ launch_vjp_ns (const Model &M, const VjpArgs &A, int blocks, size_t smem, cudaSt
   return cudaGetLastError ();
 }
 
+template <int NS, bool S2, bool TREE>
+cudaError_t
+launch_march_t (const Model &M, const FusedArgs &A, int blocks, cudaStream_t s)
+{
+  const size_t sm = march_smem_bytes<NS> ();
+  cudaFuncSetAttribute (k_march<NS, S2, TREE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+  k_march<NS, S2, TREE><<<blocks, 32 * MARCH_WPB, sm, s>>> (M, A);
+  return cudaGetLastError ();
+}
+
+template <int NS>
+cudaError_t
+launch_march_ns (bool s2, bool tree, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s)
+{
+  if (tree) return s2 ? launch_march_t<NS, true, true> (M, A, blocks, s) : launch_march_t<NS, false, true> (M, A, blocks, s);
+  return s2 ? launch_march_t<NS, true, false> (M, A, blocks, s) : launch_march_t<NS, false, false> (M, A, blocks, s);
+}
+
+template cudaError_t launch_march_ns<ARCOS_NS> (bool, bool, const Model &, const FusedArgs &, int, cudaStream_t);
 template cudaError_t launch_stage_ns<ARCOS_NS> (int, int, const Model &, const StageArgs &, int, cudaStream_t, int *);
 template cudaError_t launch_fused_ns<ARCOS_NS> (bool, int, const Model &, const FusedArgs &, int, cudaStream_t, int *);
 template cudaError_t launch_vjp_ns<ARCOS_NS> (const Model &, const VjpArgs &, int, size_t, cudaStream_t, int *);

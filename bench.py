@@ -53,13 +53,34 @@ def workload_config(extra=None):
 
 # ---------------------------------------------------------------- clocks ----
 class ClockSampler:
+    """SM clock and clock-event reasons of one GPU, sampled in a background
+    thread while the timed region runs: through NVML every ~0.5 ms (the
+    timed region of a short run lasts a few milliseconds), else through
+    nvidia-smi every 50 ms.  Reads only; no setting is changed."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # nvmlClocksEventReason* bits
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+            "hw_thermal_slowdown": 0x40}
 
     def __init__(self, device: int):
-        self.lines = []
+        self.lines = []          # (time, sm_mhz, max_mhz, set of reasons)
         self.proc = None
+        self.stop_flag = False
+        self.th = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[device]) if vis and vis.split(",")[device].isdigit() else device
+            self.nv, self.h = pynvml, pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self.mx = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.th = threading.Thread(target=self._poll_nvml, daemon=True)
+            self.th.start()
+            return
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
@@ -68,42 +89,60 @@ class ClockSampler:
         except Exception:
             self.proc = None
             return
-        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th = threading.Thread(target=self._read_smi, daemon=True)
         self.th.start()
         t0 = time.time()
         while not self.lines and time.time() - t0 < 10:
             time.sleep(0.02)
 
-    def _read(self):
+    def _poll_nvml(self):
+        nv = self.nv
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop_flag:
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                bits = int(get_reasons(self.h))
+            except Exception:
+                break
+            rs = {n for n, b in self.BITS.items() if bits & b}
+            self.lines.append((time.time(), sm, self.mx, rs))
+            time.sleep(0.0005)
+
+    def _read_smi(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.proc.stdout:
-            self.lines.append((time.time(), line.strip()))
+            f = [x.strip() for x in line.strip().split(",")]
+            try:
+                sm, mx = float(f[1]), float(f[2])
+            except (ValueError, IndexError):
+                continue
+            rs = {n for n, v in zip(names, f[5:9]) if v.lower().startswith("active")}
+            self.lines.append((time.time(), sm, mx, rs))
 
     def stop(self):
+        self.stop_flag = True
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.th is not None:
+            self.th.join(timeout=2)
 
     def summary(self, t0: float, t1: float):
-        rows = [l for (ts, l) in self.lines if t0 - 0.06 <= ts <= t1 + 0.06]
+        rows = [r for r in self.lines if t0 <= r[0] <= t1]
         if not rows and self.lines:
-            rows = [min(self.lines, key=lambda x: abs(x[0] - (t0 + t1) / 2))[1]]
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            rows = [min(self.lines, key=lambda x: abs(x[0] - (t0 + t1) / 2))]
+        sm = [r[1] for r in rows]
+        mx = rows[-1][2] if rows else None
+        reasons = set()
         for r in rows:
-            f = [x.strip() for x in r.split(",")]
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except (ValueError, IndexError):
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
+            reasons |= r[3]
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.nv else "nvidia-smi"}
 
 
 # ------------------------------------------------------------ CPU baseline ----
@@ -178,20 +217,29 @@ def run_reference(args):
 
 
 def _reference_line(args):
+    """The reference's own CPU step on this workload: the serial build as
+    shipped (oracle/_ref/libarcos_ref.so, the reference's C with its Fortran
+    flux kernel restated), drift/diffusion on every theta plane.  Each timed
+    step is one RK2 step of the whole 512 x 1024 x 16 grid when the run is
+    short enough (K + W <= 40 steps, about 3 s per step on one core);
+    otherwise a slab of the grid's rows sized so the run stays within a few
+    minutes.  The reference's OpenMP build is not used: the parallel region
+    of react_apply (src/reaction.c:95-160) shares its per-cell temporaries
+    (eabs, log_e, pos, e1, e2, rate, r_mod, ...) between threads, a data race
+    that makes it both slower than the serial build and wrong."""
     from oracle import bind
-    omp = bind.ref_available(True)
-    # each "step" is one RK2 step of the 512 x 64 x 16 slab
     from arcos_b200 import workloads
-    pb = workloads.plain(nr=NR, nz=SAMPLE_NZ, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=0)
-    threads = os.cpu_count() or 1
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    if bind.ref_available(omp):
-        t = bind.RefTree(pb.params, pb.model, pb.specs, field_mode=bind.FIELD_FIXED, omp=omp)
+    total_steps = args.steps + args.warmup
+    nz = NZ if total_steps <= 40 else max(16, min(NZ, (NZ * 40 // max(1, total_steps)) // 16 * 16))
+    pb = workloads.plain(nr=NR, nz=nz, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=0)
+    threads = 1
+    if bind.ref_available(False):
+        t = bind.RefTree(pb.params, pb.model, pb.specs, field_mode=bind.FIELD_FIXED, omp=False)
         kind = "reference"
         step = lambda: t.rk2_sw(50.0, per_plane=True, zero_all=False)  # noqa: E731
     else:
         t = bind.PortTree(pb.params, pb.model, pb.specs, field_mode=bind.FIELD_FIXED)
-        kind, threads = "port", 1
+        kind = "port"
         step = lambda: t.rk2(50.0)  # noqa: E731
     for s in range(NS):
         t.dens(0, s)[...] = pb.dens[0][s]
@@ -203,14 +251,15 @@ def _reference_line(args):
     for _ in range(args.steps):
         step()
     el = time.perf_counter() - t0
-    value = NR * SAMPLE_NZ * NTHETA * NS * args.steps / el
-    sample = (f"each step: one RK2 step of a {NR}x{SAMPLE_NZ}x{NTHETA} slab of the grid "
-              f"({'OpenMP build' if omp else 'serial build'})")
+    value = NR * nz * NTHETA * NS * args.steps / el
+    what = "the whole grid" if nz == NZ else f"a {NR}x{nz}x{NTHETA} slab of the grid"
+    sample = (f"each step: one RK2 step of {what} (serial build as shipped; "
+              f"{'the reference C' if kind == 'reference' else 'the CPU restatement'})")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": workload_config({"reference_sample": sample}),
+            "config": workload_config({"replicas": args.gpus}),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -533,10 +582,13 @@ def run_device(args):
     else:
         tree.set_tile(args.tile)
         tune = {}
-    warm = max(4, args.warmup + (args.warmup & 1))
-    steps = args.steps + (args.steps & 1)
+    # the lean path takes any step count; the bit-exact path alternates storage sets
+    warm, steps = args.warmup, args.steps
+    if args.exact:
+        warm, steps = warm + (warm & 1), steps + (steps & 1)
     check(L.arcos_run_prepare(h, 50.0))
-    check(L.arcos_run_enqueue(h, warm))
+    if warm > 0:
+        check(L.arcos_run_enqueue(h, warm))
     torch.cuda.synchronize()
 
     clk = ClockSampler(dev_id) if rank == 0 else None

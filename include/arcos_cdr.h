@@ -125,6 +125,18 @@ int arcos_set_field (void *ctx, int grid, int set, const double *er,
 typedef int (*arcos_field_fn) (void *user, int stage, const double *charge,
                                double *er, double *ez, double *etheta);
 int arcos_set_field_fn (void *ctx, arcos_field_fn fn, void *user);
+/* The field solve of pois_solve_a (src/poisson.c:763-767, FISHPACK hstcyl,
+ * fish90/src/hst_procs.f90:1439) on the device, for one 2-D grid with every
+ * side external: the 5-point cylindrical operator, regular axis, Dirichlet
+ * conditions on r = L_r, z = 0, z = L_z, solved by a sine transform in z and
+ * a tridiagonal solve in r per mode.  When on (1), every stage of arcos_run
+ * and arcos_cdr_rk2 solves the field from the current charge with no host
+ * round trip (arcos_run replays the whole step from a CUDA graph).  Excludes
+ * arcos_set_field_fn. */
+int arcos_set_field_poisson (void *ctx, int on);
+/* One device field solve of storage set `set` from its current charge, then
+ * the external field, |E| and theta periodicity (as arcos_field_post). */
+int arcos_solve_field (void *ctx, int set);
 
 /* ---- reference entry points (src/cdr.c, src/reaction.c) -----------------
  * Each acts on the whole grid family of the given storage set, with the
@@ -207,7 +219,9 @@ int arcos_set_per_patch (void *ctx, int on);
 int arcos_set_exact (void *ctx, int on);
 /* Tile shape of the stencil kernel: 0 = 32x16 cells with 128 threads,
  * 1 = 32x32 cells with 256 threads, 2 (default) = 32x16 cells with 256
- * threads.  Any time. */
+ * threads; 3, 4, 5 = the marching form of the lean fused step (one warp per
+ * 31-column strip and segment of 16, 32 or 64 rows; the other kernels keep
+ * shape 2).  Any time. */
 int arcos_set_tile (void *ctx, int cfg);
 /* 1 (default): stage stencil tiles in shared memory with TMA bulk tensor
  * copies; 0: with per-thread cp.async.  Same results either way. */
@@ -216,7 +230,8 @@ int arcos_get_tile (void *ctx);
 int arcos_num_items (void *ctx);
 /* Device-timed runs: arcos_run_prepare sets the attempted step, computes the
  * first step's h and instantiates the two-step CUDA graph; arcos_run_enqueue
- * enqueues nsteps (even) steps on the context stream without synchronising. */
+ * enqueues nsteps steps on the context stream without synchronising (an odd
+ * nsteps only on the lean fused path, whose state stays in one storage set). */
 int arcos_run_prepare (void *ctx, double h);
 int arcos_run_enqueue (void *ctx, int nsteps);
 /* Enqueue one fused stage kernel (1: stage 1, 2: stage 2) reading dens[src]. */

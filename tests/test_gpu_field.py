@@ -69,7 +69,7 @@ def test_fast_limiter_per_step_on_wavy_field(cuda_device, ntheta):
             dev.upload(0, "dens", b, s)
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("ntheta", [1, 4])
 def test_fused_every_tile_shape_on_wavy_field(cuda_device, tile, ntheta):
     pb = wavy(ntheta=ntheta, seed=21)
@@ -99,7 +99,7 @@ def test_fast_limiter_long_run_on_wavy_field(cuda_device):
         assert rel_err(a, b) <= 1e-9, rel_err(a, b)
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5])
 def test_kinetic_batch_on_wavy_field(cuda_device, tile):
     """Six species, nine reactions, |E| beyond both ends of the 200-node
     tables, three families with their own applied fields, each tile shape."""

@@ -102,6 +102,33 @@ def test_amr_tree(cuda_device):
     compare_state(dev, port, pb)
 
 
+@pytest.mark.parametrize("tile", [3, 4, 5])
+@pytest.mark.parametrize("field", ["uniform", "wavy"])
+def test_amr_tree_lean_batched_step(cuda_device, tile, field):
+    """The lean batched tree step (k_march over every patch, ghosts from
+    prepare_grid) per step against the oracle at 1e-12; also 3 steps replayed
+    from the step graph in one call."""
+    pb = workloads.amr(n_patches=12, levels=3, root_nr=32, root_nz=64, side_lo=8, side_hi=24, seed=2)
+    if field == "wavy":
+        pb.fields = [workloads.wavy_field(sp, pb.params, seed=50 + g) for g, sp in enumerate(pb.specs)]
+    port = port_tree(pb, zero_all=True)
+    dev = device_tree(pb, exact=False)
+    dev.set_tile(tile)
+    for _ in range(3):
+        hp = port.rk2(50.0)[0]
+        hd = dev.run(1, 50.0)[0][0]
+        assert abs(hd - hp) <= TOL * hp
+        for g in range(len(pb.specs)):
+            for s in range(2):
+                a, b = dev.download(g, "dens", s), port.dens(g, s)
+                assert rel_err(a, b) <= TOL, (tile, g, s, rel_err(a, b))
+                dev.upload(g, "dens", b, s)
+    dts_p = [port.rk2(50.0)[0] for _ in range(3)]
+    dts_d = dev.run(3, 50.0)[0]
+    assert rel_err(dts_d, np.array(dts_p)) <= TOL
+    compare_state(dev, port, pb)
+
+
 def test_amr_per_patch_mode_identical(cuda_device):
     pb = workloads.amr(n_patches=10, levels=3, root_nr=32, root_nz=64, side_lo=8, side_hi=24, seed=4)
     a = device_tree(pb)
@@ -200,7 +227,7 @@ def test_fast_limiter_long_run(cuda_device):
         assert rel_err(a, b) <= 1e-9, rel_err(a, b)
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("ntheta", [1, 4])
 def test_fused_every_tile_shape(cuda_device, tile, ntheta):
     """The fused step (division-free limiter) with each tile shape the
@@ -225,7 +252,7 @@ def test_fused_every_tile_shape(cuda_device, tile, ntheta):
         assert rel_err(dev.download(0, "dens", s), port.dens(0, s)) <= 4 * TOL
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5])
 def test_kinetic_batch_fused_every_tile_shape(cuda_device, tile):
     """Six species, nine reactions, three families of different sizes on the
     fused path with each tile shape, per step against the oracle at 1e-12."""
