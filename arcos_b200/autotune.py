@@ -46,3 +46,31 @@ def autotune_tiles(tree, steps: int = 6, h: float = 50.0, stream=None) -> Dict[i
     best = min(times, key=times.get)
     tree.set_tile(best)
     return times
+
+
+TREE_SHAPES = (2, 3, 4, 5)   # 2: the general tree step (k_stage tiles); 3-5: the lean batched step
+
+
+def autotune_tree(tree, steps: int = 4, h: float = 50.0, stream=None,
+                  shapes=TREE_SHAPES) -> Dict[int, float]:
+    """Times ``steps`` batched steps of a refinement tree (arcos_run, one
+    CUDA graph per step) per shape and selects the fastest.  Shape 2 runs
+    the general tree step, shapes 3-5 the lean one (k_march with segments
+    of 16, 32, 64 rows).  Returns {shape: ms per step}; the state advances."""
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream()
+    times = {}
+    for cfg in shapes:
+        tree.set_tile(cfg)
+        tree.run(1, h)                      # capture the step graph
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        tree.run(steps, h)
+        e1.record(s)
+        e1.synchronize()
+        times[cfg] = e0.elapsed_time(e1) / steps
+    best = min(times, key=times.get)
+    tree.set_tile(best)
+    return times

@@ -285,10 +285,13 @@ def _load(tree, pb):
 
 def extra_amr(stream, steps: int = 10):
     """Batched AMR: 4 levels, 320 patches (sides 16..256) advanced by one
-    launch per kernel kind over all patches (replayed from a CUDA graph)
+    launch per kernel kind over all patches (one CUDA graph per step), the
+    step form picked by the tree autotuner (the general step with tiled
+    stage kernels, or the lean step with k_march at three segment heights),
     against one launch per patch, same GPU, same steps."""
     import numpy as np
     from arcos_b200 import workloads
+    from arcos_b200.autotune import autotune_tree
     from arcos_b200.cdr import CdrTree
     from arcos_b200._lib import check
     pb = workloads.amr()
@@ -298,6 +301,11 @@ def extra_amr(stream, steps: int = 10):
     for mode in ("batched", "per_patch"):
         tree = CdrTree(pb.params, pb.model, pb.specs, stream=stream.cuda_stream, per_patch=(mode == "per_patch"))
         _load(tree, pb)
+        if mode == "batched":
+            tune = autotune_tree(tree, steps=4, stream=stream)
+            out["tree_autotune_ms_per_step"] = {str(k): v for k, v in tune.items()}
+            out["tree_shape"] = tree.L.arcos_get_tile(tree.h)
+            _load(tree, pb)
         nf = sum(1 for sp in pb.specs if sp.parent < 0)
         dts = np.zeros(nf * steps)
         tree.run(2, 50.0)
@@ -310,7 +318,21 @@ def extra_amr(stream, steps: int = 10):
         tree.close()
     out["batched_value"] = pb.cells * 2 / (out["batched_ms_per_step"] / 1e3)
     out["batched_over_per_patch"] = out["per_patch_ms_per_step"] / out["batched_ms_per_step"]
+    step_bytes = 8 * (5 * 2 + 4) * pb.cells          # 8 (5S + 4) per cell and step
+    gbs = step_bytes / (out["batched_ms_per_step"] / 1e3) / 1e9
+    peak, src = _peak_hbm()
+    out["roofline"] = {"bound": "hbm", "achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak,
+                       "peak_source": src, "algorithmic_bytes_per_step": step_bytes}
     return out
+
+
+def _peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fp:
+            peaks = json.load(fp)
+        return float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
 
 
 def _time_sweep(tree, stream) -> float:
