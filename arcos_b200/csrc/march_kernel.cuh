@@ -34,6 +34,8 @@ namespace arcos {
 
 constexpr int MARCH_OUT = 31;     // result columns per strip (lane 31 only supplies a face)
 constexpr int MARCH_RW = 36;      // doubles per staged row of one array: columns X0-2 .. X0+33
+constexpr int MARCH_AS = 48;      // ring stride of one array's row: a bulk tensor copy writes
+                                  // to a 128-byte aligned shared-memory address (384 = 3 x 128)
 constexpr int MARCH_R = 8;        // ring rows per warp (power of two)
 constexpr int MARCH_WPB = 4;      // warps per block
 
@@ -44,9 +46,10 @@ struct MarchUnit {
 template <int NS>
 struct MarchLayout {
   static constexpr int NA = NS + 2;                // densities, er, ez
-  static constexpr int ROW = NA * MARCH_RW;        // doubles per ring row
+  static constexpr int ROW = NA * MARCH_AS;        // doubles per ring row
   static constexpr int WARP = MARCH_R * ROW;       // doubles per warp
-  static constexpr unsigned ROW_BYTES = sizeof (double) * ROW;
+  static constexpr unsigned ROW_BYTES = sizeof (double) * NA * MARCH_RW;   // bytes the copies deliver
+  static_assert ((sizeof (double) * MARCH_AS) % 128 == 0, "ring rows must stay 128-byte aligned");
 };
 
 template <int NS>
@@ -142,9 +145,9 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       mbar_expect_tx (&bar[slot], LY::ROW_BYTES);
       const int y = zb + i, z = plane - P->theta0;  // map rows start at ghost row -2
 #pragma unroll
-      for (int s = 0; s < NS; s++) tma_load_3d (dst + s * MARCH_RW, tm + fset * per_set + s, X0, y, z, &bar[slot]);
-      tma_load_3d (dst + NS * MARCH_RW, tm + fset * per_set + 2 * NS + 0, X0, y, z, &bar[slot]);
-      tma_load_3d (dst + (NS + 1) * MARCH_RW, tm + fset * per_set + 2 * NS + 1, X0, y, z, &bar[slot]);
+      for (int s = 0; s < NS; s++) tma_load_3d (dst + s * MARCH_AS, tm + fset * per_set + s, X0, y, z, &bar[slot]);
+      tma_load_3d (dst + NS * MARCH_AS, tm + fset * per_set + 2 * NS + 0, X0, y, z, &bar[slot]);
+      tma_load_3d (dst + (NS + 1) * MARCH_AS, tm + fset * per_set + 2 * NS + 1, X0, y, z, &bar[slot]);
     };
     auto rowp = [&] (int j) -> double * {          // ring row of absolute row j
       return ring + ((g + (unsigned) (j - zb + 2)) & (MARCH_R - 1)) * LY::ROW;
@@ -159,8 +162,8 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       if (clamp) {
 #pragma unroll
         for (int s = 0; s < NS; s++) {
-          rp[s * MARCH_RW + lane] = clamp0 (rp[s * MARCH_RW + lane]);
-          if (lane < MARCH_RW - 32) rp[s * MARCH_RW + 32 + lane] = clamp0 (rp[s * MARCH_RW + 32 + lane]);
+          rp[s * MARCH_AS + lane] = clamp0 (rp[s * MARCH_AS + lane]);
+          if (lane < MARCH_RW - 32) rp[s * MARCH_AS + 32 + lane] = clamp0 (rp[s * MARCH_AS + 32 + lane]);
         }
         __syncwarp ();
       }
@@ -171,18 +174,18 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
             const int gc = -1 - o;
             double v;
             if (nt == 1) {
-              v = rp[s * MARCH_RW + (-1 - gc) + 2 - X0];
+              v = rp[s * MARCH_AS + (-1 - gc) + 2 - X0];
             } else {
               const int pl2 = (plane + nt / 2) % nt;
               v = P->arr (fset, K_DENS, s)[P->off (-1 - gc, j, pl2)];
               if (!S2) v = clamp0 (v);
             }
-            rp[s * MARCH_RW + gc + 2 - X0] = v;
+            rp[s * MARCH_AS + gc + 2 - X0] = v;
           }
           const int gc = nr + o;                    // r = L_r: columns nr, nr+1
           const int ix = gc + 2 - X0;
           if (ix >= 0 && ix < MARCH_RW)
-            rp[s * MARCH_RW + ix] = (double) M.bnd_sign[1] * rp[s * MARCH_RW + (2 * nr - 1 - gc) + 2 - X0];
+            rp[s * MARCH_AS + ix] = (double) M.bnd_sign[1] * rp[s * MARCH_AS + (2 * nr - 1 - gc) + 2 - X0];
         }
         __syncwarp ();
       }
@@ -194,7 +197,7 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       double *rp = rowp (j);
       const double *sp = rowp (src);
 #pragma unroll
-      for (int s = 0; s < NS; s++) rp[s * MARCH_RW + ci] = sg * sp[s * MARCH_RW + ci];
+      for (int s = 0; s < NS; s++) rp[s * MARCH_AS + ci] = sg * sp[s * MARCH_AS + ci];
       __syncwarp ();
     };
 
@@ -240,15 +243,15 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
 
     // face below the first row (.f90:310-386), velocity from ez at row zb - 1
     double fzb[NS];
-    double ez_prev = rowp (zb - 1)[(NS + 1) * MARCH_RW + ci];
+    double ez_prev = rowp (zb - 1)[(NS + 1) * MARCH_AS + ci];
     {
       const int zs = field_sign1 (ez_prev);
       const double *rm2 = rowp (zb - 2), *rm1 = rowp (zb - 1), *r0 = rowp (zb), *rp1 = rowp (zb + 1);
 #pragma unroll
       for (int s = 0; s < NS; s++) {
         const int orient = species_orient (zs, A.cm[s]);
-        fzb[s] = face_oriented<false> (orient, rm2[s * MARCH_RW + ci], rm1[s * MARCH_RW + ci], r0[s * MARCH_RW + ci],
-                                       rp1[s * MARCH_RW + ci], A.cm[s] * ez_prev, A.ddz[s] * lsc);
+        fzb[s] = face_oriented<false> (orient, rm2[s * MARCH_AS + ci], rm1[s * MARCH_AS + ci], r0[s * MARCH_AS + ci],
+                                       rp1[s * MARCH_AS + ci], A.cm[s] * ez_prev, A.ddz[s] * lsc);
       }
     }
     // stage 2: n0 of the first row in flight
@@ -286,8 +289,8 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
           n0n[s] = (out_lane && k + 1 < zb + zlen) ? n0p[s][(long long) (k + 1) * pitch] : 0.0;
         }
       }
-      const double ez_k = r0[(NS + 1) * MARCH_RW + ci];
-      const double er_l = r0[NS * MARCH_RW + ci - 1];
+      const double ez_k = r0[(NS + 1) * MARCH_AS + ci];
+      const double er_l = r0[NS * MARCH_AS + ci - 1];
       const int zs = field_sign1 (ez_k);
       const int rs = field_sign1 (er_l);
       double acc[NS];
@@ -296,7 +299,7 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       if (A.nreact > 0) {
         double eabs;
         if (etz) {
-          const double er_c = r0[NS * MARCH_RW + ci];
+          const double er_c = r0[NS * MARCH_AS + ci];
           const double e_r = 0.5 * (er_c + er_l);                 // cdr.c:681-682
           const double e_z = 0.5 * (ez_k + ez_prev);              // cdr.c:683-684
           eabs = sqrt (__fma_rn (e_r, e_r, e_z * e_z));           // cdr.c:691-692
@@ -309,7 +312,7 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
           double rate = rate_lookup (A.nodes + A.r_node0[r], A.r_steps[r], A.r_emin_f[r], A.r_inv_f[r], eabs);
           const int nin = A.r_nin[r];
 #pragma unroll 1
-          for (int i = 0; i < nin; i++) rate *= fabs (r0[A.r_in[r][i] * MARCH_RW + ci]);
+          for (int i = 0; i < nin; i++) rate *= fabs (r0[A.r_in[r][i] * MARCH_AS + ci]);
           rate = zin ? rate : 0.0;
 #pragma unroll
           for (int s = 0; s < NS; s++) acc[s] = __fma_rn (A.r_coef[r][s], rate, acc[s]);
@@ -318,12 +321,12 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       double chg = 0.0;
 #pragma unroll
       for (int s = 0; s < NS; s++) {
-        const double *q = r0 + s * MARCH_RW + ci;
+        const double *q = r0 + s * MARCH_AS + ci;
         const double nC = q[0];
         const double cm = A.cm[s];
         // axial face above row k (.f90:310-386)
-        const double fz = face_oriented<false> (species_orient (zs, cm), rm1[s * MARCH_RW + ci], nC,
-                                                rp1[s * MARCH_RW + ci], rp2[s * MARCH_RW + ci], cm * ez_k, A.ddz[s] * lsc);
+        const double fz = face_oriented<false> (species_orient (zs, cm), rm1[s * MARCH_AS + ci], nC,
+                                                rp1[s * MARCH_AS + ci], rp2[s * MARCH_AS + ci], cm * ez_k, A.ddz[s] * lsc);
         // radial face left of the column (.f90:233-308)
         const double fl = face_oriented<true> (species_orient (rs, cm), q[-2], q[-1], nC, q[1], cm * er_l, A.ddr[s] * lsc);
         const double fr = __shfl_down_sync (0xffffffffu, fl, 1);
