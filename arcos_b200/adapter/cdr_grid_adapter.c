@@ -256,8 +256,28 @@ ensure_context (cdr_grid_t *root)
   g_key = key;
 }
 
-/* g_inter: the same for the intermediate tree (cdr_like_a copies the
- * shape and the child order). */
+/* The intermediate tree of cdr_rk2: a grid like every grid of the tree,
+ * linked in the same child order, as cdr_like_update_ar (src/cdr.c:1184-1208)
+ * builds it (cdr_like_a itself copies one grid, not its children). */
+static cdr_grid_t *
+like_tree (cdr_grid_t *grid)
+{
+  cdr_grid_t *n = cdr_like_a (grid), *child, *prev = NULL;
+  iter_childs (grid, child) {
+    cdr_grid_t *nc = like_tree (child);
+    if (NULL == prev) n->first_child = nc;
+    else prev->next = nc;
+    nc->parent = n;
+    nc->next = NULL;
+    nc->level = n->level + 1;
+    grid_inherit_ext_bound ((grid_t *) nc);
+    prev = nc;
+  }
+  return n;
+}
+
+/* g_inter: the same for the intermediate tree (like_tree copies the shape
+ * and the child order). */
 static void
 list_like (cdr_grid_t *like)
 {
@@ -336,7 +356,7 @@ cdr_rk2 (cdr_grid_t *grid, double h, double t)
     if (0 == count_min_timestep--) fatal ("Too many warnings about small timesteps.\n");
   }
 
-  inter = cdr_like_a (grid);
+  inter = like_tree (grid);
   list_like (inter);
   check (arcos_cdr_update (g_ctx, h), "cdr_like_update_ar");
   check (arcos_prepare_grid (g_ctx, ARCOS_SET_INTER), "prepare_grid (inter)");

@@ -48,15 +48,15 @@ def autotune_tiles(tree, steps: int = 6, h: float = 50.0, stream=None) -> Dict[i
     return times
 
 
-TREE_SHAPES = (2, 3, 4, 5)   # 2: the general tree step (k_stage tiles); 3-5: the lean batched step
+TREE_SHAPES = (0, 1, 2, 3, 4, 5)   # the lean batched step: tiled k_fused (0-2) or k_march (3-5)
 
 
 def autotune_tree(tree, steps: int = 4, h: float = 50.0, stream=None,
                   shapes=TREE_SHAPES) -> Dict[int, float]:
     """Times ``steps`` batched steps of a refinement tree (arcos_run, one
-    CUDA graph per step) per shape and selects the fastest.  Shape 2 runs
-    the general tree step, shapes 3-5 the lean one (k_march with segments
-    of 16, 32, 64 rows).  Returns {shape: ms per step}; the state advances."""
+    CUDA graph per step) per shape and selects the fastest.  Shapes 0-2 run
+    the lean step with the tiled fused kernel, 3-5 with k_march (segments of
+    16, 32, 64 rows).  Returns {shape: ms per step}; the state advances."""
     import torch
 
     s = stream if stream is not None else torch.cuda.current_stream()

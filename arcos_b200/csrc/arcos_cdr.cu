@@ -129,7 +129,9 @@ struct Ctx {
   cudaGraphExec_t graph2 = nullptr;   // two fused steps
   cudaGraphExec_t graph_tree = nullptr;   // one step of a tree (batched launches)
   int graph_items = -1;
-  double *colfac_d = nullptr;         // fused kernels: per column ir/((ir+1/2)dr), (ir+1)/((ir+1/2)dr)
+  double *colfac_d = nullptr;         // fused kernels: per level, per absolute column ir:
+                                      // ir/((ir+1/2)dr), (ir+1)/((ir+1/2)dr)
+  std::vector<int> colfac_off;        // first column entry of each level
   TableNode *lean_nodes_d = nullptr;  // fused kernels: nodes with under/overflow sentinels
   bool lean_tables = false;           // every table's position estimate is within one node
   // discrete adjoint (adjoint_kernel.cuh): per patch a block of work arrays
@@ -293,15 +295,15 @@ launch_march (int ns, bool s2, bool tree, const Model &M, const FusedArgs &A, in
 
 template <bool S2>
 cudaError_t
-launch_fused_m (int ns, int cfg, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
+launch_fused_m (int ns, bool tree, int cfg, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
 {
   switch (ns) {
-  case 1: return launch_fused_ns<1> (S2, cfg, M, A, blocks, s, occ);
-  case 2: return launch_fused_ns<2> (S2, cfg, M, A, blocks, s, occ);
-  case 3: return launch_fused_ns<3> (S2, cfg, M, A, blocks, s, occ);
-  case 4: return launch_fused_ns<4> (S2, cfg, M, A, blocks, s, occ);
-  case 5: return launch_fused_ns<5> (S2, cfg, M, A, blocks, s, occ);
-  case 6: return launch_fused_ns<6> (S2, cfg, M, A, blocks, s, occ);
+  case 1: return launch_fused_ns<1> (S2, tree, cfg, M, A, blocks, s, occ);
+  case 2: return launch_fused_ns<2> (S2, tree, cfg, M, A, blocks, s, occ);
+  case 3: return launch_fused_ns<3> (S2, tree, cfg, M, A, blocks, s, occ);
+  case 4: return launch_fused_ns<4> (S2, tree, cfg, M, A, blocks, s, occ);
+  case 5: return launch_fused_ns<5> (S2, tree, cfg, M, A, blocks, s, occ);
+  case 6: return launch_fused_ns<6> (S2, tree, cfg, M, A, blocks, s, occ);
   default: return cudaErrorInvalidValue;
   }
 }
@@ -403,6 +405,7 @@ fused_args (Ctx *c)
   A.rmaps = c->rmaps_d;
   A.rmaps_per_patch = c->maps_per_patch;
   A.colfac = c->colfac_d;
+  for (int l = 0; l < ARCOS_MAXLEVELS; l++) A.colfac_level[l] = l < (int) c->colfac_off.size () ? c->colfac_off[l] : 0;
   // reaction program: node 0 of reaction r sits after r + 1 sentinels
   const Model &M = c->M;
   A.nreact = M.nreact;
@@ -449,17 +452,18 @@ run_fused (Ctx *c, bool s2, int fold, int fam_state = 1, int frozen_k = -1)
     return ARCOS_OK;
   }
   const int cfg = stage_cfg (c);
+  const bool tree = !c->fused_ok;       // ghosts from memory (prepare_grid), per-level factors
   int &o = c->occ_fused[c->stage_eabs][s2 ? 1 : 0][cfg];
   if (o == 0) {
     int b = 0;
-    if (s2) launch_fused_m<true> (c->M.ns, cfg, c->M, A, 0, 0, &b);
-    else launch_fused_m<false> (c->M.ns, cfg, c->M, A, 0, 0, &b);
+    if (s2) launch_fused_m<true> (c->M.ns, tree, cfg, c->M, A, 0, 0, &b);
+    else launch_fused_m<false> (c->M.ns, tree, cfg, c->M, A, 0, 0, &b);
     o = b > 0 ? b : 1;
   }
   const int blocks = std::min (c->n_items, c->num_sms * o);
   if (blocks <= 0) return ARCOS_OK;
-  cudaError_t e = s2 ? launch_fused_m<true> (c->M.ns, cfg, c->M, A, blocks, c->stream, nullptr)
-                     : launch_fused_m<false> (c->M.ns, cfg, c->M, A, blocks, c->stream, nullptr);
+  cudaError_t e = s2 ? launch_fused_m<true> (c->M.ns, tree, cfg, c->M, A, blocks, c->stream, nullptr)
+                     : launch_fused_m<false> (c->M.ns, tree, cfg, c->M, A, blocks, c->stream, nullptr);
   if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("fused launch: ") + cudaGetErrorString (e));
   return ARCOS_OK;
 }
@@ -870,8 +874,9 @@ rk2_inloop_step (Ctx *c)
 bool
 lean_tree_ok (Ctx *c)
 {
-  return !c->fused_ok && march_on (c) && c->lean_tables && !c->exact && c->use_tma && c->lean_nodes_d
-         && !inloop (c) && !c->per_patch && (c->p.per_plane || c->p.max_ntheta == 1);
+  return !c->fused_ok && (c->tile_cfg < N_TILE_CFG ? c->maps_d != nullptr : march_on (c)) && c->lean_tables
+         && !c->exact && c->use_tma && c->lean_nodes_d && c->colfac_d && !inloop (c) && !c->per_patch
+         && (c->p.per_plane || c->p.max_ntheta == 1);
 }
 
 int
@@ -1080,7 +1085,7 @@ run_vjp (Ctx *c, int mode, int st_idx, int lam_idx, int lams_idx, int out_idx, i
   A.g_table = c->adj_gtab_d;
   A.n_nodes = (int) c->nodes_h.size ();
   A.g_part = c->adj_gpart_d;
-  A.colfac = c->colfac_d;
+  A.colfac = c->colfac_d;                // level 0 (single-grid families) starts at entry 0
   const double dr = c->dr[0], dz = c->dz[0], D = c->p.diffusion_coeff;
   for (int s = 0; s < c->M.ns; s++) {
     const double mass = c->M.mass[s];
@@ -1265,6 +1270,8 @@ arcos_create (const arcos_params *p, void **out)
   if (p->no_species < 1 || p->no_species > 6)
     return fail (ARCOS_ERR_ARG, "no_species must be 1..6 for the device kernels");
   if (p->max_ntheta < 1 || p->max_ntheta > 64) return fail (ARCOS_ERR_ARG, "max_ntheta must be 1..64");
+  if (p->max_levels < 0 || p->max_levels >= ARCOS_MAXLEVELS)
+    return fail (ARCOS_ERR_ARG, "max_levels must be 0..15");
   Ctx *c = new Ctx ();
   c->p = *p;
   Model &M = c->M;
@@ -1833,17 +1840,22 @@ arcos_commit (void *ctx)
   for (int i = 0; i < np; i++)
     if (c->g[i].parent >= 0 || c->g[i].ext_bound != 15 || c->g[i].r0 != 0 || c->pd_h[i].level != 0)
       c->fused_ok = false;
-  if (c->fused_ok) {
-    // radial divergence factors of every column of the root level (.f90:408-412),
-    // padded to whole 32-column tiles
-    int maxnr = 0;
-    for (auto &P : c->pd_h) maxnr = std::max (maxnr, P.nr);
-    const int ncol = (maxnr + 31) / 32 * 32 + 32;
-    std::vector<double> cf (2 * (size_t) ncol);
-    for (int ir = 0; ir < ncol; ir++) {
-      const double r_inv = 1.0 / (((double) ir + 0.5) * c->dr[0]);
-      cf[2 * ir] = (double) ir * r_inv;
-      cf[2 * ir + 1] = (double) (ir + 1) * r_inv;
+  {
+    // radial divergence factors of every absolute column of every level
+    // (.f90:408-412), each level padded past its last patch by whole 32-column tiles
+    std::vector<double> cf;
+    c->colfac_off.assign (c->max_level + 1, 0);
+    for (int l = 0; l <= c->max_level; l++) {
+      int maxr = 0;
+      for (auto &P : c->pd_h)
+        if (P.level == l) maxr = std::max (maxr, P.r0 + P.nr);
+      const int ncol = (maxr + 31) / 32 * 32 + 32;
+      c->colfac_off[l] = (int) (cf.size () / 2);
+      for (int ir = 0; ir < ncol; ir++) {
+        const double r_inv = 1.0 / (((double) ir + 0.5) * c->dr[l]);
+        cf.push_back ((double) ir * r_inv);
+        cf.push_back ((double) (ir + 1) * r_inv);
+      }
     }
     CK (cudaMalloc (&c->colfac_d, sizeof (double) * cf.size ()));
     CK (cudaMemcpy (c->colfac_d, cf.data (), sizeof (double) * cf.size (), cudaMemcpyHostToDevice));

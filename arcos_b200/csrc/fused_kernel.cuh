@@ -55,7 +55,8 @@ struct FusedArgs {
   int n_units;
   const CUtensorMap *rmaps;  // k_march: one-row boxes [patch][set][array]
   int rmaps_per_patch;
-  const double *colfac;      // per column ir: ir / ((ir + 1/2) dr), (ir + 1) / ((ir + 1/2) dr)
+  const double *colfac;      // per level, per absolute column ir: ir / ((ir + 1/2) dr), (ir + 1) / ((ir + 1/2) dr)
+  int colfac_level[ARCOS_MAXLEVELS];   // first entry of each level in colfac
   double cm[FUSED_MAXS];     // charge / mass (0 for immobile species: zero flux) (.f90:90)
   double ddr[FUSED_MAXS];    // (diffusion_coeff / mass) / dr (.f90:85,174)
   double ddz[FUSED_MAXS];    // (diffusion_coeff / mass) / dz (.f90:85,224)
@@ -97,6 +98,9 @@ struct TileInfo {
   int nr, nz, nt, pitch, c0, zb, width, zlen, plane, patch, fam, level, etz, edge;
   int z0zb;                  // absolute index of the tile's first row (z cutoff)
   int clamp;                 // stage 1: the state may hold negatives (cdr_nonegative has work)
+  int cf0;                   // colfac entry of the patch's column 0 (level table + r0)
+  double lsc;                // 2^level: D/dr, D/dz and 1/dz of the level are the root's times lsc
+  double dz;                 // dz of the level (z cutoff)
 };
 
 __device__ __forceinline__ double
@@ -191,7 +195,7 @@ rate_lookup (const TableNode *__restrict__ nd, int steps, float emin_f, float in
 }
 
 // Issues the bulk tensor copies of one tile and fills its TileInfo (thread 0).
-template <int NS, bool S2, int TY>
+template <int NS, bool S2, int TY, bool TREE>
 __device__ __forceinline__ void
 fused_issue (const FusedArgs &A, int item, double *buf, int plane_doubles, unsigned long long *bar,
              TileInfo<NS> *ti)
@@ -223,14 +227,18 @@ fused_issue (const FusedArgs &A, int item, double *buf, int plane_doubles, unsig
   ti->nr = P.nr; ti->nz = P.nz; ti->nt = P.ntheta; ti->pitch = P.pitch;
   ti->c0 = w.c0; ti->zb = w.zb; ti->width = w.width; ti->zlen = w.zlen; ti->plane = w.plane;
   ti->patch = w.patch; ti->fam = P.fam; ti->level = P.level; ti->etz = etz;
-  ti->edge = (w.c0 == 0) || (w.c0 + 34 > P.nr) || (w.zb == 0) || (w.zb + TY + 2 > P.nz);
+  // trees: every ghost cell was set in memory by prepare_grid, the state clamped by cdr_nonegative_r
+  ti->edge = !TREE && ((w.c0 == 0) || (w.c0 + 34 > P.nr) || (w.zb == 0) || (w.zb + TY + 2 > P.nz));
   ti->z0zb = P.z0 + w.zb;
   // max(0, n) is the identity on a state without negatives (stage 2 of the
   // previous step records whether it wrote any); frozen steps always clamp
-  ti->clamp = A.h_seq ? 1 : (int) A.st[P.fam].neg[A.st[P.fam].step & 1];
+  ti->clamp = TREE ? 0 : (A.h_seq ? 1 : (int) A.st[P.fam].neg[A.st[P.fam].step & 1]);
+  ti->cf0 = A.colfac_level[P.level] + P.r0;
+  ti->lsc = (double) (1 << P.level);
+  ti->dz = P.dz;
 }
 
-template <int NS, bool S2, int WY, int RPW>
+template <int NS, bool S2, int WY, int RPW, bool TREE>
 __global__ void __launch_bounds__ (32 * WY)
 k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
 {
@@ -250,7 +258,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
   if (t == 0) {
     mbar_init (&bar[0], 1);
     mbar_init (&bar[1], 1);
-    if ((int) blockIdx.x < A.n_items) fused_issue<NS, S2, TY> (A, blockIdx.x, buf0, PL, &bar[0], &tinfo[0]);
+    if ((int) blockIdx.x < A.n_items) fused_issue<NS, S2, TY, TREE> (A, blockIdx.x, buf0, PL, &bar[0], &tinfo[0]);
   }
   __syncthreads ();
 
@@ -305,7 +313,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
     const bool otf = edge || (!S2 && T.clamp);
     if (!otf && t == 0 && item + (int) gridDim.x < A.n_items)
       // every thread is past the previous tile: its buffer is free
-      fused_issue<NS, S2, TY> (A, item + gridDim.x, (it & 1) ? buf0 : buf1, PL, &bar[(it + 1) & 1],
+      fused_issue<NS, S2, TY, TREE> (A, item + gridDim.x, (it & 1) ? buf0 : buf1, PL, &bar[(it + 1) & 1],
                                &tinfo[(it + 1) & 1]);
 
     // ---- stencil values: clamp n0 (stage 1), ghost cells from the boundary
@@ -370,7 +378,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       __syncthreads ();
       // the other buffer is free (every thread is past the previous tile)
       if (t == 0 && item + (int) gridDim.x < A.n_items)
-        fused_issue<NS, S2, TY> (A, item + gridDim.x, (it & 1) ? buf0 : buf1, PL, &bar[(it + 1) & 1],
+        fused_issue<NS, S2, TY, TREE> (A, item + gridDim.x, (it & 1) ? buf0 : buf1, PL, &bar[(it + 1) & 1],
                                  &tinfo[(it + 1) & 1]);
     }
 
@@ -407,7 +415,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
 #pragma unroll
       for (int j = 0; j <= RPW; j++) vz[j] = A.cm[s] * ezw[j];
       const int orient = species_orient (zsigns, A.cm[s]);
-      const double dd = A.ddz[s];
+      const double dd = A.ddz[s] * T.lsc;
       if (orient == 1) {
 #pragma unroll
         for (int k = 0; k < RPW; k++) fzt[k][s] = face_o<false, true> (nw[k + 1], nw[k + 2], nw[k + 3], vz[k + 1], dd);
@@ -428,7 +436,8 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
     for (int i = lane; i < RPW * NS; i += 32) {
       const int row = r_first + i % RPW, s = i / RPW;
       const double *q = sm + s * PL + (row + 2) * TXP;
-      rb[s][row] = face_any<true> (0, q[32], q[33], q[34], q[35], A.cm[s] * sm[NS * PL + (row + 2) * TXP + 33], A.ddr[s]);
+      rb[s][row] = face_any<true> (0, q[32], q[33], q[34], q[35], A.cm[s] * sm[NS * PL + (row + 2) * TXP + 33],
+                                   A.ddr[s] * T.lsc);
     }
 #pragma unroll
     for (int k = 0; k < RPW; k++)
@@ -447,7 +456,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
         }
       }
       // z_cutoff gate (reaction.c:121): only a tile reaching it tests its rows
-      const bool gate = ((double) (T.z0zb + TY) + 0.5) * A.dz >= M.z_cutoff;
+      const bool gate = ((double) (T.z0zb + TY) + 0.5) * T.dz >= M.z_cutoff;
 #pragma unroll 1
       for (int r = 0; r < A.nreact; r++) {
         const TableNode *nd = nodes + A.r_node0[r];
@@ -466,7 +475,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
         if (gate) {
 #pragma unroll
           for (int k = 0; k < RPW; k++)
-            if (!(((double) (T.z0zb + r_first + k) + 0.5) * A.dz < M.z_cutoff)) rate[k] = 0.0;
+            if (!(((double) (T.z0zb + r_first + k) + 0.5) * T.dz < M.z_cutoff)) rate[k] = 0.0;
         }
 #pragma unroll
         for (int s = 0; s < NS; s++) {
@@ -484,7 +493,8 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       for (int s = 0; s < NS; s++) fzb[s] = zt[wq - 1][s][lane];
     }
     const int c = c0 + lane;
-    const double erm = A.colfac[2 * c], erp = A.colfac[2 * c + 1];   // .f90:408-412
+    const double erm = A.colfac[2 * (T.cf0 + c)], erp = A.colfac[2 * (T.cf0 + c) + 1];   // .f90:408-412
+    const double gdz = A.gdz * T.lsc;
     const bool last = lane == 31;
     const double h = T.h, hh = 0.5 * h;
     double erl[RPW];
@@ -512,7 +522,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
 #pragma unroll
       for (int k = 0; k < RPW; k++) vr[k] = A.cm[s] * erl[k];
       const int orient = species_orient (rsigns, A.cm[s]);
-      const double dd = A.ddr[s];
+      const double dd = A.ddr[s] * T.lsc;
       double *outp = T.out[s] + ro;
       const bool mob = M.mobile[s];
 #pragma unroll
@@ -529,7 +539,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
         double dv = acc[k][s];
         dv = __fma_rn (erm, fl, dv);                           // .f90:113-117
         dv = __fma_rn (-erp, fr, dv);
-        dv = __fma_rn (A.gdz, fd - fzt[k][s], dv);             // .f90:128-130
+        dv = __fma_rn (gdz, fd - fzt[k][s], dv);               // .f90:128-130
         const bool wr = active && r_first + k < T.zlen;
         if (!S2) {
           if (wr) outp[(long long) k * pitch] = __fma_rn (h, dv, nC);

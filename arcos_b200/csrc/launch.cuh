@@ -33,7 +33,7 @@ template <int NS>
 cudaError_t launch_stage_ns (int mode, int cfg, const Model &M, const StageArgs &A, int blocks,
                              cudaStream_t s, int *occ);
 template <int NS>
-cudaError_t launch_fused_ns (bool s2, int cfg, const Model &M, const FusedArgs &A, int blocks,
+cudaError_t launch_fused_ns (bool s2, bool tree, int cfg, const Model &M, const FusedArgs &A, int blocks,
                              cudaStream_t s, int *occ);
 template <int NS>
 cudaError_t launch_march_ns (bool s2, bool tree, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s);
@@ -44,8 +44,8 @@ cudaError_t launch_vjp_ns (const Model &M, const VjpArgs &A, int blocks, size_t 
 #define ARCOS_DECLARE_NS(N)                                                                          \
   extern template cudaError_t launch_stage_ns<N> (int, int, const Model &, const StageArgs &, int,   \
                                                   cudaStream_t, int *);                              \
-  extern template cudaError_t launch_fused_ns<N> (bool, int, const Model &, const FusedArgs &, int,  \
-                                                  cudaStream_t, int *);                              \
+  extern template cudaError_t launch_fused_ns<N> (bool, bool, int, const Model &, const FusedArgs &,  \
+                                                  int, cudaStream_t, int *);                         \
   extern template cudaError_t launch_vjp_ns<N> (const Model &, const VjpArgs &, int, size_t,         \
                                                 cudaStream_t, int *);                                \
   extern template cudaError_t launch_march_ns<N> (bool, bool, const Model &, const FusedArgs &, int, \

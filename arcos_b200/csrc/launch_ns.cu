@@ -60,37 +60,41 @@ launch_stage_ns (int mode, int cfg, const Model &M, const StageArgs &A, int bloc
   }
 }
 
-template <int NS, bool S2, int WY, int RPW>
+template <int NS, bool S2, int WY, int RPW, bool TREE>
 cudaError_t
 launch_fused_t (const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
 {
   const size_t sm = sizeof (double) * 2 * fused_buffer_doubles<NS, WY, RPW> (A.stage_eabs);
-  cudaFuncSetAttribute (k_fused<NS, S2, WY, RPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+  cudaFuncSetAttribute (k_fused<NS, S2, WY, RPW, TREE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
   if (occ) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor (occ, k_fused<NS, S2, WY, RPW>, 32 * WY, sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor (occ, k_fused<NS, S2, WY, RPW, TREE>, 32 * WY, sm);
     return cudaGetLastError ();
   }
-  k_fused<NS, S2, WY, RPW><<<blocks, 32 * WY, sm, s>>> (M, A);
+  k_fused<NS, S2, WY, RPW, TREE><<<blocks, 32 * WY, sm, s>>> (M, A);
   return cudaGetLastError ();
 }
 
-template <int NS, bool S2>
+template <int NS, bool S2, bool TREE>
 cudaError_t
 launch_fused_c (int cfg, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
 {
   switch (cfg) {
-  case 0: return launch_fused_t<NS, S2, 4, 4> (M, A, blocks, s, occ);
-  case 1: return launch_fused_t<NS, S2, 8, 4> (M, A, blocks, s, occ);
-  default: return launch_fused_t<NS, S2, 8, 2> (M, A, blocks, s, occ);
+  case 0: return launch_fused_t<NS, S2, 4, 4, TREE> (M, A, blocks, s, occ);
+  case 1: return launch_fused_t<NS, S2, 8, 4, TREE> (M, A, blocks, s, occ);
+  default: return launch_fused_t<NS, S2, 8, 2, TREE> (M, A, blocks, s, occ);
   }
 }
 
 template <int NS>
 cudaError_t
-launch_fused_ns (bool s2, int cfg, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s, int *occ)
+launch_fused_ns (bool s2, bool tree, int cfg, const Model &M, const FusedArgs &A, int blocks, cudaStream_t s,
+                 int *occ)
 {
-  return s2 ? launch_fused_c<NS, true> (cfg, M, A, blocks, s, occ)
-            : launch_fused_c<NS, false> (cfg, M, A, blocks, s, occ);
+  if (tree)
+    return s2 ? launch_fused_c<NS, true, true> (cfg, M, A, blocks, s, occ)
+              : launch_fused_c<NS, false, true> (cfg, M, A, blocks, s, occ);
+  return s2 ? launch_fused_c<NS, true, false> (cfg, M, A, blocks, s, occ)
+            : launch_fused_c<NS, false, false> (cfg, M, A, blocks, s, occ);
 }
 
 template <int NS>
@@ -126,7 +130,7 @@ launch_march_ns (bool s2, bool tree, const Model &M, const FusedArgs &A, int blo
 
 template cudaError_t launch_march_ns<ARCOS_NS> (bool, bool, const Model &, const FusedArgs &, int, cudaStream_t);
 template cudaError_t launch_stage_ns<ARCOS_NS> (int, int, const Model &, const StageArgs &, int, cudaStream_t, int *);
-template cudaError_t launch_fused_ns<ARCOS_NS> (bool, int, const Model &, const FusedArgs &, int, cudaStream_t, int *);
+template cudaError_t launch_fused_ns<ARCOS_NS> (bool, bool, int, const Model &, const FusedArgs &, int, cudaStream_t, int *);
 template cudaError_t launch_vjp_ns<ARCOS_NS> (const Model &, const VjpArgs &, int, size_t, cudaStream_t, int *);
 
 }  // namespace arcos

@@ -18,7 +18,7 @@
 // stencil arrays (the densities, er, ez: columns c0-2 .. c0+33, even-aligned)
 // arrives in a ring of MR rows in the warp's own shared memory by one bulk
 // tensor copy per array (cp.async.bulk.tensor, one mbarrier per ring slot,
-// bounded waits), issued MR - 4 rows ahead of use.  Row k needs rows
+// bounded waits), issued three to four rows ahead of use.  Row k needs rows
 // k-1 .. k+2 at its own column (the axial face above it; the face below is
 // the previous row's, kept in a register) and columns c-2 .. c+1 of row k
 // (the radial face).  Ghost cells come from the boundary conditions, written
@@ -123,7 +123,10 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
     const int X0 = c0 & ~1, sh = c0 - X0;          // TMA x must be even (16-byte rows)
     const int ci = lane + 2 + sh;                   // ring index of this lane's column
     const int c = c0 + lane;
-    const int total = zlen + 4;                     // stream rows zb-2 .. zb+zlen+1
+    // rows are computed in pairs; an odd segment (only at the top of a grid)
+    // computes one extra row whose results are not written
+    const int zl2 = zlen + (zlen & 1);
+    const int total = zl2 + 4;                      // stream rows zb-2 .. zb+zl2+1
     const int fam = P->fam;
     const bool etz = A.etz[U.patch * 2 + fset] == 0;
     const double h = A.h_seq ? A.h_seq[(size_t) fam * A.h_stride + A.h_k] : A.st[fam].h;
@@ -254,11 +257,14 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
                                        rp1[s * MARCH_AS + ci], A.cm[s] * ez_prev, A.ddz[s] * lsc);
       }
     }
-    // stage 2: n0 of the first row in flight
-    double n0n[S2 ? NS : 1];
+    // stage 2: n0 of the first two rows in flight
+    double n0a[S2 ? NS : 1], n0b[S2 ? NS : 1];
     if (S2) {
 #pragma unroll
-      for (int s = 0; s < NS; s++) n0n[s] = out_lane ? n0p[s][(long long) zb * pitch] : 0.0;
+      for (int s = 0; s < NS; s++) {
+        n0a[s] = out_lane ? n0p[s][(long long) zb * pitch] : 0.0;
+        n0b[s] = (out_lane && zb + 1 < zb + zlen) ? n0p[s][(long long) (zb + 1) * pitch] : 0.0;
+      }
     }
     __syncwarp ();
     if (!failed && MARCH_R < total) {              // row zb-2's slot is free
@@ -269,95 +275,127 @@ k_march (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       nissued++;
     }
 
-    // ---- march ----
-    for (int k = zb; k < zb + zlen && !failed; k++) {
-      const int j = k + 2;
-      {
-        const bool okr = wait_row (j);
-        if (!__all_sync (0xffffffffu, okr)) { failed = true; break; }
-        nwaited++;
+    // one row's reaction source at this lane's cell (react_apply, reaction.c:110-156)
+    auto reactions = [&] (int k, const double *rk, double ez_k, double ez_km1, double er_l, double (&acc)[NS]) {
+#pragma unroll
+      for (int s = 0; s < NS; s++) acc[s] = 0.0;
+      if (A.nreact == 0) return;
+      double eabs;
+      if (etz) {
+        const double er_c = rk[NS * MARCH_AS + ci];
+        const double e_r = 0.5 * (er_c + er_l);                   // cdr.c:681-682
+        const double e_z = 0.5 * (ez_k + ez_km1);                 // cdr.c:683-684
+        eabs = sqrt (__fma_rn (e_r, e_r, e_z * e_z));             // cdr.c:691-692
+      } else {
+        eabs = (out_lane && k < zb + zlen) ? fabs (eabsp[(long long) k * pitch]) : 1.0;
       }
-      prep_row (j);
-      if (!TREE && j >= nz) mirror_row (j);
-      const double *rm1 = rowp (k - 1), *r0 = rowp (k), *rp1 = rowp (k + 1), *rp2 = rowp (k + 2);
-      double n0c[S2 ? NS : 1];
+      const bool zin = !gate || (((double) (P->z0 + k) + 0.5) * P->dz < M.z_cutoff);   // reaction.c:121
+#pragma unroll 1
+      for (int r = 0; r < A.nreact; r++) {
+        double rate = rate_lookup (A.nodes + A.r_node0[r], A.r_steps[r], A.r_emin_f[r], A.r_inv_f[r], eabs);
+        const int nin = A.r_nin[r];
+#pragma unroll 1
+        for (int i = 0; i < nin; i++) rate *= fabs (rk[A.r_in[r][i] * MARCH_AS + ci]);
+        rate = zin ? rate : 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; s++) acc[s] = __fma_rn (A.r_coef[r][s], rate, acc[s]);
+      }
+    };
+
+    // ---- march, two rows (a = k, b = k + 1) per pass ----
+    for (int k = zb; k < zb + zl2 && !failed; k += 2) {
+      {
+        const bool okr = wait_row (k + 2) && wait_row (k + 3);
+        if (!__all_sync (0xffffffffu, okr)) { failed = true; break; }
+        nwaited += 2;
+      }
+      prep_row (k + 2);
+      prep_row (k + 3);
+      if (!TREE) {
+        if (k + 2 >= nz && k + 2 <= nz + 1) mirror_row (k + 2);
+        if (k + 3 >= nz && k + 3 <= nz + 1) mirror_row (k + 3);
+      }
+      const bool wa = out_lane && k < zb + zlen, wb = out_lane && k + 1 < zb + zlen;
+      const double *rm1 = rowp (k - 1), *r0 = rowp (k), *rp1 = rowp (k + 1), *rp2 = rowp (k + 2),
+                   *rp3 = rowp (k + 3);
+      double n0ca[S2 ? NS : 1], n0cb[S2 ? NS : 1];
       if (S2) {
 #pragma unroll
         for (int s = 0; s < NS; s++) {
-          n0c[s] = clamp0 (n0n[s]);
-          // the next row's n0, one row ahead
-          n0n[s] = (out_lane && k + 1 < zb + zlen) ? n0p[s][(long long) (k + 1) * pitch] : 0.0;
+          n0ca[s] = clamp0 (n0a[s]);
+          n0cb[s] = clamp0 (n0b[s]);
+          // the next pair's n0, one pass ahead
+          n0a[s] = (out_lane && k + 2 < zb + zlen) ? n0p[s][(long long) (k + 2) * pitch] : 0.0;
+          n0b[s] = (out_lane && k + 3 < zb + zlen) ? n0p[s][(long long) (k + 3) * pitch] : 0.0;
         }
       }
-      const double ez_k = r0[(NS + 1) * MARCH_AS + ci];
-      const double er_l = r0[NS * MARCH_AS + ci - 1];
-      const int zs = field_sign1 (ez_k);
-      const int rs = field_sign1 (er_l);
-      double acc[NS];
-#pragma unroll
-      for (int s = 0; s < NS; s++) acc[s] = 0.0;
-      if (A.nreact > 0) {
-        double eabs;
-        if (etz) {
-          const double er_c = r0[NS * MARCH_AS + ci];
-          const double e_r = 0.5 * (er_c + er_l);                 // cdr.c:681-682
-          const double e_z = 0.5 * (ez_k + ez_prev);              // cdr.c:683-684
-          eabs = sqrt (__fma_rn (e_r, e_r, e_z * e_z));           // cdr.c:691-692
-        } else {
-          eabs = out_lane ? fabs (eabsp[(long long) k * pitch]) : 1.0;
-        }
-        const bool zin = !gate || (((double) (P->z0 + k) + 0.5) * P->dz < M.z_cutoff);   // reaction.c:121
-#pragma unroll 1
-        for (int r = 0; r < A.nreact; r++) {
-          double rate = rate_lookup (A.nodes + A.r_node0[r], A.r_steps[r], A.r_emin_f[r], A.r_inv_f[r], eabs);
-          const int nin = A.r_nin[r];
-#pragma unroll 1
-          for (int i = 0; i < nin; i++) rate *= fabs (r0[A.r_in[r][i] * MARCH_AS + ci]);
-          rate = zin ? rate : 0.0;
-#pragma unroll
-          for (int s = 0; s < NS; s++) acc[s] = __fma_rn (A.r_coef[r][s], rate, acc[s]);
-        }
-      }
-      double chg = 0.0;
+      const double ez_a = r0[(NS + 1) * MARCH_AS + ci], ez_b = rp1[(NS + 1) * MARCH_AS + ci];
+      const double er_la = r0[NS * MARCH_AS + ci - 1], er_lb = rp1[NS * MARCH_AS + ci - 1];
+      const double eza2[2] = {ez_a, ez_b}, era2[2] = {er_la, er_lb};
+      const int zs = field_signs (eza2);
+      const int rs = field_signs (era2);
+      double acc_a[NS], acc_b[NS];
+      reactions (k, r0, ez_a, ez_prev, er_la, acc_a);
+      reactions (k + 1, rp1, ez_b, ez_a, er_lb, acc_b);
+      double chg_a = 0.0, chg_b = 0.0;
 #pragma unroll
       for (int s = 0; s < NS; s++) {
-        const double *q = r0 + s * MARCH_AS + ci;
-        const double nC = q[0];
-        const double cm = A.cm[s];
-        // axial face above row k (.f90:310-386)
-        const double fz = face_oriented<false> (species_orient (zs, cm), rm1[s * MARCH_AS + ci], nC,
-                                                rp1[s * MARCH_AS + ci], rp2[s * MARCH_AS + ci], cm * ez_k, A.ddz[s] * lsc);
-        // radial face left of the column (.f90:233-308)
-        const double fl = face_oriented<true> (species_orient (rs, cm), q[-2], q[-1], nC, q[1], cm * er_l, A.ddr[s] * lsc);
-        const double fr = __shfl_down_sync (0xffffffffu, fl, 1);
-        double dv = acc[s];
-        dv = __fma_rn (erm, fl, dv);                               // .f90:113-117
-        dv = __fma_rn (-erp, fr, dv);
-        dv = __fma_rn (gdz, fzb[s] - fz, dv);                      // .f90:128-130
-        fzb[s] = fz;
+        const double *qa = r0 + s * MARCH_AS + ci, *qb = rp1 + s * MARCH_AS + ci;
+        const double nA = qa[0], nB = qb[0];
+        const double cm = A.cm[s], ddz = A.ddz[s] * lsc, ddr = A.ddr[s] * lsc;
+        const int oz = species_orient (zs, cm), orr = species_orient (rs, cm);
+        const double nm1 = rm1[s * MARCH_AS + ci], np2 = rp2[s * MARCH_AS + ci], np3 = rp3[s * MARCH_AS + ci];
+        // axial faces above rows a and b (.f90:310-386)
+        const double fza = face_oriented<false> (oz, nm1, nA, nB, np2, cm * ez_a, ddz);
+        const double fzb2 = face_oriented<false> (oz, nA, nB, np2, np3, cm * ez_b, ddz);
+        // radial faces left of the column (.f90:233-308)
+        const double fla = face_oriented<true> (orr, qa[-2], qa[-1], nA, qa[1], cm * er_la, ddr);
+        const double flb = face_oriented<true> (orr, qb[-2], qb[-1], nB, qb[1], cm * er_lb, ddr);
+        const double fra = __shfl_down_sync (0xffffffffu, fla, 1);
+        const double frb = __shfl_down_sync (0xffffffffu, flb, 1);
+        double dva = acc_a[s], dvb = acc_b[s];
+        dva = __fma_rn (erm, fla, dva);                            // .f90:113-117
+        dvb = __fma_rn (erm, flb, dvb);
+        dva = __fma_rn (-erp, fra, dva);
+        dvb = __fma_rn (-erp, frb, dvb);
+        dva = __fma_rn (gdz, fzb[s] - fza, dva);                   // .f90:128-130
+        dvb = __fma_rn (gdz, fza - fzb2, dvb);
+        fzb[s] = fzb2;
         if (!S2) {
-          if (out_lane) outp[s][(long long) k * pitch] = __fma_rn (h, dv, nC);
+          if (wa) outp[s][(long long) k * pitch] = __fma_rn (h, dva, nA);
+          if (wb) outp[s][(long long) (k + 1) * pitch] = __fma_rn (h, dvb, nB);
         } else {
-          const double n1 = __fma_rn (hh, dv, 0.5 * (n0c[s] + nC));
-          if (out_lane) {
-            outp[s][(long long) k * pitch] = n1;
-            if (A.want_charge) chg += (n1 * M.charge[s]) / nt;     // cdr.c:380-381
-            const double n1c = clamp0 (n1);
-            if (M.mobile[s] && mob_any && n1c > dmax_local) dmax_local = n1c;
-            neg_local = neg_local || n1 < 0.0;
+          const double n1a = __fma_rn (hh, dva, 0.5 * (n0ca[s] + nA));
+          const double n1b = __fma_rn (hh, dvb, 0.5 * (n0cb[s] + nB));
+          if (wa) outp[s][(long long) k * pitch] = n1a;
+          if (wb) outp[s][(long long) (k + 1) * pitch] = n1b;
+          if (A.want_charge) {                                     // cdr.c:380-381
+            chg_a += (n1a * M.charge[s]) / nt;
+            chg_b += (n1b * M.charge[s]) / nt;
           }
+          if (M.mobile[s] && mob_any) {
+            const double ca = wa ? clamp0 (n1a) : -1.0, cb = wb ? clamp0 (n1b) : -1.0;
+            if (ca > dmax_local) dmax_local = ca;
+            if (cb > dmax_local) dmax_local = cb;
+          }
+          neg_local = neg_local || (wa && n1a < 0.0) || (wb && n1b < 0.0);
         }
       }
-      if (S2 && A.want_charge && out_lane) chgp[(long long) k * pitch] = chg;
-      ez_prev = ez_k;
-      // row k-1 is done with: its slot takes the stream row MARCH_R further on
+      if (S2 && A.want_charge) {
+        if (wa) chgp[(long long) k * pitch] = chg_a;
+        if (wb) chgp[(long long) (k + 1) * pitch] = chg_b;
+      }
+      ez_prev = ez_b;
+      // rows k-1 and k are done with: their slots take the stream rows MARCH_R further on
       asm volatile ("fence.proxy.async.shared::cta;\n" ::: "memory");
       __syncwarp ();
       const int inext = (k - 1) - zb + 2 + MARCH_R;
-      if (inext < total) {
-        if (lane == 0) issue (inext);
-        nissued++;
-      }
+#pragma unroll
+      for (int d = 0; d < 2; d++)
+        if (inext + d < total) {
+          if (lane == 0) issue (inext + d);
+          nissued++;
+        }
     }
     if (failed) {
       // let every copy this warp issued land before the ring is abandoned

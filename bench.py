@@ -286,9 +286,9 @@ def _load(tree, pb):
 def extra_amr(stream, steps: int = 10):
     """Batched AMR: 4 levels, 320 patches (sides 16..256) advanced by one
     launch per kernel kind over all patches (one CUDA graph per step), the
-    step form picked by the tree autotuner (the general step with tiled
-    stage kernels, or the lean step with k_march at three segment heights),
-    against one launch per patch, same GPU, same steps."""
+    lean step with its kernel shape picked by the tree autotuner (tiled
+    fused kernel or k_march), against one launch per patch of the general
+    step, same GPU, same steps."""
     import numpy as np
     from arcos_b200 import workloads
     from arcos_b200.autotune import autotune_tree

@@ -102,12 +102,12 @@ def test_amr_tree(cuda_device):
     compare_state(dev, port, pb)
 
 
-@pytest.mark.parametrize("tile", [3, 4, 5])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("field", ["uniform", "wavy"])
 def test_amr_tree_lean_batched_step(cuda_device, tile, field):
-    """The lean batched tree step (k_march over every patch, ghosts from
-    prepare_grid) per step against the oracle at 1e-12; also 3 steps replayed
-    from the step graph in one call."""
+    """The lean batched tree step (the fused stage kernels over every patch,
+    tiled or marching, ghosts from prepare_grid) per step against the oracle
+    at 1e-12; also 3 steps replayed from the step graph in one call."""
     pb = workloads.amr(n_patches=12, levels=3, root_nr=32, root_nz=64, side_lo=8, side_hi=24, seed=2)
     if field == "wavy":
         pb.fields = [workloads.wavy_field(sp, pb.params, seed=50 + g) for g, sp in enumerate(pb.specs)]
