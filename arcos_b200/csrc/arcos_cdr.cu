@@ -49,6 +49,7 @@ fail (int code, const std::string &msg)
   } while (0)
 
 constexpr int N_TILE_CFG_MAX = 3;
+constexpr int NONNEG_CHUNK = 4096;    // elements per block of the flat streaming kernels
 
 struct GridH {
   int r0, z0, r1, z1, ntheta, level, ext_bound, parent, fam;
@@ -95,6 +96,10 @@ struct Ctx {
   CUtensorMap *maps_d = nullptr;      // [patch][set][array]
   int maps_per_patch = 0;
   int *plist_d = nullptr;             // 0..npatch-1
+  int *roots_d = nullptr;             // the level-0 patches (the CFL maxima are the roots')
+  int n_roots = 0;
+  Chunk *chunks_d = nullptr;          // flat chunks of every patch's species arrays
+  int n_chunks = 0;
   std::vector<int> level_off, level_cnt;   // children lists per level inside kids_d
   int *kids_d = nullptr;
   StripDesc *strips_d = nullptr;
@@ -532,6 +537,11 @@ chk_committed (Ctx *c)
 int
 do_nonneg (Ctx *c, int set)
 {
+  if (!c->per_patch && c->chunks_d) {
+    k_nonneg_chunks<<<c->n_chunks, 256, 0, c->stream>>> (c->pd_d, c->chunks_d, set, NONNEG_CHUNK);
+    CKL ();
+    return ARCOS_OK;
+  }
   return for_patches (c, max_patch_work (c), [&] (dim3 g, const int *pl) {
     k_nonneg<<<g, 256, 0, c->stream>>> (c->pd_d, pl, set);
   });
@@ -790,6 +800,12 @@ do_dmax (Ctx *c, int set, int slot_rel)
 {
   long long w = 0;
   for (auto &P : c->pd_h) w = std::max (w, (long long) P.nr * P.nz * P.ntheta);
+  if (!c->per_patch && c->roots_d) {          // cdr_courant reads the roots only (cdr.c:998-1013)
+    k_dmax<<<dim3 (grid_blocks (w, 256, 1024), c->n_roots), 256, 0, c->stream>>> (c->M, c->pd_d, c->roots_d, set,
+                                                                                   c->st_d, slot_rel);
+    CKL ();
+    return ARCOS_OK;
+  }
   return for_patches (c, w, [&] (dim3 g, const int *pl) {
     k_dmax<<<g, 256, 0, c->stream>>> (c->M, c->pd_d, pl, set, c->st_d, slot_rel);
   });
@@ -1324,7 +1340,7 @@ arcos_destroy (void *ctx)
   cudaFree (c->adj_gpart_d); cudaFree (c->adj_invde_d); cudaFree (c->adj_tiles_d);
   cudaFree (c->pool); cudaFree (c->pd_d); cudaFree (c->nodes_d); cudaFree (c->st_d);
   cudaFree (c->dtlog_d); cudaFree (c->etz_d); cudaFree (c->done_d); cudaFree (c->items_d);
-  cudaFree (c->plist_d); cudaFree (c->kids_d); cudaFree (c->strips_d); cudaFree (c->ext_d);
+  cudaFree (c->plist_d); cudaFree (c->roots_d); cudaFree (c->chunks_d); cudaFree (c->kids_d); cudaFree (c->strips_d); cudaFree (c->ext_d);
   for (int s = 0; s < 2; s++) { cudaFree (c->match_src_d[s]); cudaFree (c->match_dst_d[s]); }
   cudaFree (c->match_tmp_d);
   cudaFree (c->xfer_d);
@@ -1701,6 +1717,21 @@ arcos_commit (void *ctx)
   for (int i = 0; i < np; i++) pl[i] = i;
   CK (cudaMalloc (&c->plist_d, sizeof (int) * np));
   CK (cudaMemcpyAsync (c->plist_d, pl.data (), sizeof (int) * np, cudaMemcpyHostToDevice, c->stream));
+  {
+    std::vector<int> roots;
+    std::vector<Chunk> ch;
+    for (int i = 0; i < np; i++) {
+      if (c->pd_h[i].level == 0) roots.push_back (i);
+      const long long n = c->pd_h[i].asz * ns;
+      for (long long st = 0; st < n; st += NONNEG_CHUNK) ch.push_back ({i, (int) st});
+    }
+    c->n_roots = (int) roots.size ();
+    c->n_chunks = (int) ch.size ();
+    CK (cudaMalloc (&c->roots_d, sizeof (int) * roots.size ()));
+    CK (cudaMemcpy (c->roots_d, roots.data (), sizeof (int) * roots.size (), cudaMemcpyHostToDevice));
+    CK (cudaMalloc (&c->chunks_d, sizeof (Chunk) * ch.size ()));
+    CK (cudaMemcpy (c->chunks_d, ch.data (), sizeof (Chunk) * ch.size (), cudaMemcpyHostToDevice));
+  }
   // children per level (restriction) and ghost strips per level (interpolation)
   std::vector<int> kids;
   std::vector<StripDesc> strips;

@@ -39,6 +39,24 @@ k_nonneg (const PatchDesc *pd, const int *plist, int set)
     a[i] = clamp0 (a[i]);
 }
 
+// The same over a flat list of chunks: chunk b is
+// elements [start, start + chunk) of the species arrays of patch `patch`, so a
+// tree of patches of any sizes is one launch with every block busy.
+struct Chunk {
+  int patch, start;
+};
+
+__global__ void
+k_nonneg_chunks (const PatchDesc *pd, const Chunk *chunks, int set, int chunk)
+{
+  const Chunk ch = chunks[blockIdx.x];
+  const PatchDesc &P = pd[ch.patch];
+  double *a = P.arr (set, K_DENS, 0);
+  const long long n = P.asz * P.ns;
+  const long long end = (long long) ch.start + chunk < n ? (long long) ch.start + chunk : n;
+  for (long long i = ch.start + threadIdx.x; i < end; i += blockDim.x) a[i] = clamp0 (a[i]);
+}
+
 // ---- A10: cdr_update (cdr.c:1091-1097): dens[dst] = dens[src] + h d_dens[src] ----
 __global__ void
 k_update (const PatchDesc *pd, const int *plist, int src, int dst, const DevState *st,
@@ -216,13 +234,12 @@ k_restrict (const PatchDesc *pd, const int *children, int set)
   const int iz0 = (cz0 >> 1) + (cz0 % 2), iz1 = (cz1 >> 1);
   const int wr = ir1 - ir0, wz = iz1 - iz0;
   if (wr <= 0 || wz <= 0) return;
-  const long long total = (long long) wr * wz * Pp.ntheta * C.ns;
-  for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long long) gridDim.x * blockDim.x) {
-    const int ir = ir0 + (int) (i % wr);
-    const int iz = iz0 + (int) ((i / wr) % wz);
-    const int it = (int) ((i / wr / wz) % Pp.ntheta);
-    const int s = (int) (i / wr / wz / Pp.ntheta);
+  // 32-bit indices (a child's covered cells x planes x species stay far below 2^31)
+  const int total = wr * wz * Pp.ntheta * C.ns;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const int q = i / wr, ir = ir0 + (i - q * wr);
+    const int q2 = q / wz, iz = iz0 + (q - q2 * wz);
+    const int s = q2 / Pp.ntheta, it = q2 - s * Pp.ntheta;
     const double *cn = C.arr (set, K_DENS, s);
     double sum = 0;
     for (int cr = (ir << 1); cr <= (ir << 1) + 1; cr++)
@@ -289,14 +306,12 @@ k_interp (const PatchDesc *pd, const StripDesc *strips, int set)
   const int fz0 = max (S.sz0 - 2, z0c << 1), fz1 = min (S.sz1 + 2, z1c << 1);
   const int wr = fr1 - fr0, wz = fz1 - fz0;
   if (wr <= 0 || wz <= 0) return;
-  const long long total = (long long) wr * wz * C.ntheta * C.ns;
+  const int total = wr * wz * C.ntheta * C.ns;       // a strip's cells: far below 2^31
   const double Lr = Pp.dr, Lz = Pp.dz;
-  for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long long) gridDim.x * blockDim.x) {
-    const int ir = fr0 + (int) (i % wr);
-    const int iz = fz0 + (int) ((i / wr) % wz);
-    const int it = (int) ((i / wr / wz) % C.ntheta);
-    const int s = (int) (i / wr / wz / C.ntheta);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const int q = i / wr, ir = fr0 + (i - q * wr);
+    const int q2 = q / wz, iz = fz0 + (q - q2 * wz);
+    const int s = q2 / C.ntheta, it = q2 - s * C.ntheta;
     const int pr = ir >> 1, pz = iz >> 1;
     // stay inside the ghost extents of child and parent
     if (ir - C.r0 < -2 || ir - C.r0 >= C.nr + 2 || iz - C.z0 < -2 || iz - C.z0 >= C.nz + 2) continue;
