@@ -713,6 +713,17 @@ read_states (Ctx *c, std::vector<DevState> &st)
   return ARCOS_OK;
 }
 
+// Before a run: a step computed ahead is the sixth small one and would be
+// taken now - the reference stops there (cdr.c:1300-1301).
+int
+small_dt_pending (Ctx *c, const std::vector<DevState> &st)
+{
+  for (int f = 0; f < c->nfam; f++)
+    if ((st[f].error & (1 << ARCOS_ERR_SMALL_DT)) && st[f].small_dt_step <= st[f].step)
+      return fail (ARCOS_ERR_SMALL_DT, "too many steps below warn_min_timestep (cdr.c:1296-1302), family " + std::to_string (f));
+  return ARCOS_OK;
+}
+
 int
 check_state_errors (Ctx *c)
 {
@@ -724,7 +735,9 @@ check_state_errors (Ctx *c)
       return fail (ARCOS_ERR_NAN, "CFL maxima invalid (the assertion of cdr_courant, cdr.c:1023), family " + std::to_string (f));
     if (st[f].error & (1 << ARCOS_ERR_TIMEOUT))
       return fail (ARCOS_ERR_TIMEOUT, "a bounded wait for a tile copy gave up, family " + std::to_string (f));
-    if (st[f].error & (1 << ARCOS_ERR_SMALL_DT))
+    // the sixth small step counts once it has been taken (or is about to be:
+    // see small_dt_pending)
+    if ((st[f].error & (1 << ARCOS_ERR_SMALL_DT)) && st[f].small_dt_step < st[f].step)
       return fail (ARCOS_ERR_SMALL_DT, "too many steps below warn_min_timestep (cdr.c:1296-1302), family " + std::to_string (f));
   }
   return ARCOS_OK;
@@ -1835,6 +1848,8 @@ arcos_commit (void *ctx)
     s.courant_const[2] = (6.283185307179586477 / c->p.max_ntheta) * rmin;
     s.courant_const[3] = (c->p.max_ntheta == 1) ? 0.0 : 1.0;
     s.dt_cap = c->dt_cap;
+    s.counted_step = -1;
+    s.small_dt_step = -1;
     s.dt_log = c->dtlog_d + (size_t) f * c->dt_cap;
   }
   CK (cudaMalloc (&c->st_d, sizeof (DevState) * c->nfam));
@@ -2365,6 +2380,11 @@ arcos_cdr_rk2 (void *ctx, double h, double t, double *h_used)
   if (r) return r;
   if (!inloop (c) && !(c->field_set[0] && c->field_set[1]))
     return fail (ARCOS_ERR_STATE, "no field: call arcos_set_field (+ arcos_field_post) for both sets, or arcos_set_field_fn");
+  {
+    std::vector<DevState> st0;
+    if ((r = read_states (c, st0))) return r;
+    if ((r = small_dt_pending (c, st0))) return r;
+  }
   if ((r = set_h_attempt (c, h))) return r;
   if ((r = rk2_general (c))) return r;
   CK (cudaStreamSynchronize (c->stream));
@@ -2386,6 +2406,7 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
     return fail (ARCOS_ERR_STATE, "no field: call arcos_set_field (+ arcos_field_post) for both sets, or arcos_set_field_fn");
   std::vector<DevState> st0;
   if ((r = read_states (c, st0))) return r;
+  if (nsteps > 0 && (r = small_dt_pending (c, st0))) return r;
   const int step0 = st0[0].step;
   const bool fixed_fused = c->fused_ok && !inloop (c);
   if (fixed_fused) {

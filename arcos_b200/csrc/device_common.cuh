@@ -109,6 +109,8 @@ struct DevState {
   unsigned int neg[2];            // per step (ping-pong): the state may hold negative densities
   double courant_const[4];        // dr_min, dz_min, rdtheta_min, is_3d
   int dt_cap;                     // capacity of the dt log
+  int counted_step;               // step whose small h was last counted (-1: none)
+  int small_dt_step;              // step whose h was the sixth small one
   int pad_;
   double *dt_log;                 // steps taken
 };

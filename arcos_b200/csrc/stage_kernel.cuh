@@ -204,9 +204,18 @@ cfl_step (DevState *st, const Model &M, int slot, int eset, int idx)
   const double h = mymin (st->h_attempt, cour);                          // cdr.c:1288
   st->h = h;
   if (!ok) st->error |= 1 << 3;
-  if (h < M.warn_min_timestep) {                                          // cdr.c:1290-1302
+  // cdr.c:1269,1290-1302: five small steps are tolerated, the sixth stops the
+  // run.  A step's h may be computed twice (ahead by the last stage of the
+  // previous step, again at the start of a run): it counts once, and the step
+  // that is the sixth is recorded, so the host reports the stop when that
+  // step is about to be taken.
+  if (h < M.warn_min_timestep && st->counted_step != idx) {
+    st->counted_step = idx;
     st->small_dt_count++;
-    if (st->small_dt_count >= 6) st->error |= 1 << 4;
+    if (st->small_dt_count == 6) {
+      st->error |= 1 << 4;
+      st->small_dt_step = idx;
+    }
   }
   if (idx >= 0 && idx < st->dt_cap) st->dt_log[idx] = h;
 }

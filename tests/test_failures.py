@@ -143,6 +143,28 @@ def test_small_timestep_stops_at_the_sixth_step(cuda_device, exact):
 
 
 @pytest.mark.gpu
+def test_small_timestep_per_call_and_tree_step(cuda_device):
+    """Step by step (the step size of the next step is computed ahead and
+    again at the next call: it counts once), and through cdr_rk2."""
+    pb = workloads.plain(nr=24, nz=40, ion_mass=1.0, noise=1e-3, seed=3)
+    pb.params.warn_min_timestep = 1.0
+    t = _tree(pb, exact=False)
+    for _ in range(5):
+        t.run(1, 50.0)
+    with pytest.raises(ArcosError) as ei:
+        t.run(1, 50.0)
+    assert ei.value.code == ERR_SMALL_DT
+    t.close()
+    t = _tree(pb, exact=True)
+    for _ in range(5):
+        t.cdr_rk2(50.0)
+    with pytest.raises(ArcosError) as ei:
+        t.cdr_rk2(50.0)
+    assert ei.value.code == ERR_SMALL_DT
+    t.close()
+
+
+@pytest.mark.gpu
 def test_degenerate_grids_are_refused_before_any_launch(cuda_device):
     pb = workloads.plain(nr=16, nz=16, ion_mass=1.0, seed=4)
     L = lib()
