@@ -600,11 +600,15 @@ do_set_bnd (Ctx *c, int set)
   for (int l = 1; l <= c->max_level; l++) {
     const int n = c->strip_cnt[l];
     if (n == 0) continue;
-    if (!c->per_patch)
-      k_interp<<<dim3 (8, n), 256, 0, c->stream>>> (c->pd_d, c->strips_d + c->strip_off[l], set);
-    else
+    const StripDesc *sd = c->strips_d + c->strip_off[l];
+    if (!c->per_patch) {
+      if (c->exact) k_interp<false><<<dim3 (8, n), 256, 0, c->stream>>> (c->pd_d, sd, set);
+      else k_interp<true><<<dim3 (8, n), 256, 0, c->stream>>> (c->pd_d, sd, set);
+    } else {
       for (int i = 0; i < n; i++)
-        k_interp<<<dim3 (8, 1), 256, 0, c->stream>>> (c->pd_d, c->strips_d + c->strip_off[l] + i, set);
+        if (c->exact) k_interp<false><<<dim3 (8, 1), 256, 0, c->stream>>> (c->pd_d, sd + i, set);
+        else k_interp<true><<<dim3 (8, 1), 256, 0, c->stream>>> (c->pd_d, sd + i, set);
+    }
     CKL ();
   }
   return ARCOS_OK;

@@ -287,6 +287,11 @@ struct StripDesc {
   int child, sr0, sz0, sr1, sz1;
 };
 
+// FAST (the division-free step): the coefficients are scaled by reciprocal
+// powers of the parent's spacing instead of divided by the powers
+// (interpol_set_coeffs divides twice per coefficient, interpol2.c:180); the
+// result differs in the last bits only.
+template <bool FAST>
 __global__ void
 k_interp (const PatchDesc *pd, const StripDesc *strips, int set)
 {
@@ -327,14 +332,30 @@ k_interp (const PatchDesc *pd, const StripDesc *strips, int set)
     // interpol_set_coeffs (interpol2.c:161-186)
     double cf[6], Lrn[4], Lzn[4];
     int pindx = 0, mindx = 0;
-    Lrn[0] = 1.0; Lzn[0] = 1.0;
-    for (int ip = 0; ip < 3; ip++) {
-      Lrn[ip + 1] = Lrn[ip] * Lr;
-      Lzn[ip + 1] = Lzn[ip] * Lz;
-      for (int n = 0; n <= ip; n++) {
-        double sum = 0;
-        for (int j = 0; j < 9; j++) sum += c_quad[mindx++] * st[j];
-        cf[pindx++] = sum / Lrn[n] / Lzn[ip - n];
+    if (FAST) {
+      Lrn[0] = 1.0; Lzn[0] = 1.0;
+      Lrn[1] = 1.0 / Lr; Lzn[1] = 1.0 / Lz;
+      Lrn[2] = Lrn[1] * Lrn[1]; Lzn[2] = Lzn[1] * Lzn[1];
+#pragma unroll
+      for (int ip = 0; ip < 3; ip++)
+#pragma unroll
+        for (int n = 0; n <= ip; n++) {
+          double sum = 0;
+#pragma unroll
+          for (int j = 0; j < 9; j++) sum = __fma_rn (c_quad[mindx + j], st[j], sum);
+          mindx += 9;
+          cf[pindx++] = sum * (Lrn[n] * Lzn[ip - n]);
+        }
+    } else {
+      Lrn[0] = 1.0; Lzn[0] = 1.0;
+      for (int ip = 0; ip < 3; ip++) {
+        Lrn[ip + 1] = Lrn[ip] * Lr;
+        Lzn[ip + 1] = Lzn[ip] * Lz;
+        for (int n = 0; n <= ip; n++) {
+          double sum = 0;
+          for (int j = 0; j < 9; j++) sum += c_quad[mindx++] * st[j];
+          cf[pindx++] = sum / Lrn[n] / Lzn[ip - n];
+        }
       }
     }
     // interpol_apply + gen_apply (interpol2.c:190-241), masses: divide by r
