@@ -130,6 +130,14 @@ class CdrTree:
         check(self.L.arcos_download(self.h, self.ids[gid], set, KINDS[what], s, _dp(a)))
         return a
 
+    def dump(self, path, gid: int = 0, what: str = "dens", s: int = 0, set: int = SET_GRID):
+        """FP64 dump of one array's interior (rz_dump_3d's order, lossless)."""
+        check(self.L.arcos_dump(self.h, self.ids[gid], set, KINDS[what], s, str(path).encode(), 1))
+
+    def load(self, path, gid: int = 0, what: str = "dens", s: int = 0, set: int = SET_GRID):
+        """Load a dump written by ``dump`` into the interior (ghosts kept)."""
+        check(self.L.arcos_dump(self.h, self.ids[gid], set, KINDS[what], s, str(path).encode(), 0))
+
     def set_field(self, gid: int, er, ez, etheta=None, set: int = SET_GRID):
         arrs = [None if x is None else np.ascontiguousarray(x, dtype=np.float64) for x in (er, ez, etheta)]
         ptrs = [None if x is None else _dp(x) for x in arrs]

@@ -1998,6 +1998,59 @@ arcos_download (void *ctx, int grid, int set, int kind, int species, double *hos
   return ARCOS_OK;
 }
 
+// FP64 dump of one array of one grid (rz_dump_3d, src/rz_array.c:352-407,
+// which prints "%15.5e" text): the interior cells in rz_dump_3d's order (theta
+// outermost, then r, z fastest), as raw little-endian doubles after a 32-byte
+// header (magic "ARCOSF64", nr, nz, ntheta, 0).  Loading writes the interior
+// cells back and leaves the ghosts as they are, as rz_dump_3d's "r" mode
+// does; a file of another shape is refused.
+int
+arcos_dump (void *ctx, int grid, int set, int kind, int species, const char *path, int write)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (!path || grid < 0 || grid >= (int) c->pd_h.size () || set < 0 || set > 1 || !kind_ok (kind, species, c->M.ns))
+    return fail (ARCOS_ERR_ARG, "arcos_dump: bad argument");
+  const PatchDesc &P = c->pd_h[grid];
+  const int nr = P.nr, nz = P.nz, nt = P.ntheta, w = nr + 4;
+  const size_t plane = (size_t) w * (nz + 4);
+  std::vector<double> img (plane * P.planes), cells ((size_t) nr * nz * nt);
+  if ((r = arcos_download (ctx, grid, set, kind, species, img.data ()))) return r;
+  const int t0 = nt == 1 ? 0 : 2;                  // plane index of theta = 0
+  auto at = [&] (int it, int ir, int iz) -> double & {
+    return img[(size_t) (it + t0) * plane + (size_t) (iz + 2) * w + (ir + 2)];
+  };
+  const char magic[8] = {'A', 'R', 'C', 'O', 'S', 'F', '6', '4'};
+  int hdr[6] = {nr, nz, nt, 0, 0, 0};
+  if (write) {
+    size_t q = 0;
+    for (int it = 0; it < nt; it++)
+      for (int ir = 0; ir < nr; ir++)
+        for (int iz = 0; iz < nz; iz++) cells[q++] = at (it, ir, iz);
+    FILE *fp = fopen (path, "wb");
+    if (!fp) return fail (ARCOS_ERR_ARG, std::string ("arcos_dump: cannot open ") + path);
+    const bool ok = fwrite (magic, 1, 8, fp) == 8 && fwrite (hdr, sizeof (int), 6, fp) == 6
+                    && fwrite (cells.data (), sizeof (double), cells.size (), fp) == cells.size ();
+    if (fclose (fp) != 0 || !ok) return fail (ARCOS_ERR_ARG, std::string ("arcos_dump: write failed: ") + path);
+    return ARCOS_OK;
+  }
+  FILE *fp = fopen (path, "rb");
+  if (!fp) return fail (ARCOS_ERR_ARG, std::string ("arcos_dump: cannot open ") + path);
+  char m[8];
+  int h[6];
+  bool ok = fread (m, 1, 8, fp) == 8 && memcmp (m, magic, 8) == 0 && fread (h, sizeof (int), 6, fp) == 6
+            && h[0] == nr && h[1] == nz && h[2] == nt
+            && fread (cells.data (), sizeof (double), cells.size (), fp) == cells.size ();
+  fclose (fp);
+  if (!ok) return fail (ARCOS_ERR_ARG, std::string ("arcos_dump: not a dump of this grid's shape: ") + path);
+  size_t q = 0;
+  for (int it = 0; it < nt; it++)
+    for (int ir = 0; ir < nr; ir++)
+      for (int iz = 0; iz < nz; iz++) at (it, ir, iz) = cells[q++];
+  return arcos_upload (ctx, grid, set, kind, species, img.data ());
+}
+
 int
 arcos_sync (void *ctx)
 {

@@ -111,6 +111,13 @@ int arcos_upload (void *ctx, int grid, int set, int kind, int species,
 int arcos_download (void *ctx, int grid, int set, int kind, int species,
                     double *host);
 int arcos_sync (void *ctx);
+/* FP64 dump (write = 1) or load (write = 0) of one array of one grid, in place
+ * of rz_dump_3d's "%15.5e" text (src/rz_array.c:352-407): the interior cells
+ * in the same order (theta outermost, then r, z fastest) as raw doubles
+ * after a 32-byte header ("ARCOSF64", nr, nz, ntheta); lossless, and a load
+ * refuses a file of another shape.  Loading leaves the ghost cells as they
+ * are. */
+int arcos_dump (void *ctx, int grid, int set, int kind, int species, const char *path, int write);
 
 /* ---- the field seam ----------------------------------------------------
  * Replaces what pois_solve_a (src/poisson.c:763) writes into the CDR grids:
