@@ -31,7 +31,7 @@ k_pack_rows (const double *__restrict__ src, double *__restrict__ dst, int w, lo
 __global__ void
 k_nonneg (const PatchDesc *pd, const int *plist, int set)
 {
-  const PatchDesc &P = pd[plist[blockIdx.y]];
+  const PatchDesc P = pd[plist[blockIdx.y]];
   double *a = P.arr (set, K_DENS, 0);
   const long long n = P.asz * P.ns;       // the species arrays are contiguous
   for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -50,7 +50,7 @@ __global__ void
 k_nonneg_chunks (const PatchDesc *pd, const Chunk *chunks, int set, int chunk)
 {
   const Chunk ch = chunks[blockIdx.x];
-  const PatchDesc &P = pd[ch.patch];
+  const PatchDesc P = pd[ch.patch];
   double *a = P.arr (set, K_DENS, 0);
   const long long n = P.asz * P.ns;
   const long long end = (long long) ch.start + chunk < n ? (long long) ch.start + chunk : n;
@@ -62,7 +62,7 @@ __global__ void
 k_update (const PatchDesc *pd, const int *plist, int src, int dst, const DevState *st,
           double h_host, int use_dev_h)
 {
-  const PatchDesc &P = pd[plist[blockIdx.y]];
+  const PatchDesc P = pd[plist[blockIdx.y]];
   const double h = use_dev_h ? st[P.fam].h : h_host;
   const double *n = P.arr (src, K_DENS, 0), *d = P.arr (src, K_DDENS, 0);
   double *o = P.arr (dst, K_DENS, 0);
@@ -78,7 +78,7 @@ __global__ void
 k_rk2_update (const PatchDesc *pd, const int *plist, const DevState *st, double h_host,
               int use_dev_h)
 {
-  const PatchDesc &P = pd[plist[blockIdx.y]];
+  const PatchDesc P = pd[plist[blockIdx.y]];
   const double h = use_dev_h ? st[P.fam].h : h_host;
   double *n = P.arr (0, K_DENS, 0);
   const double *d1 = P.arr (0, K_DDENS, 0), *d2 = P.arr (1, K_DDENS, 0);
@@ -93,7 +93,7 @@ k_rk2_update (const PatchDesc *pd, const int *plist, const DevState *st, double 
 __global__ void
 k_charge (const Model M, const PatchDesc *pd, const int *plist, int set)
 {
-  const PatchDesc &P = pd[plist[blockIdx.y]];
+  const PatchDesc P = pd[plist[blockIdx.y]];
   double *ch = P.arr (set, K_CHARGE);
   const long long len = P.asz;
   const int nr4 = P.nr + 4;
@@ -118,7 +118,7 @@ __global__ void
 k_charge_star (const Model M, const PatchDesc *pd, const int *plist, int src,
                const DevState *st)
 {
-  const PatchDesc &P = pd[plist[blockIdx.y]];
+  const PatchDesc P = pd[plist[blockIdx.y]];
   const double h = st[P.fam].h;
   double *ch = P.arr (1, K_CHARGE);
   const long long len = P.asz;
@@ -149,7 +149,7 @@ k_ext_bnd (const Model M, const PatchDesc *pd, const int *plist, int set)
 {
   // one block per (patch, theta plane, species); the sides in the reference
   // order, since the z sides copy the r sides' ghost columns (the corners)
-  const PatchDesc &P = pd[plist[blockIdx.x]];
+  const PatchDesc P = pd[plist[blockIdx.x]];
   const int nr = P.nr, nz = P.nz, nt = P.ntheta;
   const int it = blockIdx.y, s = blockIdx.z;
   if (it >= nt || s >= P.ns) return;
@@ -198,7 +198,7 @@ k_ext_bnd (const Model M, const PatchDesc *pd, const int *plist, int set)
 __global__ void
 k_periodic (const PatchDesc *pd, const int *plist, int set, int what)
 {
-  const PatchDesc &P = pd[plist[blockIdx.y]];
+  const PatchDesc P = pd[plist[blockIdx.y]];
   const int nt = P.ntheta;
   if (nt == 1) return;
   const long long ps = P.plane_stride;
@@ -227,8 +227,8 @@ k_periodic (const PatchDesc *pd, const int *plist, int set, int what)
 __global__ void
 k_restrict (const PatchDesc *pd, const int *children, int set)
 {
-  const PatchDesc &C = pd[children[blockIdx.y]];
-  const PatchDesc &Pp = pd[C.parent];
+  const PatchDesc C = pd[children[blockIdx.y]];
+  const PatchDesc Pp = pd[C.parent];
   const int cr0 = C.r0, cz0 = C.z0, cr1 = C.r0 + C.nr, cz1 = C.z0 + C.nz;
   const int ir0 = (cr0 >> 1) + (cr0 % 2), ir1 = (cr1 >> 1);
   const int iz0 = (cz0 >> 1) + (cz0 % 2), iz1 = (cz1 >> 1);
@@ -296,8 +296,8 @@ __global__ void
 k_interp (const PatchDesc *pd, const StripDesc *strips, int set)
 {
   const StripDesc S = strips[blockIdx.y];
-  const PatchDesc &C = pd[S.child];
-  const PatchDesc &Pp = pd[C.parent];
+  const PatchDesc C = pd[S.child];
+  const PatchDesc Pp = pd[C.parent];
   const int pr0 = Pp.r0, pz0 = Pp.z0, pr1 = Pp.r0 + Pp.nr, pz1 = Pp.z0 + Pp.nz;
   // grid_overlap (parent, strip, s_buff = 1, t_buff = 0), grid.c:145-198
   const int left = max (S.sr0, (pr0 - 1) << 1), right = min (S.sr1, (pr1 + 1) << 1);
@@ -396,7 +396,7 @@ k_add_ext (const PatchDesc *pd, const int *plist, int set, const double *ext_r,
            const double *ext_t, const double *ext_z, int *etz)
 {
   const int p = plist[blockIdx.y];
-  const PatchDesc &P = pd[p];
+  const PatchDesc P = pd[p];
   double *er = P.arr (set, K_ER), *ez = P.arr (set, K_EZ), *et = P.arr (set, K_ETHETA);
   const long long len = P.asz;
   const int nr4 = P.nr + 4;
@@ -422,7 +422,7 @@ __global__ void
 k_eabs (const PatchDesc *pd, const int *plist, int set, DevState *st)
 {
   const int p = plist[blockIdx.y];
-  const PatchDesc &P = pd[p];
+  const PatchDesc P = pd[p];
   const double *er = P.arr (set, K_ER), *ez = P.arr (set, K_EZ), *et = P.arr (set, K_ETHETA);
   double *ea = P.arr (set, K_EABS);
   const long long total = (long long) P.nr * P.nz * P.ntheta;
@@ -459,7 +459,7 @@ k_eabs (const PatchDesc *pd, const int *plist, int set, DevState *st)
 __global__ void
 k_dmax (const Model M, const PatchDesc *pd, const int *plist, int set, DevState *st, int slot_rel)
 {
-  const PatchDesc &P = pd[plist[blockIdx.y]];
+  const PatchDesc P = pd[plist[blockIdx.y]];
   if (P.level != 0) return;
   const int nr = P.nr, nz = P.nz, ns = P.ns, rows = nz * P.ntheta;
   const long long asz = P.asz;                 // the species arrays of a set are consecutive
