@@ -415,7 +415,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
 #pragma unroll
       for (int j = 0; j <= RPW; j++) vz[j] = A.cm[s] * ezw[j];
       const int orient = species_orient (zsigns, A.cm[s]);
-      const double dd = A.ddz[s] * T.lsc;
+      const double dd = TREE ? A.ddz[s] * T.lsc : A.ddz[s];
       if (orient == 1) {
 #pragma unroll
         for (int k = 0; k < RPW; k++) fzt[k][s] = face_o<false, true> (nw[k + 1], nw[k + 2], nw[k + 3], vz[k + 1], dd);
@@ -437,7 +437,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       const int row = r_first + i % RPW, s = i / RPW;
       const double *q = sm + s * PL + (row + 2) * TXP;
       rb[s][row] = face_any<true> (0, q[32], q[33], q[34], q[35], A.cm[s] * sm[NS * PL + (row + 2) * TXP + 33],
-                                   A.ddr[s] * T.lsc);
+                                   TREE ? A.ddr[s] * T.lsc : A.ddr[s]);
     }
 #pragma unroll
     for (int k = 0; k < RPW; k++)
@@ -456,7 +456,8 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
         }
       }
       // z_cutoff gate (reaction.c:121): only a tile reaching it tests its rows
-      const bool gate = ((double) (T.z0zb + TY) + 0.5) * T.dz >= M.z_cutoff;
+      const double dzl = TREE ? T.dz : A.dz;
+      const bool gate = ((double) (T.z0zb + TY) + 0.5) * dzl >= M.z_cutoff;
 #pragma unroll 1
       for (int r = 0; r < A.nreact; r++) {
         const TableNode *nd = nodes + A.r_node0[r];
@@ -475,7 +476,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
         if (gate) {
 #pragma unroll
           for (int k = 0; k < RPW; k++)
-            if (!(((double) (T.z0zb + r_first + k) + 0.5) * T.dz < M.z_cutoff)) rate[k] = 0.0;
+            if (!(((double) (T.z0zb + r_first + k) + 0.5) * dzl < M.z_cutoff)) rate[k] = 0.0;
         }
 #pragma unroll
         for (int s = 0; s < NS; s++) {
@@ -493,8 +494,9 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
       for (int s = 0; s < NS; s++) fzb[s] = zt[wq - 1][s][lane];
     }
     const int c = c0 + lane;
-    const double erm = A.colfac[2 * (T.cf0 + c)], erp = A.colfac[2 * (T.cf0 + c) + 1];   // .f90:408-412
-    const double gdz = A.gdz * T.lsc;
+    const int cfi = TREE ? T.cf0 + c : c;
+    const double erm = A.colfac[2 * cfi], erp = A.colfac[2 * cfi + 1];   // .f90:408-412
+    const double gdz = TREE ? A.gdz * T.lsc : A.gdz;
     const bool last = lane == 31;
     const double h = T.h, hh = 0.5 * h;
     double erl[RPW];
@@ -522,7 +524,7 @@ k_fused (const __grid_constant__ Model M, const __grid_constant__ FusedArgs A)
 #pragma unroll
       for (int k = 0; k < RPW; k++) vr[k] = A.cm[s] * erl[k];
       const int orient = species_orient (rsigns, A.cm[s]);
-      const double dd = A.ddr[s] * T.lsc;
+      const double dd = TREE ? A.ddr[s] * T.lsc : A.ddr[s];
       double *outp = T.out[s] + ro;
       const bool mob = M.mobile[s];
 #pragma unroll
