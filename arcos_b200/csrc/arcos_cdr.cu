@@ -105,6 +105,11 @@ struct Ctx {
   StripDesc *strips_d = nullptr;
   std::vector<int> strip_off, strip_cnt;   // per level
   std::vector<int> strip_patch;            // per strip: child patch (for per-patch mode)
+  WorkBlk *rblk_d = nullptr, *iblk_d = nullptr;   // flat work blocks of restriction / interpolation
+  std::vector<int> rblk_off, rblk_cnt, iblk_off, iblk_cnt;   // per level
+  int *extp_d = nullptr;              // the patches with an external boundary
+  int n_extp = 0;
+  int ext_slices = 1;                 // blocks per (patch, species) of k_ext_bnd
   long long *match_src_d[2] = {nullptr, nullptr}, *match_dst_d[2] = {nullptr, nullptr};
   double *match_tmp_d = nullptr;
   int n_match = 0;
@@ -551,12 +556,12 @@ int
 do_ext_bnd (Ctx *c, int set)
 {
   const int np = (int) c->pd_h.size ();
-  int maxnt = 1;
-  for (auto &P : c->pd_h) maxnt = std::max (maxnt, P.ntheta);
-  if (!c->per_patch) k_ext_bnd<<<dim3 (np, maxnt, c->M.ns), 256, 0, c->stream>>> (c->M, c->pd_d, c->plist_d, set);
-  else
+  if (!c->per_patch) {
+    if (c->n_extp)
+      k_ext_bnd<<<dim3 (c->n_extp, c->M.ns, c->ext_slices), 256, 0, c->stream>>> (c->M, c->pd_d, c->extp_d, set);
+  } else
     for (int p = 0; p < np; p++)
-      k_ext_bnd<<<dim3 (1, c->pd_h[p].ntheta, c->M.ns), 256, 0, c->stream>>> (c->M, c->pd_d, c->plist_d + p, set);
+      k_ext_bnd<<<dim3 (1, c->M.ns, c->ext_slices), 256, 0, c->stream>>> (c->M, c->pd_d, c->plist_d + p, set);
   CKL ();
   return ARCOS_OK;
 }
@@ -584,9 +589,10 @@ do_restrict (Ctx *c, int set)
   for (int l = c->max_level; l >= 1; l--) {
     const int n = c->level_cnt[l];
     if (n == 0) continue;
-    if (!c->per_patch)
-      k_restrict<<<dim3 (64, n), 256, 0, c->stream>>> (c->pd_d, c->kids_d + c->level_off[l], set);
-    else
+    if (!c->per_patch) {
+      if (c->rblk_cnt[l])
+        k_restrict_blk<<<c->rblk_cnt[l], RESTRICT_THREADS, 0, c->stream>>> (c->pd_d, c->rblk_d + c->rblk_off[l], set);
+    } else
       for (int i = 0; i < n; i++)
         k_restrict<<<dim3 (64, 1), 256, 0, c->stream>>> (c->pd_d, c->kids_d + c->level_off[l] + i, set);
     CKL ();
@@ -602,8 +608,11 @@ do_set_bnd (Ctx *c, int set)
     if (n == 0) continue;
     const StripDesc *sd = c->strips_d + c->strip_off[l];
     if (!c->per_patch) {
-      if (c->exact) k_interp<false><<<dim3 (8, n), 256, 0, c->stream>>> (c->pd_d, sd, set);
-      else k_interp<true><<<dim3 (8, n), 256, 0, c->stream>>> (c->pd_d, sd, set);
+      const int nb = c->iblk_cnt[l];
+      const WorkBlk *wb = c->iblk_d + c->iblk_off[l];
+      if (nb == 0) continue;
+      if (c->exact) k_interp_blk<false><<<nb, INTERP_THREADS, 0, c->stream>>> (c->pd_d, c->strips_d, wb, set);
+      else k_interp_blk<true><<<nb, INTERP_THREADS, 0, c->stream>>> (c->pd_d, c->strips_d, wb, set);
     } else {
       for (int i = 0; i < n; i++)
         if (c->exact) k_interp<false><<<dim3 (8, 1), 256, 0, c->stream>>> (c->pd_d, sd + i, set);
@@ -1358,6 +1367,7 @@ arcos_destroy (void *ctx)
   cudaFree (c->pool); cudaFree (c->pd_d); cudaFree (c->nodes_d); cudaFree (c->st_d);
   cudaFree (c->dtlog_d); cudaFree (c->etz_d); cudaFree (c->done_d); cudaFree (c->items_d);
   cudaFree (c->plist_d); cudaFree (c->roots_d); cudaFree (c->chunks_d); cudaFree (c->kids_d); cudaFree (c->strips_d); cudaFree (c->ext_d);
+  cudaFree (c->rblk_d); cudaFree (c->iblk_d); cudaFree (c->extp_d);
   for (int s = 0; s < 2; s++) { cudaFree (c->match_src_d[s]); cudaFree (c->match_dst_d[s]); }
   cudaFree (c->match_tmp_d);
   cudaFree (c->xfer_d);
@@ -1771,6 +1781,55 @@ arcos_commit (void *ctx)
     }
     c->level_cnt[l] = (int) kids.size () - c->level_off[l];
     c->strip_cnt[l] = (int) strips.size () - c->strip_off[l];
+  }
+  // flat work blocks per level: the covered parent cells of every child (the
+  // count restrict_geom gives) and the fine cells of every strip (interp_geom)
+  {
+    std::vector<WorkBlk> rb, ib;
+    c->rblk_off.assign (c->max_level + 1, 0);
+    c->rblk_cnt.assign (c->max_level + 1, 0);
+    c->iblk_off.assign (c->max_level + 1, 0);
+    c->iblk_cnt.assign (c->max_level + 1, 0);
+    for (int l = 1; l <= c->max_level; l++) {
+      c->rblk_off[l] = (int) rb.size ();
+      for (int k = c->level_off[l]; k < c->level_off[l] + c->level_cnt[l]; k++) {
+        const PatchDesc &C = c->pd_h[kids[k]];
+        const int ir0 = (C.r0 >> 1) + (C.r0 % 2), iz0 = (C.z0 >> 1) + (C.z0 % 2);
+        const int wr = ((C.r0 + C.nr) >> 1) - ir0, wz = ((C.z0 + C.nz) >> 1) - iz0;
+        const long long n = (wr <= 0 || wz <= 0) ? 0 : (long long) wr * wz * c->pd_h[C.parent].ntheta * C.ns;
+        for (long long f = 0; f < n; f += RESTRICT_PER_BLOCK) rb.push_back ({kids[k], C.parent, -1, (int) f});
+      }
+      c->rblk_cnt[l] = (int) rb.size () - c->rblk_off[l];
+      c->iblk_off[l] = (int) ib.size ();
+      for (int k = c->strip_off[l]; k < c->strip_off[l] + c->strip_cnt[l]; k++) {
+        const StripDesc &S = strips[k];
+        const PatchDesc &C = c->pd_h[S.child];
+        const long long n = interp_geom (S, C, c->pd_h[C.parent]).total;
+        for (long long f = 0; f < n; f += INTERP_PER_BLOCK) ib.push_back ({S.child, C.parent, k, (int) f});
+      }
+      c->iblk_cnt[l] = (int) ib.size () - c->iblk_off[l];
+    }
+    if (!rb.empty ()) {
+      CK (cudaMalloc (&c->rblk_d, sizeof (WorkBlk) * rb.size ()));
+      CK (cudaMemcpy (c->rblk_d, rb.data (), sizeof (WorkBlk) * rb.size (), cudaMemcpyHostToDevice));
+    }
+    if (!ib.empty ()) {
+      CK (cudaMalloc (&c->iblk_d, sizeof (WorkBlk) * ib.size ()));
+      CK (cudaMemcpy (c->iblk_d, ib.data (), sizeof (WorkBlk) * ib.size (), cudaMemcpyHostToDevice));
+    }
+    std::vector<int> ep;
+    long long most = 0;
+    for (int i = 0; i < np; i++) {
+      const PatchDesc &P = c->pd_h[i];
+      if (P.ext_bound) ep.push_back (i);
+      most = std::max (most, (long long) P.ntheta * (P.nr + P.nz + 8));
+    }
+    c->ext_slices = (int) std::max (1LL, std::min (64LL, (most + 255) / 256));
+    c->n_extp = (int) ep.size ();
+    if (!ep.empty ()) {
+      CK (cudaMalloc (&c->extp_d, sizeof (int) * ep.size ()));
+      CK (cudaMemcpy (c->extp_d, ep.data (), sizeof (int) * ep.size (), cudaMemcpyHostToDevice));
+    }
   }
   if (!kids.empty ()) {
     CK (cudaMalloc (&c->kids_d, sizeof (int) * kids.size ()));

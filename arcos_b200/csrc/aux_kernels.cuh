@@ -54,7 +54,21 @@ k_nonneg_chunks (const PatchDesc *pd, const Chunk *chunks, int set, int chunk)
   double *a = P.arr (set, K_DENS, 0);
   const long long n = P.asz * P.ns;
   const long long end = (long long) ch.start + chunk < n ? (long long) ch.start + chunk : n;
-  for (long long i = ch.start + threadIdx.x; i < end; i += blockDim.x) a[i] = clamp0 (a[i]);
+  // four independent loads per thread in flight; a value changes only when it
+  // is below zero (clamp0 keeps NaN and -0), so only those are written back
+  for (long long i0 = ch.start + threadIdx.x; i0 < end; i0 += 4 * blockDim.x) {
+    double v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const long long i = i0 + (long long) k * blockDim.x;
+      v[k] = i < end ? a[i] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const long long i = i0 + (long long) k * blockDim.x;
+      if (i < end && 0 > v[k]) a[i] = 0.0;
+    }
+  }
 }
 
 // ---- A10: cdr_update (cdr.c:1091-1097): dens[dst] = dens[src] + h d_dens[src] ----
@@ -141,53 +155,60 @@ k_charge_star (const Model M, const PatchDesc *pd, const int *plist, int src,
 }
 
 // ---- A16: cdr_set_ext_bnd (cdr.c:726-768) with set_axis_bnd (:798-824) and
-// rz_copy_bnd / rz_set_bnd (rz_array.c:196-235).  One block per patch; the four
-// sides are done in the reference order (axis, right, bottom, top) with a block
-// barrier in between, because corner cells are written by more than one side. ----
+// rz_copy_bnd / rz_set_bnd (rz_array.c:196-235).  The reference copies side by
+// side over the whole array: axis, right, bottom, top.  The z sides copy the r
+// sides' ghost columns (the corners), so a z-side thread takes the value its
+// source cell has once the r sides are done (p1, reading only interior cells);
+// an r-side thread leaves a corner to the z side when that side is external
+// (its value would be overwritten), and otherwise reads a ghost row that no
+// side of this call writes.  So every write is independent and one launch of
+// (patch, species, slice) blocks does the lot.  The two r sides (and the two
+// z sides) touch disjoint cells, since a patch has at least 2 x 2 cells. ----
 __global__ void
 k_ext_bnd (const Model M, const PatchDesc *pd, const int *plist, int set)
 {
-  // one block per (patch, theta plane, species); the sides in the reference
-  // order, since the z sides copy the r sides' ghost columns (the corners)
   const PatchDesc P = pd[plist[blockIdx.x]];
-  const int nr = P.nr, nz = P.nz, nt = P.ntheta;
-  const int it = blockIdx.y, s = blockIdx.z;
-  if (it >= nt || s >= P.ns) return;
-  const int t = threadIdx.x;
+  const int nr = P.nr, nz = P.nz, nt = P.ntheta, eb = P.ext_bound;
+  const int s = blockIdx.y;
+  if (s >= P.ns || eb == 0) return;
   double *a = P.arr (set, K_DENS, s);
-  if (P.ext_bound & 1) {                             // axis
-    const int it2 = (it + nt / 2) % nt;
-    for (int i = t; i < nz + 4; i += blockDim.x) {
-      const int iz = i - 2;
-      a[P.off (-1, iz, it)] = a[P.off (0, iz, it2)];
-      a[P.off (-2, iz, it)] = a[P.off (1, iz, it2)];
-    }
-  }
-  __syncthreads ();
-  if (P.ext_bound & 2) {                             // r = r1
-    const double sg = (double) M.bnd_sign[1];
-    for (int i = t; i < nz + 4; i += blockDim.x) {
-      const int iz = i - 2;
-      a[P.off (nr, iz, it)] = sg * a[P.off (nr - 1, iz, it)];
-      a[P.off (nr + 1, iz, it)] = sg * a[P.off (nr - 2, iz, it)];
-    }
-  }
-  __syncthreads ();
-  if (P.ext_bound & 4) {                             // z = z0
-    const double sg = (double) M.bnd_sign[2];
-    for (int i = t; i < nr + 4; i += blockDim.x) {
-      const int ir = i - 2;
-      a[P.off (ir, -1, it)] = sg * a[P.off (ir, 0, it)];
-      a[P.off (ir, -2, it)] = sg * a[P.off (ir, 1, it)];
-    }
-  }
-  __syncthreads ();
-  if (P.ext_bound & 8) {                             // z = z1
-    const double sg = (double) M.bnd_sign[3];
-    for (int i = t; i < nr + 4; i += blockDim.x) {
-      const int ir = i - 2;
-      a[P.off (ir, nz, it)] = sg * a[P.off (ir, nz - 1, it)];
-      a[P.off (ir, nz + 1, it)] = sg * a[P.off (ir, nz - 2, it)];
+  const double sg1 = (double) M.bnd_sign[1], sg2 = (double) M.bnd_sign[2], sg3 = (double) M.bnd_sign[3];
+  const int rows = nz + 4, cols = nr + 4;
+  const int nrs = (eb & 3) ? nt * rows : 0;           // r-side items (plane, row)
+  const int nzs = (eb & 12) ? nt * cols : 0;          // z-side items (plane, column)
+  // cell (c, r) of plane it, r an interior row, after the r sides
+  auto p1 = [&] (int c, int r, int it) -> double {
+    if (c < 0 && (eb & 1)) return a[P.off (-1 - c, r, (it + nt / 2) % nt)];
+    if (c >= nr && (eb & 2)) return sg1 * a[P.off (2 * nr - 1 - c, r, it)];
+    return a[P.off (c, r, it)];
+  };
+  for (int i = blockIdx.z * blockDim.x + threadIdx.x; i < nrs + nzs; i += gridDim.z * blockDim.x) {
+    if (i < nrs) {
+      const int it = i / rows, iz = i - it * rows - 2;
+      if ((iz < 0 && (eb & 4)) || (iz >= nz && (eb & 8))) continue;
+      if (eb & 1) {                                   // axis: the opposite plane
+        const int it2 = (it + nt / 2) % nt;
+        const double v0 = a[P.off (0, iz, it2)], v1 = a[P.off (1, iz, it2)];
+        a[P.off (-1, iz, it)] = v0;
+        a[P.off (-2, iz, it)] = v1;
+      }
+      if (eb & 2) {                                   // r = r1
+        const double v0 = a[P.off (nr - 1, iz, it)], v1 = a[P.off (nr - 2, iz, it)];
+        a[P.off (nr, iz, it)] = sg1 * v0;
+        a[P.off (nr + 1, iz, it)] = sg1 * v1;
+      }
+    } else {
+      const int j = i - nrs, it = j / cols, ir = j - it * cols - 2;
+      if (eb & 4) {                                   // z = z0
+        const double v0 = p1 (ir, 0, it), v1 = p1 (ir, 1, it);
+        a[P.off (ir, -1, it)] = sg2 * v0;
+        a[P.off (ir, -2, it)] = sg2 * v1;
+      }
+      if (eb & 8) {                                   // z = z1
+        const double v0 = p1 (ir, nz - 1, it), v1 = p1 (ir, nz - 2, it);
+        a[P.off (ir, nz, it)] = sg3 * v0;
+        a[P.off (ir, nz + 1, it)] = sg3 * v1;
+      }
     }
   }
 }
@@ -223,30 +244,104 @@ k_periodic (const PatchDesc *pd, const int *plist, int set, int what)
 }
 
 // ---- A17: restrict_from (cdr.c:2050-2078) for every child of one level:
-// parent(ir, iz) = 0.25 * sum_{2x2} r_c n_c / r_p. ----
+// parent(ir, iz) = 0.25 * sum_{2x2} r_c n_c / r_p.  Item i of a child runs over
+// its covered parent cells, ir fastest, then iz, plane, species. ----
+struct RestrictGeom {
+  int ir0, iz0, wr, wz, total;
+};
+
+__device__ __forceinline__ RestrictGeom
+restrict_geom (const PatchDesc &C, int ntheta_parent)
+{
+  const int cr0 = C.r0, cz0 = C.z0, cr1 = C.r0 + C.nr, cz1 = C.z0 + C.nz;
+  RestrictGeom G;
+  G.ir0 = (cr0 >> 1) + (cr0 % 2);
+  G.iz0 = (cz0 >> 1) + (cz0 % 2);
+  G.wr = (cr1 >> 1) - G.ir0;
+  G.wz = (cz1 >> 1) - G.iz0;
+  // 32-bit indices (a child's covered cells x planes x species stay far below 2^31)
+  G.total = (G.wr <= 0 || G.wz <= 0) ? 0 : G.wr * G.wz * ntheta_parent * C.ns;
+  return G;
+}
+
+// the four child values of item i, in the order the sum takes them
+struct RestrictLoad {
+  double v[4];
+  long long dst;
+  int ir, s;
+};
+
+__device__ __forceinline__ RestrictLoad
+restrict_load (const PatchDesc &C, const PatchDesc &Pp, const RestrictGeom &G, int i, int set)
+{
+  RestrictLoad L;
+  const int q = i / G.wr, ir = G.ir0 + (i - q * G.wr);
+  const int q2 = q / G.wz, iz = G.iz0 + (q - q2 * G.wz);
+  const int s = q2 / Pp.ntheta, it = q2 - s * Pp.ntheta;
+  const double *cn = C.arr (set, K_DENS, s);
+  const long long o = C.off ((ir << 1) - C.r0, (iz << 1) - C.z0, it);
+  L.v[0] = cn[o];
+  L.v[1] = cn[o + C.pitch];
+  L.v[2] = cn[o + 1];
+  L.v[3] = cn[o + 1 + C.pitch];
+  L.dst = Pp.off (ir - Pp.r0, iz - Pp.z0, it);
+  L.ir = ir;
+  L.s = s;
+  return L;
+}
+
+__device__ __forceinline__ void
+restrict_store (const PatchDesc &C, const PatchDesc &Pp, const RestrictLoad &L, int set)
+{
+  const double ra = ((double) (L.ir << 1) + 0.5) * C.dr, rb = ((double) ((L.ir << 1) + 1) + 0.5) * C.dr;
+  double sum = 0;
+  sum += ra * L.v[0];
+  sum += ra * L.v[1];
+  sum += rb * L.v[2];
+  sum += rb * L.v[3];
+  Pp.arr (set, K_DENS, L.s)[L.dst] = 0.25 * sum / (((double) L.ir + 0.5) * Pp.dr);
+}
+
 __global__ void
 k_restrict (const PatchDesc *pd, const int *children, int set)
 {
   const PatchDesc C = pd[children[blockIdx.y]];
   const PatchDesc Pp = pd[C.parent];
-  const int cr0 = C.r0, cz0 = C.z0, cr1 = C.r0 + C.nr, cz1 = C.z0 + C.nz;
-  const int ir0 = (cr0 >> 1) + (cr0 % 2), ir1 = (cr1 >> 1);
-  const int iz0 = (cz0 >> 1) + (cz0 % 2), iz1 = (cz1 >> 1);
-  const int wr = ir1 - ir0, wz = iz1 - iz0;
-  if (wr <= 0 || wz <= 0) return;
-  // 32-bit indices (a child's covered cells x planes x species stay far below 2^31)
-  const int total = wr * wz * Pp.ntheta * C.ns;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-    const int q = i / wr, ir = ir0 + (i - q * wr);
-    const int q2 = q / wz, iz = iz0 + (q - q2 * wz);
-    const int s = q2 / Pp.ntheta, it = q2 - s * Pp.ntheta;
-    const double *cn = C.arr (set, K_DENS, s);
-    double sum = 0;
-    for (int cr = (ir << 1); cr <= (ir << 1) + 1; cr++)
-      for (int cz = (iz << 1); cz <= (iz << 1) + 1; cz++)
-        sum += (((double) cr + 0.5) * C.dr) * cn[C.off (cr - cr0, cz - cz0, it)];
-    Pp.arr (set, K_DENS, s)[Pp.off (ir - Pp.r0, iz - Pp.z0, it)] =
-      0.25 * sum / (((double) ir + 0.5) * Pp.dr);
+  const RestrictGeom G = restrict_geom (C, Pp.ntheta);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G.total; i += gridDim.x * blockDim.x)
+    restrict_store (C, Pp, restrict_load (C, Pp, G, i, set), set);
+}
+
+// A block of flat work of a ghost phase over one level of a tree: items
+// [first, first + per block) of child `child` (parent `parent`, ghost strip
+// `strip` for the interpolation).  Built once per tree, so a level of patches
+// of any sizes is one launch with every block busy.
+struct WorkBlk {
+  int child, parent, strip, first;
+};
+
+constexpr int RESTRICT_PER_THREAD = 4;
+constexpr int RESTRICT_THREADS = 256;
+constexpr int RESTRICT_PER_BLOCK = RESTRICT_PER_THREAD * RESTRICT_THREADS;
+
+__global__ void __launch_bounds__ (RESTRICT_THREADS)
+k_restrict_blk (const PatchDesc *pd, const WorkBlk *wb, int set)
+{
+  const WorkBlk W = wb[blockIdx.x];
+  const PatchDesc C = pd[W.child];
+  const PatchDesc Pp = pd[W.parent];
+  const RestrictGeom G = restrict_geom (C, Pp.ntheta);
+  const int end = min (G.total, W.first + RESTRICT_PER_BLOCK);
+  RestrictLoad L[RESTRICT_PER_THREAD];
+#pragma unroll
+  for (int k = 0; k < RESTRICT_PER_THREAD; k++) {
+    const int i = W.first + k * RESTRICT_THREADS + threadIdx.x;
+    if (i < end) L[k] = restrict_load (C, Pp, G, i, set);
+  }
+#pragma unroll
+  for (int k = 0; k < RESTRICT_PER_THREAD; k++) {
+    const int i = W.first + k * RESTRICT_THREADS + threadIdx.x;
+    if (i < end) restrict_store (C, Pp, L[k], set);
   }
 }
 
@@ -287,10 +382,112 @@ struct StripDesc {
   int child, sr0, sz0, sr1, sz1;
 };
 
+// The fine cells a strip writes: [fr0, fr0 + wr) x [fz0, fz0 + wz) over planes
+// and species, ir fastest (total = 0 when the strip misses the parent).
+struct InterpGeom {
+  int fr0, fz0, wr, wz, total;
+};
+
+__host__ __device__ inline int imax_ (int a, int b) { return a > b ? a : b; }
+__host__ __device__ inline int imin_ (int a, int b) { return a < b ? a : b; }
+
+__host__ __device__ inline InterpGeom
+interp_geom (const StripDesc &S, const PatchDesc &C, const PatchDesc &Pp)
+{
+  InterpGeom G;
+  G.total = 0;
+  G.fr0 = G.fz0 = G.wr = G.wz = 0;
+  const int pr0 = Pp.r0, pz0 = Pp.z0, pr1 = Pp.r0 + Pp.nr, pz1 = Pp.z0 + Pp.nz;
+  // grid_overlap (parent, strip, s_buff = 1, t_buff = 0), grid.c:145-198
+  const int left = imax_ (S.sr0, (pr0 - 1) << 1), right = imin_ (S.sr1, (pr1 + 1) << 1);
+  const int bottom = imax_ (S.sz0, (pz0 - 1) << 1), top = imin_ (S.sz1, (pz1 + 1) << 1);
+  if (left >= right || bottom >= top) return G;
+  // map_interpol coarse range (mapper.c:199-210)
+  const int r0c = imax_ (left >> 1, pr0 - 1), r1c = imin_ (((right - 1) >> 1) + 1, pr1 + 1);
+  const int z0c = imax_ (bottom >> 1, pz0 - 1), z1c = imin_ (((top - 1) >> 1) + 1, pz1 + 1);
+  // fine cells written (interpol_inner, mapper.c:296-299)
+  const int fr0 = imax_ (S.sr0 - 2, r0c << 1), fr1 = imin_ (S.sr1 + 2, r1c << 1);
+  const int fz0 = imax_ (S.sz0 - 2, z0c << 1), fz1 = imin_ (S.sz1 + 2, z1c << 1);
+  if (fr1 <= fr0 || fz1 <= fz0) return G;
+  G.fr0 = fr0; G.fz0 = fz0; G.wr = fr1 - fr0; G.wz = fz1 - fz0;
+  G.total = G.wr * G.wz * C.ntheta * C.ns;        // a strip's cells: far below 2^31
+  return G;
+}
+
 // FAST (the division-free step): the coefficients are scaled by reciprocal
 // powers of the parent's spacing instead of divided by the powers
 // (interpol_set_coeffs divides twice per coefficient, interpol2.c:180); the
 // result differs in the last bits only.
+template <bool FAST>
+__device__ __forceinline__ void
+interp_item (const PatchDesc &C, const PatchDesc &Pp, const InterpGeom &G, int i, int set)
+{
+  const int q = i / G.wr, ir = G.fr0 + (i - q * G.wr);
+  const int q2 = q / G.wz, iz = G.fz0 + (q - q2 * G.wz);
+  const int s = q2 / C.ntheta, it = q2 - s * C.ntheta;
+  const int pr = ir >> 1, pz = iz >> 1;
+  const int pr0 = Pp.r0, pz0 = Pp.z0;
+  // stay inside the ghost extents of child and parent
+  if (ir - C.r0 < -2 || ir - C.r0 >= C.nr + 2 || iz - C.z0 < -2 || iz - C.z0 >= C.nz + 2) return;
+  if (pr - 1 - pr0 < -2 || pr + 1 - pr0 >= Pp.nr + 2 || pz - 1 - pz0 < -2 || pz + 1 - pz0 >= Pp.nz + 2) return;
+  const double Lr = Pp.dr, Lz = Pp.dz;
+  const double *pn = Pp.arr (set, K_DENS, s);
+  // interpol_set_stencil_at (interpol2.c:116-155)
+  double st[9];
+  const long long pb = Pp.off (pr - 1 - pr0, pz - 1 - pz0, it);
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) st[a * 3 + b] = pn[pb + a + (long long) b * Pp.pitch];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double r = ((double) (pr + a - 1) + 0.5) * Lr;
+#pragma unroll
+    for (int b = 0; b < 3; b++) st[a * 3 + b] = r * st[a * 3 + b];
+  }
+  // interpol_set_coeffs (interpol2.c:161-186)
+  double cf[6], Lrn[4], Lzn[4];
+  int pindx = 0, mindx = 0;
+  if (FAST) {
+    Lrn[0] = 1.0; Lzn[0] = 1.0;
+    Lrn[1] = 1.0 / Lr; Lzn[1] = 1.0 / Lz;
+    Lrn[2] = Lrn[1] * Lrn[1]; Lzn[2] = Lzn[1] * Lzn[1];
+#pragma unroll
+    for (int ip = 0; ip < 3; ip++)
+#pragma unroll
+      for (int n = 0; n <= ip; n++) {
+        double sum = 0;
+#pragma unroll
+        for (int j = 0; j < 9; j++) sum = __fma_rn (c_quad[mindx + j], st[j], sum);
+        mindx += 9;
+        cf[pindx++] = sum * (Lrn[n] * Lzn[ip - n]);
+      }
+  } else {
+    Lrn[0] = 1.0; Lzn[0] = 1.0;
+#pragma unroll
+    for (int ip = 0; ip < 3; ip++) {
+      Lrn[ip + 1] = Lrn[ip] * Lr;
+      Lzn[ip + 1] = Lzn[ip] * Lz;
+#pragma unroll
+      for (int n = 0; n <= ip; n++) {
+        double sum = 0;
+#pragma unroll
+        for (int j = 0; j < 9; j++) sum += c_quad[mindx++] * st[j];
+        cf[pindx++] = sum / Lrn[n] / Lzn[ip - n];
+      }
+    }
+  }
+  // interpol_apply + gen_apply (interpol2.c:190-241), masses: divide by r
+  const double r = ((double) ir + 0.5) * C.dr, z = ((double) iz + 0.5) * C.dz;
+  const double dr_ = r - ((double) pr + 0.5) * Lr, dz_ = z - ((double) pz + 0.5) * Lz;
+  double res;
+  if (dr_ == dz_)
+    res = cf[0] + dr_ * (cf[1] + cf[2] + dr_ * (cf[3] + cf[4] + cf[5]));
+  else
+    res = cf[0] + dz_ * (cf[1] + dz_ * cf[3]) + dr_ * (cf[2] + dz_ * cf[4] + dr_ * cf[5]);
+  C.arr (set, K_DENS, s)[C.off (ir - C.r0, iz - C.z0, it)] = res / r;
+}
+
 template <bool FAST>
 __global__ void
 k_interp (const PatchDesc *pd, const StripDesc *strips, int set)
@@ -298,76 +495,26 @@ k_interp (const PatchDesc *pd, const StripDesc *strips, int set)
   const StripDesc S = strips[blockIdx.y];
   const PatchDesc C = pd[S.child];
   const PatchDesc Pp = pd[C.parent];
-  const int pr0 = Pp.r0, pz0 = Pp.z0, pr1 = Pp.r0 + Pp.nr, pz1 = Pp.z0 + Pp.nz;
-  // grid_overlap (parent, strip, s_buff = 1, t_buff = 0), grid.c:145-198
-  const int left = max (S.sr0, (pr0 - 1) << 1), right = min (S.sr1, (pr1 + 1) << 1);
-  const int bottom = max (S.sz0, (pz0 - 1) << 1), top = min (S.sz1, (pz1 + 1) << 1);
-  if (left >= right || bottom >= top) return;
-  // map_interpol coarse range (mapper.c:199-210)
-  const int r0c = max (left >> 1, pr0 - 1), r1c = min (((right - 1) >> 1) + 1, pr1 + 1);
-  const int z0c = max (bottom >> 1, pz0 - 1), z1c = min (((top - 1) >> 1) + 1, pz1 + 1);
-  // fine cells written (interpol_inner, mapper.c:296-299)
-  const int fr0 = max (S.sr0 - 2, r0c << 1), fr1 = min (S.sr1 + 2, r1c << 1);
-  const int fz0 = max (S.sz0 - 2, z0c << 1), fz1 = min (S.sz1 + 2, z1c << 1);
-  const int wr = fr1 - fr0, wz = fz1 - fz0;
-  if (wr <= 0 || wz <= 0) return;
-  const int total = wr * wz * C.ntheta * C.ns;       // a strip's cells: far below 2^31
-  const double Lr = Pp.dr, Lz = Pp.dz;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-    const int q = i / wr, ir = fr0 + (i - q * wr);
-    const int q2 = q / wz, iz = fz0 + (q - q2 * wz);
-    const int s = q2 / C.ntheta, it = q2 - s * C.ntheta;
-    const int pr = ir >> 1, pz = iz >> 1;
-    // stay inside the ghost extents of child and parent
-    if (ir - C.r0 < -2 || ir - C.r0 >= C.nr + 2 || iz - C.z0 < -2 || iz - C.z0 >= C.nz + 2) continue;
-    if (pr - 1 - pr0 < -2 || pr + 1 - pr0 >= Pp.nr + 2 || pz - 1 - pz0 < -2 || pz + 1 - pz0 >= Pp.nz + 2) continue;
-    const double *pn = Pp.arr (set, K_DENS, s);
-    // interpol_set_stencil_at (interpol2.c:116-155)
-    double st[9];
-    for (int a = 0; a < 3; a++) {
-      const double r = ((double) (pr + a - 1) + 0.5) * Lr;
-      for (int b = 0; b < 3; b++)
-        st[a * 3 + b] = r * pn[Pp.off (pr + a - 1 - pr0, pz - 1 + b - pz0, it)];
-    }
-    // interpol_set_coeffs (interpol2.c:161-186)
-    double cf[6], Lrn[4], Lzn[4];
-    int pindx = 0, mindx = 0;
-    if (FAST) {
-      Lrn[0] = 1.0; Lzn[0] = 1.0;
-      Lrn[1] = 1.0 / Lr; Lzn[1] = 1.0 / Lz;
-      Lrn[2] = Lrn[1] * Lrn[1]; Lzn[2] = Lzn[1] * Lzn[1];
-#pragma unroll
-      for (int ip = 0; ip < 3; ip++)
-#pragma unroll
-        for (int n = 0; n <= ip; n++) {
-          double sum = 0;
-#pragma unroll
-          for (int j = 0; j < 9; j++) sum = __fma_rn (c_quad[mindx + j], st[j], sum);
-          mindx += 9;
-          cf[pindx++] = sum * (Lrn[n] * Lzn[ip - n]);
-        }
-    } else {
-      Lrn[0] = 1.0; Lzn[0] = 1.0;
-      for (int ip = 0; ip < 3; ip++) {
-        Lrn[ip + 1] = Lrn[ip] * Lr;
-        Lzn[ip + 1] = Lzn[ip] * Lz;
-        for (int n = 0; n <= ip; n++) {
-          double sum = 0;
-          for (int j = 0; j < 9; j++) sum += c_quad[mindx++] * st[j];
-          cf[pindx++] = sum / Lrn[n] / Lzn[ip - n];
-        }
-      }
-    }
-    // interpol_apply + gen_apply (interpol2.c:190-241), masses: divide by r
-    const double r = ((double) ir + 0.5) * C.dr, z = ((double) iz + 0.5) * C.dz;
-    const double dr_ = r - ((double) pr + 0.5) * Lr, dz_ = z - ((double) pz + 0.5) * Lz;
-    double res;
-    if (dr_ == dz_)
-      res = cf[0] + dr_ * (cf[1] + cf[2] + dr_ * (cf[3] + cf[4] + cf[5]));
-    else
-      res = cf[0] + dz_ * (cf[1] + dz_ * cf[3]) + dr_ * (cf[2] + dz_ * cf[4] + dr_ * cf[5]);
-    C.arr (set, K_DENS, s)[C.off (ir - C.r0, iz - C.z0, it)] = res / r;
-  }
+  const InterpGeom G = interp_geom (S, C, Pp);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G.total; i += gridDim.x * blockDim.x)
+    interp_item<FAST> (C, Pp, G, i, set);
+}
+
+constexpr int INTERP_THREADS = 256;
+constexpr int INTERP_PER_BLOCK = INTERP_THREADS;
+
+// The same over a flat list of work blocks (one item per thread).
+template <bool FAST>
+__global__ void __launch_bounds__ (INTERP_THREADS)
+k_interp_blk (const PatchDesc *pd, const StripDesc *strips, const WorkBlk *wb, int set)
+{
+  const WorkBlk W = wb[blockIdx.x];
+  const StripDesc S = strips[W.strip];
+  const PatchDesc C = pd[W.child];
+  const PatchDesc Pp = pd[W.parent];
+  const InterpGeom G = interp_geom (S, C, Pp);
+  const int i = W.first + threadIdx.x;
+  if (i < G.total) interp_item<FAST> (C, Pp, G, i, set);
 }
 
 // ---- A17: sibling matching (match_grids, cdr.c:1808-1882), as a gather
@@ -484,8 +631,16 @@ k_dmax (const Model M, const PatchDesc *pd, const int *plist, int set, DevState 
     const unsigned long long y = __shfl_xor_sync (0xffffffffu, km, o);
     km = y > km ? y : km;
   }
-  DevState *s = st + P.fam;
-  if ((threadIdx.x & 31) == 0 && km) atomicMax (&s->dmax_key[(s->step + slot_rel) & 1], km);
+  // one atomic per block: the warps' maxima meet in shared memory first
+  __shared__ unsigned long long wmax[32];
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if ((threadIdx.x & 31) == 0) wmax[w] = km;
+  __syncthreads ();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < nw; k++) km = wmax[k] > km ? wmax[k] : km;
+    DevState *s = st + P.fam;
+    if (km) atomicMax (&s->dmax_key[(s->step + slot_rel) & 1], km);
+  }
 }
 
 // Starts a step of every family: h from the reduced maxima (cfl_step), and

@@ -17,6 +17,17 @@
  * antisymmetric-ghost second difference) and a tridiagonal solve in r per mode.
  * The field is E = -grad phi on the staggered faces of src/grid.h:40-44:
  * er(i) on the face between cells i and i+1 (i = -1..nr-1), ez(j) likewise.
+ *
+ * On a 3-D grid the reference solves one Helmholtz problem per theta mode k
+ * (src/poisson.c:836-848: pois_solve_grid with lambda = -w2k[k]) through the
+ * modified hstcyl, whose diagonal is ELMBDA / r_i^2 + ES - 2/dr^2
+ * (fish90/src/hst_procs.f90:1539-1548); for lambda != 0 the axis is a
+ * Dirichlet side (src/poisson.c:446-447) whose coefficient vanishes at r = 0,
+ * so the operator is the same and only the ghost value behind the axis
+ * changes sign (phi(-1) = -phi(0)), which enters er on the axis face.
+ * oracle_poisson_mode adds elmbda / r_i^2 + es to the diagonal and takes that
+ * ghost; etheta of the mode is phi on the interior (etheta_copy,
+ * src/poisson.c:1162-1174), zero elsewhere.
  */
 #include <math.h>
 #include <stdlib.h>
@@ -25,8 +36,8 @@
 #define IDX(ir_, iz_) (((ir_) + 2) + ((iz_) + 2) * (nr + 4))
 
 int
-oracle_poisson_cyl (int nr, int nz, double dr, double dz,
-                    const double *charge, double *er, double *ez)
+oracle_poisson_mode (int nr, int nz, double dr, double dz, double elmbda, double es,
+                     const double *charge, double *er, double *ez, double *et)
 {
   double *S, *norm, *qh, *ph, *a, *b, *c, *cp, *dp, *phi;
   int i, j, k;
@@ -66,7 +77,7 @@ oracle_poisson_cyl (int nr, int nz, double dr, double dz,
       double ri = (i + 0.5) * dr, rm = i * dr, rp = (i + 1) * dr;
       a[i] = rm / (ri * dr * dr);
       c[i] = rp / (ri * dr * dr);
-      b[i] = -(a[i] + c[i]) + lam;
+      b[i] = -(a[i] + c[i]) + lam + (elmbda / (ri * ri) + es);
     }
     b[nr - 1] -= c[nr - 1];
     c[nr - 1] = 0.0;
@@ -93,7 +104,7 @@ oracle_poisson_cyl (int nr, int nz, double dr, double dz,
 #define PHI(i_, j_) phi[(i_) * nz + (j_)]
   for (j = 0; j < nz; j++)
     for (i = -1; i < nr; i++) {
-      double pl = (i < 0) ? PHI (0, j) : PHI (i, j);
+      double pl = (i < 0) ? (elmbda == 0.0 ? PHI (0, j) : -PHI (0, j)) : PHI (i, j);
       double pr = (i + 1 >= nr) ? -PHI (nr - 1, j) : PHI (i + 1, j);
       er[IDX (i, j)] = -(pr - pl) / dr;
     }
@@ -103,8 +114,33 @@ oracle_poisson_cyl (int nr, int nz, double dr, double dz,
       double pt = (j + 1 >= nz) ? -PHI (i, nz - 1) : PHI (i, j + 1);
       ez[IDX (i, j)] = -(pt - pb) / dz;
     }
+  if (et) {
+    memset (et, 0, sizeof (double) * (nr + 4) * (nz + 4));
+    for (j = 0; j < nz; j++)
+      for (i = 0; i < nr; i++) et[IDX (i, j)] = PHI (i, j);
+  }
 #undef PHI
   free (S); free (norm); free (qh); free (ph); free (a); free (b); free (c);
   free (cp); free (dp); free (phi);
   return 0;
+}
+
+int
+oracle_poisson_cyl (int nr, int nz, double dr, double dz,
+                    const double *charge, double *er, double *ez)
+{
+  return oracle_poisson_mode (nr, nz, dr, dz, 0.0, 0.0, charge, er, ez, NULL);
+}
+
+/* Every theta mode of a 3-D grid: planes 0 .. nt-1 at stride plen from the
+ * given plane-0 pointers, mode k with elmbda = -w2k[k], es = 0. */
+int
+oracle_poisson_modes (int nr, int nz, int nt, double dr, double dz, const double *w2k,
+                      const double *charge, double *er, double *ez, double *et, long plen)
+{
+  int k, r = 0;
+  for (k = 0; k < nt; k++)
+    r |= oracle_poisson_mode (nr, nz, dr, dz, -w2k[k], 0.0, charge + k * plen, er + k * plen,
+                              ez + k * plen, et + k * plen);
+  return r;
 }
