@@ -82,6 +82,12 @@ def port_lib():
         lib.port_model_size.restype = C.c_size_t
         lib.port_grid_size.restype = C.c_size_t
         lib.oracle_poisson_cyl.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, DP, DP, DP]
+        lib.oracle_poisson_mode.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                            C.c_double, DP, DP, DP, DP]
+        lib.oracle_dft_tables.argtypes = [C.c_int, DP, DP]
+        lib.oracle_r2hc.argtypes = [C.c_int, DP, C.c_long, DP, C.c_long, DP, DP]
+        lib.oracle_hc2r.argtypes = [C.c_int, DP, C.c_long, DP, C.c_long, DP, DP]
+        lib.oracle_wk.argtypes = [C.c_int, DP, DP]
         lib.port_advect_vec.argtypes = [C.c_double, C.c_double, DP, DP, DP, DP, C.c_double,
                                         C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]
         _port = lib
@@ -362,3 +368,46 @@ def poisson_field(nr: int, nz: int, dr: float, dz: float, charge: np.ndarray):
     ch = np.ascontiguousarray(charge, dtype=np.float64).reshape(nz + 4, nr + 4)
     lib.oracle_poisson_cyl(nr, nz, dr, dz, _dp(ch), _dp(er), _dp(ez))
     return er, ez
+
+
+def poisson_mode(nr: int, nz: int, dr: float, dz: float, elmbda: float, es: float,
+                 charge: np.ndarray):
+    """One Helmholtz mode of oracle/poisson_host.c: (er, ez, etheta = phi on
+    the interior) in rz layout."""
+    lib = port_lib()
+    er, ez, et = (np.zeros((nz + 4, nr + 4)) for _ in range(3))
+    ch = np.ascontiguousarray(charge, dtype=np.float64).reshape(nz + 4, nr + 4)
+    lib.oracle_poisson_mode(nr, nz, dr, dz, elmbda, es, _dp(ch), _dp(er), _dp(ez), _dp(et))
+    return er, ez, et
+
+
+def dft_tables(n: int):
+    """The twiddle table of oracle/dft_host.c: cos, sin of 2 pi m / n."""
+    lib = port_lib()
+    c, s = np.zeros(n), np.zeros(n)
+    lib.oracle_dft_tables(n, _dp(c), _dp(s))
+    return c, s
+
+
+def dft(x: np.ndarray, sign: int) -> np.ndarray:
+    """r2hc (sign > 0) or hc2r (sign < 0) of oracle/dft_host.c along the last axis."""
+    lib = port_lib()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = x.shape[-1]
+    c, s = dft_tables(n)
+    out = np.empty_like(x)
+    fn = lib.oracle_r2hc if sign > 0 else lib.oracle_hc2r
+    for i in np.ndindex(x.shape[:-1]):
+        xi = np.ascontiguousarray(x[i])
+        yi = np.empty(n)
+        fn(n, _dp(xi), 1, _dp(yi), 1, _dp(c), _dp(s))
+        out[i] = yi
+    return out
+
+
+def wk_tables(n: int):
+    """w2k, wk of a theta period of n planes (init_wk_a, src/cstream.c:309-344)."""
+    lib = port_lib()
+    w2k, wk = np.zeros(n), np.zeros(n)
+    lib.oracle_wk(n, _dp(w2k), _dp(wk))
+    return w2k, wk

@@ -69,14 +69,6 @@ void pois_init (void) {}
 void pois_free_r (pois_grid_t *g) { if (g) never ("pois_free_r(non-NULL)"); }
 double pois_inhom_er (double r, double z) { (void) r; (void) z; never ("pois_inhom_er"); return 0; }
 double pois_inhom_ez (double r, double z) { (void) r; (void) z; never ("pois_inhom_ez"); return 0; }
-void dft_transform (rz_array_t *in, rz_array_t *out, int sign)
-{ (void) in; (void) out; (void) sign; /* field is written per plane: identity */ }
-/* cdr_dft_field_r (cdr.c:408-424) turns the Poisson modes into the physical
- * field: transforms of er/ez and the theta derivative of etheta in Fourier
- * space.  The field stub already writes the physical er/ez/etheta, so the
- * whole round trip is the identity here. */
-void dft_diff (grid_t *g, rz_array_t *f) { (void) g; (void) f; }
-void dft_dens_perturb_r (cdr_grid_t *g, int s, double *e) { (void) g; (void) s; (void) e; never ("dft_dens_perturb_r"); }
 double spr_density_at (double a) { (void) a; never ("spr_density_at"); return 1.0; }
 void spr_hook (cdr_grid_t *g) { (void) g; never ("spr_hook"); }
 void spr_init (void) { never ("spr_init"); }
@@ -84,6 +76,9 @@ void spr_init (void) { never ("spr_init"); }
 /* ---- field seam ---- */
 int oracle_poisson_cyl (int nr, int nz, double dr_, double dz_,
                         const double *charge, double *er, double *ez);
+int oracle_poisson_modes (int nr, int nz, int nt, double dr_, double dz_, const double *w2k_,
+                          const double *charge, double *er, double *ez, double *et, long plen);
+void oracle_wk (int n, double *w2k_, double *wk_);
 
 #define MAX_GRIDS 4096
 static cdr_grid_t *grids[MAX_GRIDS];
@@ -91,6 +86,17 @@ static double *fixed_er[MAX_GRIDS], *fixed_ez[MAX_GRIDS], *fixed_et[MAX_GRIDS];
 static int n_grids = 0;
 static int field_mode = 0;   /* 0: zero, 1: fixed arrays, 2: host Poisson of root charge */
 static species_t species_store[16];
+
+/* src/dft.c, compiled against oracle/fftw_shim with these two renamed.
+ * cdr_calc_field_r (cdr.c:532-580) transforms the charge to theta modes,
+ * solves per mode and transforms the field back.  The fixed-field stub
+ * writes the physical er/ez/etheta, so there the round trip is the identity;
+ * with the field solved here per mode (field_mode 2) the reference's own
+ * dft_transform and dft_diff run. */
+void ref_dft_transform (rz_array_t *in, rz_array_t *out, int sign);
+void ref_dft_diff (grid_t *grid, rz_array_t *f);
+void dft_transform (rz_array_t *in, rz_array_t *out, int sign) { if (field_mode == 2) ref_dft_transform (in, out, sign); }
+void dft_diff (grid_t *g, rz_array_t *f) { if (field_mode == 2) ref_dft_diff (g, f); }
 static double *dr_store, *dz_store;
 
 static int
@@ -135,12 +141,24 @@ pois_solve_a (cdr_grid_t *cdr, pois_problem_t *prob)
 {
   pois_grid_t **modes;
   (void) prob;
-  if (field_mode == 2) {
-    if (cdr->ntheta != 1 || cdr->first_child != NULL) never ("poisson mode on a tree/3-D grid");
+  if (field_mode == 2 && cdr->ntheta == 1) {
+    if (cdr->first_child != NULL) never ("poisson mode on a tree");
     oracle_poisson_cyl (cdr->r1 - cdr->r0, cdr->z1 - cdr->z0,
                         dr[cdr->level], dz[cdr->level],
                         cdr->charge->data, cdr->er->data, cdr->ez->data);
     memset (cdr->etheta->data, 0, sizeof (double) * cdr->etheta->len);
+  } else if (field_mode == 2) {
+    /* one mode per theta plane (pois_solve_mode, src/poisson.c:836-848, with
+     * lambda = -w2k[mode]); the charge is already in theta modes
+     * (cdr_dft_charge_r) and cdr_dft_field_r transforms the field back */
+    if (cdr->first_child != NULL) never ("poisson mode on a tree");
+    oracle_poisson_modes (cdr->r1 - cdr->r0, cdr->z1 - cdr->z0, cdr->ntheta,
+                          dr[cdr->level], dz[cdr->level], w2k,
+                          RZTP (cdr->charge, cdr->r0 - 2, cdr->z0 - 2, 0),
+                          RZTP (cdr->er, cdr->r0 - 2, cdr->z0 - 2, 0),
+                          RZTP (cdr->ez, cdr->r0 - 2, cdr->z0 - 2, 0),
+                          RZTP (cdr->etheta, cdr->r0 - 2, cdr->z0 - 2, 0),
+                          (long) cdr->charge->strides[THETA_INDX]);
   } else {
     write_field_pair (cdr, field_root >= 0 ? grids[field_root] : cdr);
   }
@@ -187,6 +205,11 @@ ref_setup (double Lr, double Lz, int gr, int gz, int ntheta, int levels,
     dz_store[i] = dz_store[i - 1] / 2.0;
   }
   dtheta = twopi / max_ntheta;
+  /* init_wk_a (src/cstream.c:309-344) is static: the same arithmetic */
+  free (w2k); free (wk);
+  w2k = malloc (sizeof (double) * max_ntheta);
+  wk = malloc (sizeof (double) * max_ntheta);
+  oracle_wk (max_ntheta, w2k, wk);
 
   no_species = 0;
   reactions_list = NULL;
