@@ -181,7 +181,8 @@ class CdrTree:
 
     def set_field_poisson(self, on: bool = True):
         """Solve the field of every stage on the device (pois_solve_a,
-        poisson.c:763, one 2-D grid): no host round trip per stage."""
+        poisson.c:763, one grid; on a 3-D grid by theta modes, cdr.c:532-580):
+        no host round trip per stage."""
         check(self.L.arcos_set_field_poisson(self.h, 1 if on else 0))
 
     def solve_field(self, set: int = SET_GRID):

@@ -695,7 +695,7 @@ do_field_post (Ctx *c, int set)
   });
   if (r) return r;
   if ((r = do_periodic (c, set, 2))) return r;
-  // the device field solve writes E_theta = 0 on 2-D grids: nothing to refresh
+  // the device field solve fixed the E_theta flag when it was switched on
   return c->pois ? ARCOS_OK : refresh_stage_eabs (c);
 }
 
@@ -762,13 +762,23 @@ int
 device_poisson (Ctx *c, int set)
 {
   const PoisArgs &A = c->pois_args;
-  const int n = A.nr * A.nz;
+  const int n = A.nr * A.nz * A.nt;
   const int b = std::min ((n + 255) / 256, 8 * c->num_sms);
+  const int cells = (A.nr + 4) * (A.nz + 4);
+  const int bd = std::min ((cells + 127) / 128, 8 * c->num_sms);
+  if (A.nt > 1) k_theta_dft<0><<<bd, 128, 0, c->stream>>> (c->pd_d, 0, set, K_CHARGE, A);   // cdr_dft_charge_r
   k_pois_fwd<<<b, 256, 0, c->stream>>> (c->pd_d, 0, set, A);
-  k_pois_tri<<<(A.nz + 127) / 128, 128, 0, c->stream>>> (A);
+  k_pois_tri<<<(A.nz * A.nt + 127) / 128, 128, 0, c->stream>>> (A);
   k_pois_inv<<<b, 256, 0, c->stream>>> (A);
-  const long long len = (long long) (A.nz + 4) * c->pd_h[0].pitch;
-  k_pois_field<<<(int) std::min<long long> ((len + 255) / 256, 8 * c->num_sms), 256, 0, c->stream>>> (c->pd_d, 0, set, A);
+  // set 1 is the RK2 intermediate grid, fresh every step in the reference
+  const int fresh = set == 1;
+  const long long len = (long long) (A.nz + 4) * c->pd_h[0].pitch * (A.nt + (fresh && A.nt > 1 ? 4 : 0));
+  k_pois_field<<<(int) std::min<long long> ((len + 255) / 256, 8 * c->num_sms), 256, 0, c->stream>>> (c->pd_d, 0, set, A, fresh);
+  if (A.nt > 1) {                               // cdr_dft_field_r
+    k_theta_dft<1><<<bd, 128, 0, c->stream>>> (c->pd_d, 0, set, K_ER, A);
+    k_theta_dft<1><<<bd, 128, 0, c->stream>>> (c->pd_d, 0, set, K_EZ, A);
+    k_theta_dft<2><<<bd, 128, 0, c->stream>>> (c->pd_d, 0, set, K_ETHETA, A);
+  }
   CKL ();
   return do_field_post (c, set);
 }
@@ -2158,13 +2168,46 @@ arcos_set_field_poisson (void *ctx, int on)
   if (r) return r;
   drop_graphs (c);
   if (!on) { c->pois = false; return ARCOS_OK; }
-  if (c->pd_h.size () != 1 || !c->fused_ok || c->pd_h[0].ntheta != 1)
-    return fail (ARCOS_ERR_ARG, "the device field solve takes one 2-D grid with every side external");
+  if (c->pd_h.size () != 1 || !c->fused_ok || c->pd_h[0].ntheta > 64)
+    return fail (ARCOS_ERR_ARG, "the device field solve takes one grid (at most 64 theta planes) with every side external");
   if (c->fn) return fail (ARCOS_ERR_STATE, "a field callback is set (arcos_set_field_fn (ctx, NULL, NULL) first)");
   const PatchDesc &P = c->pd_h[0];
-  const int nr = P.nr, nz = P.nz;
+  const int nr = P.nr, nz = P.nz, nt = P.ntheta;
   const double dr = P.dr, dz = P.dz, pi = 3.14159265358979323846;
   std::vector<double> St ((size_t) nz * nz), norm (nz, 0.0), lam (nz), ta (nr), tc (nr);
+  // theta modes: w2k and wk of init_wk_a (src/cstream.c:309-344), the
+  // Helmholtz diagonal terms elmbda_m / r_i^2 + es with elmbda_m = -w2k[m]
+  // and es = 0 (pois_solve_mode, src/poisson.c:847), the twiddles of the
+  // theta transforms (cos, sin of 2 pi q / nt)
+  std::vector<double> w2k (nt, 0.0), wk (nt, 0.0), elm (nt), mk ((size_t) nt * nr), tcs (nt), tsn (nt);
+  {
+    const double dtheta = 6.283185307179586477 / nt, twobydtheta2 = 2. / (dtheta * dtheta);
+    int k;
+    for (k = 0; k < nt / 2 + (nt % 2); k++) {
+      const double w2k_ = twobydtheta2 * (1 - cos (k * dtheta));
+      const double re_wk = (cos (k * dtheta) - 1) / dtheta, im_wk = sin (k * dtheta) / dtheta;
+      wk[k] = re_wk;
+      w2k[k] = w2k_;
+      if (k != 0) {
+        wk[nt - k] = im_wk;
+        w2k[nt - k] = w2k_;
+      }
+    }
+    if ((nt % 2) == 0) {
+      w2k[nt / 2] = twobydtheta2 * (1 - cos (k * dtheta));
+      wk[nt / 2] = (cos (k * dtheta) - 1) / dtheta;
+    }
+    if (nt == 1) { w2k[0] = 0.0; wk[0] = 0.0; }
+    for (int m = 0; m < nt; m++) {
+      elm[m] = -w2k[m];
+      for (int i = 0; i < nr; i++) {
+        const double ri = (i + 0.5) * dr;
+        mk[(size_t) m * nr + i] = elm[m] / (ri * ri) + 0.0;
+      }
+      tcs[m] = cos (6.283185307179586477 * m / nt);
+      tsn[m] = sin (6.283185307179586477 * m / nt);
+    }
+  }
   for (int k = 0; k < nz; k++)
     for (int j = 0; j < nz; j++) {
       const double v = sin (pi * (k + 1) * (j + 0.5) / nz);
@@ -2180,19 +2223,24 @@ arcos_set_field_poisson (void *ctx, int on)
     ta[i] = rm / (ri * dr * dr);
     tc[i] = rp / (ri * dr * dr);
   }
-  const size_t nn = (size_t) nr * nz;
-  const size_t total = St.size () + 3 * (size_t) nz + 2 * (size_t) nr + 5 * nn;
+  const size_t nn = (size_t) nr * nz * nt;
+  const size_t total = St.size () + 3 * (size_t) nz + 2 * (size_t) nr + mk.size () + 4 * (size_t) nt + 5 * nn;
   cudaFree (c->pois_d);
   c->pois_d = nullptr;
   CK (cudaMalloc (&c->pois_d, sizeof (double) * total));
   double *q = c->pois_d;
   PoisArgs &A = c->pois_args;
-  A.nr = nr; A.nz = nz; A.dr = dr; A.dz = dz;
+  A.nr = nr; A.nz = nz; A.nt = nt; A.r0 = P.r0; A.dr = dr; A.dz = dz;
   A.St = q; q += St.size ();
   A.norm = q; q += nz;
   A.lam = q; q += nz;
   A.ta = q; q += nr;
   A.tc = q; q += nr;
+  A.mk = q; q += mk.size ();
+  A.elm = q; q += nt;
+  A.tcos = q; q += nt;
+  A.tsin = q; q += nt;
+  A.wk = q; q += nt;
   A.qh = q; q += nn;
   A.ph = q; q += nn;
   A.cp = q; q += nn;
@@ -2203,6 +2251,13 @@ arcos_set_field_poisson (void *ctx, int on)
   CK (cudaMemcpy ((void *) A.lam, lam.data (), sizeof (double) * nz, cudaMemcpyHostToDevice));
   CK (cudaMemcpy ((void *) A.ta, ta.data (), sizeof (double) * nr, cudaMemcpyHostToDevice));
   CK (cudaMemcpy ((void *) A.tc, tc.data (), sizeof (double) * nr, cudaMemcpyHostToDevice));
+  CK (cudaMemcpy ((void *) A.mk, mk.data (), sizeof (double) * mk.size (), cudaMemcpyHostToDevice));
+  CK (cudaMemcpy ((void *) A.elm, elm.data (), sizeof (double) * nt, cudaMemcpyHostToDevice));
+  CK (cudaMemcpy ((void *) A.tcos, tcs.data (), sizeof (double) * nt, cudaMemcpyHostToDevice));
+  CK (cudaMemcpy ((void *) A.tsin, tsn.data (), sizeof (double) * nt, cudaMemcpyHostToDevice));
+  CK (cudaMemcpy ((void *) A.wk, wk.data (), sizeof (double) * nt, cudaMemcpyHostToDevice));
+  // a 3-D solve gives E_theta != 0: the stage kernels read |E| from memory
+  if (nt > 1) c->stage_eabs = 1;
   c->pois = true;
   return ARCOS_OK;
 }

@@ -21,99 +21,140 @@
 // every element of er and ez (ghosts included: zero off the faces).  The
 // work is O(nr nz^2) fused multiply-adds; at the field-in-the-loop
 // configuration (128 x 256) a few microseconds.
+//
+// On a 3-D grid (cdr_calc_field_r, src/cdr.c:532-580) the charge first goes
+// to theta modes in place (dft_transform r2hc, src/dft.c:37-88), every mode
+// m is one Helmholtz problem of the same operator plus elmbda_m / r_i^2 on the
+// diagonal (pois_solve_mode, src/poisson.c:836-848, lambda = -w2k[m]; the
+// modified hstcyl adds ELMBDA / r^2 + ES, fish90/src/hst_procs.f90:1539-1548)
+// with the ghost behind the axis antisymmetric for elmbda != 0 (a Dirichlet
+// axis, src/poisson.c:446-447), etheta of the mode is phi on the interior
+// (etheta_copy, src/poisson.c:1162-1174), and the field comes back by hc2r of
+// er and ez and dft_diff + hc2r of etheta (cdr_dft_field_r, src/cdr.c:408-424).
+// The theta transforms are FFTW's r2hc / hc2r definitions evaluated as
+// direct sums with host twiddle tables, in the same order as the host
+// restatement; ntheta is at most 64, so a thread holds one element's theta
+// column.  All modes are solved in the same four launches.
 #pragma once
 #include "device_common.cuh"
 
 namespace arcos {
 
 struct PoisArgs {
-  int nr, nz;
+  int nr, nz, nt;        // nt theta modes (1 on a 2-D grid)
+  int r0;                // the grid's first column (r of column c: (c + r0 + 1/2) dr)
   double dr, dz;
   const double *St;      // [j][k] = sin(pi (k+1) (j+1/2) / nz)
   const double *norm;    // [k] = sum_j S[k][j]^2
   const double *lam;     // [k] = -4/dz^2 sin^2(pi (k+1) / (2 nz))
   const double *ta, *tc; // [i] = r_{i-1/2} / (r_i dr^2), r_{i+1/2} / (r_i dr^2)
-  double *qh, *ph, *cp, *dp, *phi;   // [i][k] (phi: [i][j]) scratch, nr * nz each
+  const double *mk;      // [m][i] = elmbda_m / r_i^2 + es, elmbda_m = -w2k[m]
+  const double *elm;     // [m] = elmbda_m
+  const double *tcos, *tsin;   // [q] = cos, sin (2 pi q / nt): the theta twiddles
+  const double *wk;      // [m]: the theta derivative factors (init_wk_a)
+  double *qh, *ph, *cp, *dp, *phi;   // [m][i][k] (phi: [m][i][j]) scratch, nt * nr * nz each
 };
 
-// qh[i][k] = (sum_j -charge(i, j) S[k][j]) / norm[k]
+// qh[m][i][k] = (sum_j -charge_m(i, j) S[k][j]) / norm[k]
 __global__ void
 k_pois_fwd (const PatchDesc *__restrict__ pd, int patch, int set, PoisArgs A)
 {
   const PatchDesc &P = pd[patch];
-  const int n = A.nr * A.nz;
+  const int nn = A.nr * A.nz, n = nn * A.nt;
   const double *ch = P.arr (set, K_CHARGE);
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int i = t / A.nz, k = t - i * A.nz;
+    const int m = t / nn, u = t - m * nn;
+    const int i = u / A.nz, k = u - i * A.nz;
     double s = 0.0;
-    for (int j = 0; j < A.nz; j++) s += -ch[P.off (i, j, 0)] * A.St[(size_t) j * A.nz + k];
+    for (int j = 0; j < A.nz; j++) s += -ch[P.off (i, j, m)] * A.St[(size_t) j * A.nz + k];
     A.qh[t] = s / A.norm[k];
   }
 }
 
-// One z mode per thread: the tridiagonal system in r (Thomas algorithm).
+// One (theta mode, z mode) per thread: the tridiagonal system in r (Thomas).
 __global__ void
 k_pois_tri (PoisArgs A)
 {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= A.nz) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= A.nz * A.nt) return;
   const int nr = A.nr, nz = A.nz;
+  const int m = t / nz, k = t - m * nz;
+  const size_t base = (size_t) m * nr * nz;
   const double lam = A.lam[k];
+  const double *mk = A.mk + (size_t) m * nr;
   auto bcoef = [&] (int i) {
-    double b = -(A.ta[i] + A.tc[i]) + lam;
+    double b = -(A.ta[i] + A.tc[i]) + lam + mk[i];
     if (i == nr - 1) b -= A.tc[i];       // phi_{nr} = -phi_{nr-1} (Dirichlet at r = L_r)
     return b;
   };
   const double b0 = bcoef (0);
   double cpv = (nr - 1 == 0 ? 0.0 : A.tc[0]) / b0;
-  double dpv = A.qh[k] / b0;
-  A.cp[k] = cpv;
-  A.dp[k] = dpv;
+  double dpv = A.qh[base + k] / b0;
+  A.cp[base + k] = cpv;
+  A.dp[base + k] = dpv;
   for (int i = 1; i < nr; i++) {
-    const double m = bcoef (i) - A.ta[i] * cpv;
-    cpv = (i == nr - 1 ? 0.0 : A.tc[i]) / m;
-    dpv = (A.qh[(size_t) i * nz + k] - A.ta[i] * dpv) / m;
-    A.cp[(size_t) i * nz + k] = cpv;
-    A.dp[(size_t) i * nz + k] = dpv;
+    const double mm = bcoef (i) - A.ta[i] * cpv;
+    cpv = (i == nr - 1 ? 0.0 : A.tc[i]) / mm;
+    dpv = (A.qh[base + (size_t) i * nz + k] - A.ta[i] * dpv) / mm;
+    A.cp[base + (size_t) i * nz + k] = cpv;
+    A.dp[base + (size_t) i * nz + k] = dpv;
   }
   double p = dpv;
-  A.ph[(size_t) (nr - 1) * nz + k] = p;
+  A.ph[base + (size_t) (nr - 1) * nz + k] = p;
   for (int i = nr - 2; i >= 0; i--) {
-    p = A.dp[(size_t) i * nz + k] - A.cp[(size_t) i * nz + k] * p;
-    A.ph[(size_t) i * nz + k] = p;
+    p = A.dp[base + (size_t) i * nz + k] - A.cp[base + (size_t) i * nz + k] * p;
+    A.ph[base + (size_t) i * nz + k] = p;
   }
 }
 
-// phi[i][j] = sum_k ph[i][k] S[k][j]
+// phi[m][i][j] = sum_k ph[m][i][k] S[k][j]
 __global__ void
 k_pois_inv (PoisArgs A)
 {
-  const int n = A.nr * A.nz;
+  const int nn = A.nr * A.nz, n = nn * A.nt;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int i = t / A.nz, j = t - i * A.nz;
+    const int m = t / nn, u = t - m * nn;
+    const int i = u / A.nz, j = u - i * A.nz;
+    const double *ph = A.ph + (size_t) m * nn + (size_t) i * A.nz;
     double s = 0.0;
-    for (int k = 0; k < A.nz; k++) s += A.ph[(size_t) i * A.nz + k] * A.St[(size_t) j * A.nz + k];
+    for (int k = 0; k < A.nz; k++) s += ph[k] * A.St[(size_t) j * A.nz + k];
     A.phi[t] = s;
   }
 }
 
 // er(i, j) on the face between cells i and i+1 (i = -1 .. nr-1), ez(i, j)
-// between rows j and j+1 (j = -1 .. nz-1); every other element 0; etheta 0.
+// between rows j and j+1 (j = -1 .. nz-1), every other element 0, on plane m
+// of each theta mode; etheta of the mode phi on the interior (0 on a 2-D
+// grid).  With `fresh` (the RK2 intermediate grid, which the reference
+// allocates zeroed every step, cdr_like_a src/cdr.c:211-226) the four theta
+// ghost planes are zeroed too: cdr_calc_eabs reads etheta of plane -1 before
+// cdr_set_periodic refills it (src/cdr.c:560-566).
 __global__ void
-k_pois_field (const PatchDesc *__restrict__ pd, int patch, int set, PoisArgs A)
+k_pois_field (const PatchDesc *__restrict__ pd, int patch, int set, PoisArgs A, int fresh)
 {
   const PatchDesc &P = pd[patch];
   const int nr = A.nr, nz = A.nz;
-  double *er = P.arr (set, K_ER), *ez = P.arr (set, K_EZ), *et = P.arr (set, K_ETHETA);
   const long long len = (long long) (nz + 4) * P.pitch;
-  auto PHI = [&] (int i, int j) { return A.phi[(size_t) i * nz + j]; };
-  for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < len;
+  const int g = (fresh && A.nt > 1) ? 2 : 0;          // ghost planes each side
+  for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < len * (A.nt + 2 * g);
        t += (long long) gridDim.x * blockDim.x) {
-    const int row = (int) (t / P.pitch), col = (int) (t - (long long) row * P.pitch);
+    const int m = (int) (t / len) - g;
+    const long long e = t - (long long) (m + g) * len;
+    if (m < 0 || m >= A.nt) {
+      const long long o = (long long) (m - P.theta0) * P.plane_stride + e;
+      P.arr (set, K_ER)[o] = 0.0;
+      P.arr (set, K_EZ)[o] = 0.0;
+      P.arr (set, K_ETHETA)[o] = 0.0;
+      continue;
+    }
+    const double *phm = A.phi + (size_t) m * nr * nz;
+    auto PHI = [&] (int i, int j) { return phm[(size_t) i * nz + j]; };
+    const bool sym = A.elm[m] == 0.0;
+    const int row = (int) (e / P.pitch), col = (int) (e - (long long) row * P.pitch);
     const int i = col - 2, j = row - 2;
-    double vr = 0.0, vz = 0.0;
+    double vr = 0.0, vz = 0.0, vt = 0.0;
     if (j >= 0 && j < nz && i >= -1 && i < nr) {
-      const double pl = (i < 0) ? PHI (0, j) : PHI (i, j);
+      const double pl = (i < 0) ? (sym ? PHI (0, j) : -PHI (0, j)) : PHI (i, j);
       const double pr = (i + 1 >= nr) ? -PHI (nr - 1, j) : PHI (i + 1, j);
       vr = -(pr - pl) / A.dr;
     }
@@ -122,9 +163,68 @@ k_pois_field (const PatchDesc *__restrict__ pd, int patch, int set, PoisArgs A)
       const double pt = (j + 1 >= nz) ? -PHI (i, nz - 1) : PHI (i, j + 1);
       vz = -(pt - pb) / A.dz;
     }
-    er[t] = vr;
-    ez[t] = vz;
-    et[t] = 0.0;
+    if (A.nt > 1 && j >= 0 && j < nz && i >= 0 && i < nr) vt = PHI (i, j);
+    const long long o = (long long) (m - P.theta0) * P.plane_stride + e;
+    P.arr (set, K_ER)[o] = vr;
+    P.arr (set, K_EZ)[o] = vz;
+    P.arr (set, K_ETHETA)[o] = vt;
+  }
+}
+
+// ---- theta transforms of one array, every element of the (nr+4) x (nz+4)
+// rows of planes 0 .. nt-1: r2hc (WHAT 0), hc2r (WHAT 1), or dft_diff then
+// hc2r (WHAT 2), each as the host restatement sums them ----
+template <int WHAT>
+__global__ void
+k_theta_dft (const PatchDesc *__restrict__ pd, int patch, int set, int kind, PoisArgs A)
+{
+  const PatchDesc &P = pd[patch];
+  const int n = A.nt, w = A.nr + 4;
+  const int cells = w * (A.nz + 4);
+  double *a = P.arr (set, kind) + (long long) (0 - P.theta0) * P.plane_stride;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+    const int row = c / w, col = c - row * w;
+    double *e = a + (long long) row * P.pitch + col;
+    double t[64];
+    for (int j = 0; j < n; j++) t[j] = e[(long long) j * P.plane_stride];
+    if (WHAT == 0) {
+      for (int k = 0; k <= n / 2; k++) {
+        double re = 0.0;
+        for (int j = 0; j < n; j++) re += t[j] * A.tcos[(j * k) % n];
+        e[(long long) k * P.plane_stride] = re;
+      }
+      for (int k = 1; k < (n + 1) / 2; k++) {
+        double im = 0.0;
+        for (int j = 0; j < n; j++) im += t[j] * A.tsin[(j * k) % n];
+        e[(long long) (n - k) * P.plane_stride] = -im;
+      }
+      continue;
+    }
+    if (WHAT == 2) {                      // dft_diff (src/dft.c:92-128)
+      const double r = ((double) (col - 2 + A.r0) + 0.5) * A.dr;
+      for (int k = 0; k < n / 2 + 1; k++) {
+        if (k < n / 2) {
+          double re, im, re_f, im_f;
+          re_f = t[k];
+          im_f = (k == 0 ? 0 : t[n - k]);
+          re = re_f * A.wk[k] - (k == 0 ? 0 : im_f * A.wk[n - k]);
+          im = (k == 0 ? 0 : re_f * A.wk[n - k] + im_f * A.wk[k]);
+          t[k] = re / r;
+          if (k != 0) t[n - k] = im / r;
+        } else if ((n % 2) == 0) {
+          t[k] = A.wk[k] * t[k] / r;
+        }
+      }
+    }
+    for (int j = 0; j < n; j++) {         // hc2r
+      double acc = t[0];
+      for (int k = 1; k < (n + 1) / 2; k++) {
+        const int q = (j * k) % n;
+        acc += 2.0 * (t[k] * A.tcos[q] - t[n - k] * A.tsin[q]);
+      }
+      if (n % 2 == 0) acc += t[n / 2] * A.tcos[(j * (n / 2)) % n];
+      e[(long long) j * P.plane_stride] = acc;
+    }
   }
 }
 

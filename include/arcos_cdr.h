@@ -133,12 +133,17 @@ typedef int (*arcos_field_fn) (void *user, int stage, const double *charge,
                                double *er, double *ez, double *etheta);
 int arcos_set_field_fn (void *ctx, arcos_field_fn fn, void *user);
 /* The field solve of pois_solve_a (src/poisson.c:763-767, FISHPACK hstcyl,
- * fish90/src/hst_procs.f90:1439) on the device, for one 2-D grid with every
+ * fish90/src/hst_procs.f90:1439) on the device, for one grid with every
  * side external: the 5-point cylindrical operator, regular axis, Dirichlet
  * conditions on r = L_r, z = 0, z = L_z, solved by a sine transform in z and
- * a tridiagonal solve in r per mode.  When on (1), every stage of arcos_run
- * and arcos_cdr_rk2 solves the field from the current charge with no host
- * round trip (arcos_run replays the whole step from a CUDA graph).  Excludes
+ * a tridiagonal solve in r per mode.  On a 3-D grid (at most 64 theta
+ * planes) the charge goes to theta modes (FFTW r2hc, src/dft.c:37-88), each
+ * mode is a Helmholtz problem with lambda = -w2k[m] (src/poisson.c:836-848),
+ * and the field comes back with hc2r and, for etheta, dft_diff
+ * (src/cdr.c:408-424); the charge of the set is left in theta modes, as the
+ * reference leaves it.  When on (1), every stage of arcos_run and
+ * arcos_cdr_rk2 solves the field from the current charge with no host round
+ * trip (arcos_run replays the whole step from a CUDA graph).  Excludes
  * arcos_set_field_fn. */
 int arcos_set_field_poisson (void *ctx, int on);
 /* One device field solve of storage set `set` from its current charge, then

@@ -88,6 +88,8 @@ def port_lib():
         lib.oracle_r2hc.argtypes = [C.c_int, DP, C.c_long, DP, C.c_long, DP, DP]
         lib.oracle_hc2r.argtypes = [C.c_int, DP, C.c_long, DP, C.c_long, DP, DP]
         lib.oracle_wk.argtypes = [C.c_int, DP, DP]
+        lib.oracle_theta_field.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                           DP, DP, DP, DP, C.c_long]
         lib.port_advect_vec.argtypes = [C.c_double, C.c_double, DP, DP, DP, DP, C.c_double,
                                         C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]
         _port = lib
@@ -411,3 +413,20 @@ def wk_tables(n: int):
     w2k, wk = np.zeros(n), np.zeros(n)
     lib.oracle_wk(n, _dp(w2k), _dp(wk))
     return w2k, wk
+
+
+def theta_field(nr: int, nz: int, nt: int, dr: float, dz: float, charge: np.ndarray):
+    """The field solve of a 3-D root grid by theta modes (oracle/poisson_host.c
+    oracle_theta_field), before the external field: returns (charge in theta
+    modes, er, ez, etheta), each (nt + 4, nz + 4, nr + 4) with the ghost planes
+    of the field zero."""
+    lib = port_lib()
+    shape = (nt + 4, nz + 4, nr + 4)
+    ch = np.ascontiguousarray(charge, dtype=np.float64).reshape(shape).copy()
+    er, ez, et = (np.zeros(shape) for _ in range(3))
+    plen = (nz + 4) * (nr + 4)
+    o = 2 * plen
+    def p(a):                                   # pointer to plane 0
+        return C.cast(a.ctypes.data + 8 * o, DP)
+    lib.oracle_theta_field(nr, nz, nt, 0, dr, dz, p(ch), p(er), p(ez), p(et), plen)
+    return ch, er, ez, et

@@ -705,11 +705,8 @@ nonegative_r (const port_model *m, port_grid *g)
  * etheta). ---- */
 int oracle_poisson_cyl (int nr, int nz, double dr, double dz,
                         const double *charge, double *er, double *ez);
-int oracle_poisson_modes (int nr, int nz, int nt, double dr, double dz, const double *w2k,
-                          const double *charge, double *er, double *ez, double *et, long plen);
-void oracle_dft_array (int n, double *a, long plen, int sign);
-void oracle_wk (int n, double *w2k, double *wk);
-void oracle_dft_diff (int n, int nr, int nz, int r0, double dr, double *f, long plen, const double *wk);
+int oracle_theta_field (int nr, int nz, int nt, int r0, double dr, double dz,
+                        double *charge, double *er, double *ez, double *et, long plen);
 
 static void
 write_field_pair (const port_model *m, port_grid *g, const port_grid *tmpl)
@@ -747,18 +744,10 @@ port_calc_field (const port_model *m, port_grid *root, const port_grid *tmpl)
                         m->dz[root->level], root->charge, root->er, root->ez);
     memset (root->etheta, 0, alen (root) * sizeof (double));
   } else if (m->field_mode == 2) {
-    const int nt = root->ntheta, nr = root->r1 - root->r0, nz = root->z1 - root->z0;
     const long pl = plen (root), o = 2 * pl;            /* plane 0 of a 3-D array */
-    const double dr = m->dr[root->level], dz = m->dz[root->level];
-    double w2k[256], wk[256];
-    oracle_wk (nt, w2k, wk);
-    oracle_dft_array (nt, root->charge + o, pl, 1);
-    oracle_poisson_modes (nr, nz, nt, dr, dz, w2k, root->charge + o, root->er + o,
-                          root->ez + o, root->etheta + o, pl);
-    oracle_dft_array (nt, root->er + o, pl, -1);
-    oracle_dft_array (nt, root->ez + o, pl, -1);
-    oracle_dft_diff (nt, nr, nz, root->r0, dr, root->etheta + o, pl, wk);
-    oracle_dft_array (nt, root->etheta + o, pl, -1);
+    oracle_theta_field (root->r1 - root->r0, root->z1 - root->z0, root->ntheta, root->r0,
+                        m->dr[root->level], m->dz[root->level], root->charge + o,
+                        root->er + o, root->ez + o, root->etheta + o, pl);
   } else {
     write_field_pair (m, root, tmpl);
   }

@@ -144,3 +144,30 @@ oracle_poisson_modes (int nr, int nz, int nt, double dr, double dz, const double
                               ez + k * plen, et + k * plen);
   return r;
 }
+
+void oracle_dft_array (int n, double *a, long plen, int sign);
+void oracle_wk (int n, double *w2k, double *wk);
+void oracle_dft_diff (int n, int nr, int nz, int r0, double dr, double *f, long plen, const double *wk);
+
+/* The whole field solve of a 3-D root grid as cdr_calc_field_r performs it up
+ * to the external field (src/cdr.c:538-545): the charge to theta modes in
+ * place (cdr_dft_charge_r, src/cdr.c:393-404), one mode solve per plane, the
+ * field back (cdr_dft_field_r, src/cdr.c:408-424: er, ez, dft_diff and the
+ * transform of etheta).  Planes 0 .. nt-1 at stride plen from the plane-0
+ * pointers. */
+int
+oracle_theta_field (int nr, int nz, int nt, int r0, double dr, double dz,
+                    double *charge, double *er, double *ez, double *et, long plen)
+{
+  double w2k[256], wk[256];
+  int r;
+  if (nt < 2 || nt > 256) return 1;
+  oracle_wk (nt, w2k, wk);
+  oracle_dft_array (nt, charge, plen, 1);
+  r = oracle_poisson_modes (nr, nz, nt, dr, dz, w2k, charge, er, ez, et, plen);
+  oracle_dft_array (nt, er, plen, -1);
+  oracle_dft_array (nt, ez, plen, -1);
+  oracle_dft_diff (nt, nr, nz, r0, dr, et, plen, wk);
+  oracle_dft_array (nt, et, plen, -1);
+  return r;
+}
