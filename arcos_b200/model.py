@@ -88,9 +88,28 @@ class Params:
 
 
 @dataclass
+class PhotoTerm:
+    """One term of the photoionization file (photo_load_file,
+    src/photo.c:373-400): the source weight A and the Helmholtz shift lambda
+    (passed as ES to the solver, src/photo.c:296-305)."""
+    A: float
+    lam: float
+
+
+@dataclass
 class KineticModel:
     species: List[Species] = field(default_factory=list)
     reactions: List[Reaction] = field(default_factory=list)
+    # Photoionization (has_photoionization, src/rt.c:38-47): terms in file
+    # order (photo_calc visits them last-first, photo_register prepends,
+    # src/photo.c:174-185); the source species ("dummyplus", whose d_dens is
+    # the impact ionization rate), and the two species that receive A * photo
+    # ("electrons" and "xplus", src/photo.c:268-291).  The photo entry ends
+    # the reactions list.
+    photo: List[PhotoTerm] = field(default_factory=list)
+    photo_source: int = -1
+    photo_electrons: int = 0
+    photo_ions: int = -1
 
     @property
     def no_species(self) -> int:

@@ -18,7 +18,7 @@ from typing import List, Optional, Sequence, Tuple
 import numpy as np
 
 from .grids import GridSpec, inherit_ext_bound
-from .model import KineticModel, Params, Reaction, Species, minimal_model
+from .model import KineticModel, Params, PhotoTerm, Reaction, Species, minimal_model
 from .react_table import ReactTable, log_uniform_table
 
 
@@ -127,6 +127,48 @@ def plain(nr: int = 128, nz: int = 256, ntheta: int = 1, L_r: float = 2.0, L_z: 
     rng = np.random.default_rng(seed)
     dens = [[seed_dens(spec, params, rng, noise=noise, theta_mod=ntheta > 1)
              for _ in range(model.no_species)]]
+    if field == "wavy":
+        fields = [wavy_field(spec, params, seed=seed + 1000)]
+    elif field == "uniform":
+        fields = [uniform_field(spec)]
+    else:
+        raise ValueError(f"unknown field {field!r}")
+    return Problem(params, model, [spec], dens, fields)
+
+
+def photo_model(points: int = 256, terms: Sequence[Tuple[float, float]] = ((0.02, -0.8), (0.05, -6.0))
+                ) -> KineticModel:
+    """The minimal model with photoionization as the reference's kinetic
+    reader sets it up (src/rt.c:38-47): electrons, positive ions, the
+    counter pair of impact ionization ("dummyplus", the photo source, and
+    "dummyminus" to keep the charge balance; react_apply updates charged
+    species only, reaction.c:151-153) and the photo ions ("xplus"); impact
+    ionization e -> 2e + ion + dummyplus + dummyminus; photo terms (A,
+    lambda) in file order."""
+    table = log_uniform_table(lambda E: E * math.exp(-1.0 / E), 0.05, 20.0, points)
+    return KineticModel(
+        species=[Species("electrons", -1.0, 1.0), Species("ions", 1.0, 0.0),
+                 Species("dummyplus", 1.0, 0.0), Species("dummyminus", -1.0, 0.0),
+                 Species("xplus", 1.0, 0.0)],
+        reactions=[Reaction(inputs=[0], outputs=[0, 0, 1, 2, 3], table=table)],
+        photo=[PhotoTerm(a, lam) for a, lam in terms],
+        photo_source=2, photo_electrons=0, photo_ions=4)
+
+
+def photo(nr: int = 128, nz: int = 256, ntheta: int = 1, seed: int = 0, noise: float = 0.0,
+          field: str = "uniform", terms: Sequence[Tuple[float, float]] = ((0.02, -0.8), (0.05, -6.0))
+          ) -> Problem:
+    """A single grid with ``photo_model``: a seeded electron/ion cloud, the
+    counter and photo species starting at zero, uniform Ez = -1 or the wavy
+    field."""
+    params = Params(L_r=2.0, L_z=4.0, gridpoints_r=nr, gridpoints_z=nz, max_ntheta=ntheta,
+                    E0_z=-1.0, nu_a=0.5, nu_d=0.5, nu_rt=0.5, diffusion_coeff=0.1,
+                    warn_min_timestep=1e-12, max_levels=4)
+    model = photo_model(terms=terms)
+    spec = GridSpec(0, 0, nr, nz, ntheta=ntheta, level=0, ext_bound=15, parent=-1)
+    rng = np.random.default_rng(seed)
+    dens = [[seed_dens(spec, params, rng, noise=noise, theta_mod=ntheta > 1) for _ in range(2)]
+            + [spec.zeros() for _ in range(3)]]
     if field == "wavy":
         fields = [wavy_field(spec, params, seed=seed + 1000)]
     elif field == "uniform":

@@ -51,7 +51,9 @@ class PortModel(C.Structure):
                 ("E_z", C.c_double), ("z_cutoff", C.c_double), ("max_ntheta", C.c_int),
                 ("dtheta", C.c_double), ("dr", DP), ("dz", DP), ("nreact", C.c_int),
                 ("react", PortReaction * MAXR), ("per_plane", C.c_int),
-                ("zero_all", C.c_int), ("field_mode", C.c_int)]
+                ("zero_all", C.c_int), ("field_mode", C.c_int),
+                ("n_photo", C.c_int), ("photo_A", C.c_double * 8), ("photo_es", C.c_double * 8),
+                ("photo_src", C.c_int), ("photo_e", C.c_int), ("photo_pi", C.c_int)]
 
 
 class PortGrid(C.Structure):
@@ -144,6 +146,7 @@ def ref_lib(omp=False):
                                        C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                        C.c_int, C.c_int]
         lib.ref_set_field_mode.argtypes = [C.c_int, C.c_int]
+        lib.ref_set_photo.argtypes = [C.c_int, DP, DP, C.c_int, C.c_int, C.c_int]
         lib.ref_set_refine_params.argtypes = [C.c_double, C.c_int, C.c_double, C.c_double,
                                               C.c_double, C.c_int, C.c_int, C.c_int]
         lib.ref_cdr_refine.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int]
@@ -205,6 +208,11 @@ class PortTree(_TreeBase):
         m.per_plane = 1 if params.per_plane else 0
         m.zero_all = 1 if zero_all else 0
         m.field_mode = field_mode
+        # photo terms in the order photo_calc visits them (last-first)
+        m.n_photo = len(model.photo)
+        for i, t in enumerate(reversed(model.photo)):
+            m.photo_A[i], m.photo_es[i] = t.A, t.lam
+        m.photo_src, m.photo_e, m.photo_pi = model.photo_source, model.photo_electrons, model.photo_ions
         self.m = m
         self.grids: List[PortGrid] = []
         self.arrays = []
@@ -312,6 +320,12 @@ class RefTree(_TreeBase):
             write_react_table(path, re.table, "table written for the reference oracle")
             names += path.encode() + b"\0"
         lib.ref_set_reactions(nr, nin, ins, nout, outs, C.c_char_p(names + b"\0"))
+        if model.photo:
+            A = np.array([t.A for t in model.photo], dtype=np.float64)
+            lam = np.array([t.lam for t in model.photo], dtype=np.float64)
+            self._photo = (A, lam)
+            lib.ref_set_photo(len(model.photo), _dp(A), _dp(lam), model.photo_electrons,
+                              model.photo_source, model.photo_ions)
         lib.ref_finish_setup()
         self.gids = []
         for sp in self.specs:

@@ -361,10 +361,49 @@ advect_diffu_r (const port_model *m, port_grid *g)
 }
 
 /* A8: cdr_calc_d_dens (cdr.c:830-835) */
+/* ---- photo_calc (src/photo.c:313-345) on a single root grid, the last entry
+ * of react_apply_all's list: the source d_dens[src] / ntheta into charge
+ * (photo_copy_source, :247-264), to theta modes (3-D), then per term the
+ * Helmholtz solve with es = lambda (photo_calc_term -> pois_gen_solve_a, the
+ * stand-in of poisson_host.c, phi into photo), photo back to real space
+ * (photo_dft_r) and d_dens[e], d_dens[pi] += A photo (photo_add_term,
+ * :268-291), every element of the arrays (iter_grid_3d_n with 2). ---- */
+int oracle_poisson_mode (int nr, int nz, double dr, double dz, double elmbda, double es,
+                         const double *charge, double *er, double *ez, double *et);
+void oracle_dft_array (int n, double *a, long plen, int sign);
+void oracle_wk (int n, double *w2k, double *wk);
+
+static void
+port_photo_calc (const port_model *m, port_grid *g)
+{
+  const int nt = g->ntheta, nr = g->r1 - g->r0, nz = g->z1 - g->z0;
+  const long n = alen (g), pl = plen (g), o = nt == 1 ? 0 : 2 * pl;
+  double *photo = calloc (n, sizeof (double)), *scr = malloc (2 * pl * sizeof (double));
+  double w2k[256], wk[256];
+  long i;
+  int t, k;
+  for (i = 0; i < n; i++) g->charge[i] = g->d_dens[m->photo_src][i] / nt;
+  oracle_wk (nt, w2k, wk);
+  if (nt != 1) oracle_dft_array (nt, g->charge + o, pl, 1);
+  for (t = 0; t < m->n_photo; t++) {
+    for (k = 0; k < nt; k++)
+      oracle_poisson_mode (nr, nz, m->dr[g->level], m->dz[g->level], -w2k[k], m->photo_es[t],
+                           g->charge + o + k * pl, scr, scr + pl, photo + o + k * pl);
+    if (nt != 1) oracle_dft_array (nt, photo + o, pl, -1);
+    for (i = 0; i < n; i++) {
+      g->d_dens[m->photo_e][i] += m->photo_A[t] * photo[i];
+      g->d_dens[m->photo_pi][i] += m->photo_A[t] * photo[i];
+    }
+  }
+  free (photo);
+  free (scr);
+}
+
 void
 port_calc_d_dens (const port_model *m, port_grid *root)
 {
   port_react_apply_all (m, root);
+  if (m->n_photo) port_photo_calc (m, root);
   advect_diffu_r (m, root);
 }
 

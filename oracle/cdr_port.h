@@ -46,7 +46,12 @@ typedef struct {
   port_reaction react[PORT_MAX_REACT];
   int per_plane;              /* 1: drift/diffusion on every theta plane */
   int zero_all;               /* 1: every grid's d_dens starts at zero (static trees) */
-  int field_mode;             /* 0 zero, 1 fixed arrays, 2 host Poisson (2-D root) */
+  int field_mode;             /* 0 zero, 1 fixed arrays, 2 host Poisson (root) */
+  /* photoionization (src/photo.c:268-360), the entry ending the reactions
+   * list (src/rt.c:38-47); terms in the order photo_calc visits them */
+  int n_photo;
+  double photo_A[8], photo_es[8];
+  int photo_src, photo_e, photo_pi;
 } port_model;
 
 typedef struct port_grid port_grid;

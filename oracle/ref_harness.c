@@ -38,12 +38,11 @@
 #include "rz_array.h"
 #include "species.h"
 
-/* ---- globals normally defined in rt.c / poisson.c / photo.c ---- */
+/* ---- globals normally defined in rt.c / poisson.c (photo.c is compiled) ---- */
 species_t *spec_index[16];
 seed_t *seed_index[16];
 reaction_t *reaction_index[32];
 pois_problem_t *pois_electrostatic = NULL;
-photo_term_t *photo_terms = NULL;
 double pois_inhom_fixed_q_t = 0.0;
 
 extern mapper_t **dens_mappers, **dens_bnd_mappers;
@@ -61,10 +60,6 @@ never (const char *what)
   exit (3);
 }
 void kinetic_init (void) { never ("kinetic_init"); }
-void photo_init (void) {}
-void photo_load_file (char *f) { (void) f; never ("photo_load_file"); }
-void photo_unregister_all (void) {}
-void photo_calc (photo_term_t *t, cdr_grid_t *c) { (void) t; (void) c; never ("photo_calc"); }
 void pois_init (void) {}
 void pois_free_r (pois_grid_t *g) { if (g) never ("pois_free_r(non-NULL)"); }
 double pois_inhom_er (double r, double z) { (void) r; (void) z; never ("pois_inhom_er"); return 0; }
@@ -95,8 +90,47 @@ static species_t species_store[16];
  * dft_transform and dft_diff run. */
 void ref_dft_transform (rz_array_t *in, rz_array_t *out, int sign);
 void ref_dft_diff (grid_t *grid, rz_array_t *f);
-void dft_transform (rz_array_t *in, rz_array_t *out, int sign) { if (field_mode == 2) ref_dft_transform (in, out, sign); }
+static int in_photo = 0;     /* inside photo_calc: its transforms are real */
+void dft_transform (rz_array_t *in, rz_array_t *out, int sign)
+{ if (field_mode == 2 || in_photo) ref_dft_transform (in, out, sign); }
 void dft_diff (grid_t *g, rz_array_t *f) { if (field_mode == 2) ref_dft_diff (g, f); }
+
+/* src/photo.c, compiled with photo_calc renamed ref_photo_calc: the
+ * photoionization of a stage runs the reference's own code, with the
+ * Helmholtz solves of pois_gen_solve_a below. */
+void ref_photo_calc (photo_term_t *terms, cdr_grid_t *cdr);
+void photo_calc (photo_term_t *terms, cdr_grid_t *cdr)
+{
+  in_photo = 1;
+  ref_photo_calc (terms, cdr);
+  in_photo = 0;
+}
+
+/* pois_gen_solve_a (src/poisson.c:777-830) as photo_calc_term calls it
+ * (src/photo.c:296-305): per theta mode the Helmholtz problem with lambda =
+ * -w2k[mode] and es = the term's lambda, on the same 5-point operator and
+ * Dirichlet sides as the field solve (the photo problems take the
+ * electrostatic conditions by default, src/photo.c:50-57 with
+ * extra_photo_levels = -1, src/cstream.c:117), mapped into cdr->photo
+ * (photo_copy, src/photo.c:82-93: phi on the interior).  Single root grid. */
+int oracle_poisson_mode (int nr, int nz, double dr_, double dz_, double elmbda, double es,
+                         const double *charge, double *er, double *ez, double *et);
+pois_grid_t **
+pois_gen_solve_a (cdr_grid_t *cdr, pois_problem_t *prob, mapper_t **mappers, double es)
+{
+  const int nr = cdr->r1 - cdr->r0, nz = cdr->z1 - cdr->z0, nt = cdr->ntheta;
+  const long plen = (long) (nr + 4) * (nz + 4);
+  double *scr = malloc (sizeof (double) * 2 * plen);
+  int k;
+  (void) prob; (void) mappers;
+  if (cdr->first_child != NULL || cdr->photo == NULL) never ("pois_gen_solve_a: one root grid with a photo array");
+  for (k = 0; k < nt; k++)
+    oracle_poisson_mode (nr, nz, dr[cdr->level], dz[cdr->level], -w2k[k], es,
+                         RZTP (cdr->charge, cdr->r0 - 2, cdr->z0 - 2, k), scr, scr + plen,
+                         RZTP (cdr->photo, cdr->r0 - 2, cdr->z0 - 2, k));
+  free (scr);
+  return calloc (max_ntheta > 0 ? max_ntheta : 1, sizeof (pois_grid_t *));
+}
 static double *dr_store, *dz_store;
 
 static int
@@ -253,6 +287,36 @@ ref_set_reactions (int nreact, const int *nin, const int *inputs,
   }
   reactions_list = NULL;
   for (r = nreact; r > 0; r--) react_add (&react_store[r - 1]);
+  return 0;
+}
+
+/* kinetic_init (src/rt.c:38-47) with photoionization: the photo entry is
+ * added before the reactions, so it ends the reactions list; the terms are
+ * registered in file order (photo_load_file, src/photo.c:373-400), so
+ * photo_calc visits them last-first.  After ref_set_reactions, before any
+ * grid (cdr_new allocates the photo array, src/cdr.c:117). */
+static reaction_t react_photo_store;
+int
+ref_set_photo (int n, const double *A, const double *lambda, int electrons_, int ions_,
+               int photo_ions_)
+{
+  reaction_t *t;
+  int i;
+  has_photoionization = 1;
+  electrons = electrons_;
+  ions = ions_;
+  photo_ions = photo_ions_;
+  photo_unregister_all ();
+  for (i = 0; i < n; i++) photo_register (A[i], lambda[i]);
+  memset (&react_photo_store, 0, sizeof (react_photo_store));
+  react_photo_store.is_photo = 1;
+  react_photo_store.tablefile = NULL;
+  if (!reactions_list) reactions_list = &react_photo_store;
+  else {
+    for (t = reactions_list; t->next; t = t->next) ;
+    t->next = &react_photo_store;
+  }
+  photo_init ();
   return 0;
 }
 
