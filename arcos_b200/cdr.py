@@ -107,6 +107,8 @@ class CdrTree:
         check(self.L.arcos_set_per_patch(self.h, 1 if per_patch else 0))
         check(self.L.arcos_commit(self.h))
         self._field_cb = None
+        if model.photo:                         # has_photoionization (rt.c:38-47)
+            self.set_photo()
 
     def close(self):
         if getattr(self, "h", None):
@@ -178,6 +180,17 @@ class CdrTree:
 
         self._field_cb = FIELD_FN(cb)
         check(self.L.arcos_set_field_fn(self.h, self._field_cb, None))
+
+    def set_photo(self, model=None):
+        """Photoionization of ``model`` (default: the tree's own) on the device:
+        its photo terms (file order), source and receiving species
+        (photo_calc, src/photo.c:313-345); no terms switches it off."""
+        m = model if model is not None else self.model
+        n = len(m.photo)
+        A = np.array([t.A for t in m.photo] or [0.0], dtype=np.float64)
+        lam = np.array([t.lam for t in m.photo] or [0.0], dtype=np.float64)
+        check(self.L.arcos_set_photo(self.h, n, _dp(A), _dp(lam), max(m.photo_source, 0),
+                                     m.photo_electrons, max(m.photo_ions, 0)))
 
     def set_field_poisson(self, on: bool = True):
         """Solve the field of every stage on the device (pois_solve_a,

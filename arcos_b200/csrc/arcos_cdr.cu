@@ -127,6 +127,14 @@ struct Ctx {
   double *ext_d = nullptr;            // [ext_r (nfam*MAXPLANES) | ext_t | ext_z (nfam)]
   std::vector<double> famE;           // 3 per family
   arcos_field_fn fn = nullptr;
+  // photoionization (photo_calc, src/photo.c:313-345), single grid: terms
+  // in the order photo_calc visits them, one Helmholtz set-up per term
+  int photo_n = 0;
+  double photo_A[ARCOS_MAX_PHOTO] = {};
+  PoisArgs photo_args[ARCOS_MAX_PHOTO] = {};
+  double *photo_buf[ARCOS_MAX_PHOTO] = {};
+  double *photo_d = nullptr;          // the photo array (patch layout)
+  int photo_src = -1, photo_e = -1, photo_pi = -1;
   bool pois = false;                  // field of each stage from the device Poisson solve
   double *pois_d = nullptr;           // its coefficients and scratch
   PoisArgs pois_args{};
@@ -766,21 +774,76 @@ device_poisson (Ctx *c, int set)
   const int b = std::min ((n + 255) / 256, 8 * c->num_sms);
   const int cells = (A.nr + 4) * (A.nz + 4);
   const int bd = std::min ((cells + 127) / 128, 8 * c->num_sms);
-  if (A.nt > 1) k_theta_dft<0><<<bd, 128, 0, c->stream>>> (c->pd_d, 0, set, K_CHARGE, A);   // cdr_dft_charge_r
+  const PatchDesc &P = c->pd_h[0];
+  auto plane0 = [&] (int kind) { return P.arr (set, kind) + (long long) (0 - P.theta0) * P.plane_stride; };
+  if (A.nt > 1)                                 // cdr_dft_charge_r
+    k_theta_dft<0><<<bd, 128, 0, c->stream>>> (plane0 (K_CHARGE), P.pitch, P.plane_stride, A);
   k_pois_fwd<<<b, 256, 0, c->stream>>> (c->pd_d, 0, set, A);
   k_pois_tri<<<(A.nz * A.nt + 127) / 128, 128, 0, c->stream>>> (A);
   k_pois_inv<<<b, 256, 0, c->stream>>> (A);
   // set 1 is the RK2 intermediate grid, fresh every step in the reference
   const int fresh = set == 1;
-  const long long len = (long long) (A.nz + 4) * c->pd_h[0].pitch * (A.nt + (fresh && A.nt > 1 ? 4 : 0));
+  const long long len = (long long) (A.nz + 4) * P.pitch * (A.nt + (fresh && A.nt > 1 ? 4 : 0));
   k_pois_field<<<(int) std::min<long long> ((len + 255) / 256, 8 * c->num_sms), 256, 0, c->stream>>> (c->pd_d, 0, set, A, fresh);
   if (A.nt > 1) {                               // cdr_dft_field_r
-    k_theta_dft<1><<<bd, 128, 0, c->stream>>> (c->pd_d, 0, set, K_ER, A);
-    k_theta_dft<1><<<bd, 128, 0, c->stream>>> (c->pd_d, 0, set, K_EZ, A);
-    k_theta_dft<2><<<bd, 128, 0, c->stream>>> (c->pd_d, 0, set, K_ETHETA, A);
+    k_theta_dft<1><<<bd, 128, 0, c->stream>>> (plane0 (K_ER), P.pitch, P.plane_stride, A);
+    k_theta_dft<1><<<bd, 128, 0, c->stream>>> (plane0 (K_EZ), P.pitch, P.plane_stride, A);
+    k_theta_dft<2><<<bd, 128, 0, c->stream>>> (plane0 (K_ETHETA), P.pitch, P.plane_stride, A);
   }
   CKL ();
   return do_field_post (c, set);
+}
+
+// photo_calc (src/photo.c:313-345) on the single grid of the context, storage
+// set `set`, after the reactions: the source, its theta modes, then per term
+// the Helmholtz solve, photo back to real space and the two additions.
+int
+device_photo (Ctx *c, int set)
+{
+  const PatchDesc &P = c->pd_h[0];
+  const PoisArgs &A0 = c->photo_args[0];
+  const int nt = A0.nt;
+  const int n = A0.nr * A0.nz * nt;
+  const int b = std::min ((n + 255) / 256, 8 * c->num_sms);
+  const int bd = std::min (((A0.nr + 4) * (A0.nz + 4) + 127) / 128, 8 * c->num_sms);
+  const int be = (int) std::min<long long> ((P.asz + 255) / 256, 8 * c->num_sms);
+  const long long p0 = (long long) (0 - P.theta0) * P.plane_stride;
+  const long long len = (long long) (A0.nz + 4) * P.pitch * nt;
+  const int bf = (int) std::min<long long> ((len + 255) / 256, 8 * c->num_sms);
+  k_photo_source<<<be, 256, 0, c->stream>>> (c->pd_d, 0, set, c->photo_src);
+  if (nt > 1) k_theta_dft<0><<<bd, 128, 0, c->stream>>> (P.arr (set, K_CHARGE) + p0, P.pitch, P.plane_stride, A0);
+  for (int t = 0; t < c->photo_n; t++) {
+    const PoisArgs &A = c->photo_args[t];
+    k_pois_fwd<<<b, 256, 0, c->stream>>> (c->pd_d, 0, set, A);
+    k_pois_tri<<<(A.nz * A.nt + 127) / 128, 128, 0, c->stream>>> (A);
+    k_pois_inv<<<b, 256, 0, c->stream>>> (A);
+    k_photo_field<<<bf, 256, 0, c->stream>>> (c->pd_d, 0, c->photo_d, A);
+    if (nt > 1) k_theta_dft<1><<<bd, 128, 0, c->stream>>> (c->photo_d + p0, P.pitch, P.plane_stride, A);
+    k_photo_add<<<be, 256, 0, c->stream>>> (c->pd_d, 0, set, c->photo_d, c->photo_A[t], c->photo_e, c->photo_pi);
+  }
+  CKL ();
+  return ARCOS_OK;
+}
+
+// cdr_calc_d_dens (cdr.c:830-835) of storage set `set`: one derivative
+// launch, or with photoionization (the entry that ends react_apply_all's
+// list, rt.c:38-47) the reactions alone (every species taken as immobile),
+// photo_calc, then drift/diffusion added.
+int
+derive (Ctx *c, int set)
+{
+  StageArgs A = base_args (c);
+  A.nset = set; A.dset = set;
+  if (!c->photo_n) return run_stage (c, A, M_DERIV);
+  const Model keep = c->M;
+  for (int s = 0; s < c->M.ns; s++) c->M.mobile[s] = 0;
+  int r = run_stage (c, A, M_DERIV);
+  c->M = keep;
+  if (r) return r;
+  if ((r = device_photo (c, set))) return r;
+  A = base_args (c);
+  A.nset = set; A.dset = set; A.accumulate = 1;
+  return run_stage (c, A, M_DERIV);
 }
 
 // field callback for the root of family 0 (the reference solves the field on the tree root)
@@ -858,8 +921,7 @@ rk2_general (Ctx *c)
   if ((r = do_nonneg (c, 0))) return r;                 // cdr.c:1276
   if ((r = do_prepare (c, 0))) return r;                // cdr.c:1279
   if (inloop (c) && (r = field_from_callback (c, 0, 0))) return r;   // cdr.c:1283
-  A.nset = 0; A.dset = 0;
-  if ((r = run_stage (c, A, M_DERIV))) return r;        // cdr.c:1288
+  if ((r = derive (c, 0))) return r;                    // cdr.c:1288
   if ((r = do_dmax (c, 0, 0))) return r;                // cdr.c:1293
   k_cfl<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->M, c->st_d, c->nfam, 0);
   CKL ();
@@ -869,7 +931,16 @@ rk2_general (Ctx *c)
   if ((r = do_charge (c, 1))) return r;
   if ((r = do_prepare (c, 1))) return r;                // cdr.c:1311
   if (inloop (c) && (r = field_from_callback (c, 1, 1))) return r;   // cdr.c:1313
-  if ((r = run_stage (c, A, M_AMR2))) return r;         // cdr.c:1314-1317
+  if (c->photo_n) {
+    // the derivative of the intermediate state with photo_calc, then
+    // cdr_rk2_update (cdr.c:1125-1132) on every element
+    if ((r = derive (c, 1))) return r;
+    if ((r = for_patches (c, max_patch_work (c), [&] (dim3 g, const int *pl) {
+           k_rk2_update<<<g, 256, 0, c->stream>>> (c->pd_d, pl, c->st_d, 0.0, 1);
+         }))) return r;
+  } else if ((r = run_stage (c, A, M_AMR2))) {
+    return r;                                           // cdr.c:1314-1317
+  }
   if ((r = do_charge (c, 0))) return r;
   if ((r = do_prepare (c, 0))) return r;                // cdr.c:1322
   k_step_end<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->st_d, c->nfam);
@@ -1371,6 +1442,8 @@ arcos_destroy (void *ctx)
   drop_graphs (c);
   cudaFree (c->colfac_d);
   cudaFree (c->pois_d);
+  for (int t = 0; t < ARCOS_MAX_PHOTO; t++) cudaFree (c->photo_buf[t]);
+  cudaFree (c->photo_d);
   cudaFree (c->lean_nodes_d);
   cudaFree (c->adj_pool); cudaFree (c->adj_hs_d); cudaFree (c->adj_gtab_d);
   cudaFree (c->adj_gpart_d); cudaFree (c->adj_invde_d); cudaFree (c->adj_tiles_d);
@@ -2156,29 +2229,23 @@ arcos_field_post (void *ctx, int set)
   return ARCOS_OK;
 }
 
-// The field of every stage from the device solve of poisson_kernel.cuh
-// (single 2-D grid).  The transform matrix, norms, eigenvalues and
-// tridiagonal coefficients are evaluated here, in the host solver's
-// expressions, so the device field is bit-identical to the host's.
+// The tables and scratch of one device Helmholtz solve (poisson_kernel.cuh)
+// on the single grid of the context, with the constant es on the diagonal.
+// The transform matrix, norms, eigenvalues and tridiagonal coefficients are
+// evaluated here, in the host solver's expressions, so the device solve is
+// bit-identical to the host's.
 int
-arcos_set_field_poisson (void *ctx, int on)
+pois_build (Ctx *c, double es, PoisArgs &A, double *&buf)
 {
-  Ctx *c = (Ctx *) ctx;
-  int r = chk_committed (c);
-  if (r) return r;
-  drop_graphs (c);
-  if (!on) { c->pois = false; return ARCOS_OK; }
-  if (c->pd_h.size () != 1 || !c->fused_ok || c->pd_h[0].ntheta > 64)
-    return fail (ARCOS_ERR_ARG, "the device field solve takes one grid (at most 64 theta planes) with every side external");
-  if (c->fn) return fail (ARCOS_ERR_STATE, "a field callback is set (arcos_set_field_fn (ctx, NULL, NULL) first)");
   const PatchDesc &P = c->pd_h[0];
   const int nr = P.nr, nz = P.nz, nt = P.ntheta;
   const double dr = P.dr, dz = P.dz, pi = 3.14159265358979323846;
   std::vector<double> St ((size_t) nz * nz), norm (nz, 0.0), lam (nz), ta (nr), tc (nr);
   // theta modes: w2k and wk of init_wk_a (src/cstream.c:309-344), the
   // Helmholtz diagonal terms elmbda_m / r_i^2 + es with elmbda_m = -w2k[m]
-  // and es = 0 (pois_solve_mode, src/poisson.c:847), the twiddles of the
-  // theta transforms (cos, sin of 2 pi q / nt)
+  // (pois_solve_mode, src/poisson.c:847; es = 0 for the field, the term's
+  // lambda for photoionization), the twiddles of the theta transforms (cos,
+  // sin of 2 pi q / nt)
   std::vector<double> w2k (nt, 0.0), wk (nt, 0.0), elm (nt), mk ((size_t) nt * nr), tcs (nt), tsn (nt);
   {
     const double dtheta = 6.283185307179586477 / nt, twobydtheta2 = 2. / (dtheta * dtheta);
@@ -2202,7 +2269,7 @@ arcos_set_field_poisson (void *ctx, int on)
       elm[m] = -w2k[m];
       for (int i = 0; i < nr; i++) {
         const double ri = (i + 0.5) * dr;
-        mk[(size_t) m * nr + i] = elm[m] / (ri * ri) + 0.0;
+        mk[(size_t) m * nr + i] = elm[m] / (ri * ri) + es;
       }
       tcs[m] = cos (6.283185307179586477 * m / nt);
       tsn[m] = sin (6.283185307179586477 * m / nt);
@@ -2225,11 +2292,10 @@ arcos_set_field_poisson (void *ctx, int on)
   }
   const size_t nn = (size_t) nr * nz * nt;
   const size_t total = St.size () + 3 * (size_t) nz + 2 * (size_t) nr + mk.size () + 4 * (size_t) nt + 5 * nn;
-  cudaFree (c->pois_d);
-  c->pois_d = nullptr;
-  CK (cudaMalloc (&c->pois_d, sizeof (double) * total));
-  double *q = c->pois_d;
-  PoisArgs &A = c->pois_args;
+  cudaFree (buf);
+  buf = nullptr;
+  CK (cudaMalloc (&buf, sizeof (double) * total));
+  double *q = buf;
   A.nr = nr; A.nz = nz; A.nt = nt; A.r0 = P.r0; A.dr = dr; A.dz = dz;
   A.St = q; q += St.size ();
   A.norm = q; q += nz;
@@ -2256,9 +2322,62 @@ arcos_set_field_poisson (void *ctx, int on)
   CK (cudaMemcpy ((void *) A.tcos, tcs.data (), sizeof (double) * nt, cudaMemcpyHostToDevice));
   CK (cudaMemcpy ((void *) A.tsin, tsn.data (), sizeof (double) * nt, cudaMemcpyHostToDevice));
   CK (cudaMemcpy ((void *) A.wk, wk.data (), sizeof (double) * nt, cudaMemcpyHostToDevice));
+  return ARCOS_OK;
+}
+
+// The field of every stage from the device solve of poisson_kernel.cuh
+// (a single grid; 3-D by theta modes).
+int
+arcos_set_field_poisson (void *ctx, int on)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  drop_graphs (c);
+  if (!on) { c->pois = false; return ARCOS_OK; }
+  if (c->pd_h.size () != 1 || !c->fused_ok || c->pd_h[0].ntheta > 64)
+    return fail (ARCOS_ERR_ARG, "the device field solve takes one grid (at most 64 theta planes) with every side external");
+  if (c->fn) return fail (ARCOS_ERR_STATE, "a field callback is set (arcos_set_field_fn (ctx, NULL, NULL) first)");
+  if ((r = pois_build (c, 0.0, c->pois_args, c->pois_d))) return r;
+  const int nt = c->pd_h[0].ntheta;
   // a 3-D solve gives E_theta != 0: the stage kernels read |E| from memory
   if (nt > 1) c->stage_eabs = 1;
   c->pois = true;
+  return ARCOS_OK;
+}
+
+// Photoionization on the single grid of the context (photo_calc, the entry
+// that ends the reactions list, src/rt.c:38-47): terms in file order, visited
+// last-first as photo_calc visits the list photo_register builds.
+int
+arcos_set_photo (void *ctx, int n_terms, const double *A, const double *lambda, int source,
+                 int electrons, int photo_ions)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  drop_graphs (c);
+  if (n_terms == 0) { c->photo_n = 0; return ARCOS_OK; }
+  if (n_terms < 0 || n_terms > ARCOS_MAX_PHOTO || !A || !lambda)
+    return fail (ARCOS_ERR_ARG, "arcos_set_photo: 1 .. 8 terms");
+  if (c->pd_h.size () != 1 || !c->fused_ok || c->pd_h[0].ntheta > 64)
+    return fail (ARCOS_ERR_ARG, "photoionization takes one grid (at most 64 theta planes) with every side external");
+  const int ns = c->M.ns;
+  if (source < 0 || source >= ns || electrons < 0 || electrons >= ns || photo_ions < 0 || photo_ions >= ns)
+    return fail (ARCOS_ERR_ARG, "arcos_set_photo: species out of range");
+  for (int t = 0; t < n_terms; t++) {
+    const int k = n_terms - 1 - t;
+    c->photo_A[t] = A[k];
+    if ((r = pois_build (c, lambda[k], c->photo_args[t], c->photo_buf[t]))) return r;
+  }
+  if (!c->photo_d) {
+    CK (cudaMalloc (&c->photo_d, sizeof (double) * c->pd_h[0].asz));
+    CK (cudaMemset (c->photo_d, 0, sizeof (double) * c->pd_h[0].asz));
+  }
+  c->photo_n = n_terms;
+  c->photo_src = source;
+  c->photo_e = electrons;
+  c->photo_pi = photo_ions;
   return ARCOS_OK;
 }
 
@@ -2466,7 +2585,8 @@ arcos_react_apply_all (void *ctx, int set)
   A.nset = set; A.dset = set;
   r = run_stage (c, A, M_DERIV);
   c->M = keep;
-  return r;
+  if (r) return r;
+  return c->photo_n ? device_photo (c, set) : ARCOS_OK;   // the photo entry ends the list
 }
 
 // cdr_advect_diffu_r alone: d_dens += drift/diffusion divergence.
@@ -2489,9 +2609,7 @@ arcos_cdr_calc_d_dens (void *ctx, int set)
   int r = chk_committed (c);
   if (r) return r;
   SET_OK (set);
-  StageArgs A = base_args (c);
-  A.nset = set; A.dset = set;
-  return run_stage (c, A, M_DERIV);
+  return derive (c, set);
 }
 
 int
@@ -2579,7 +2697,7 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
   if ((r = read_states (c, st0))) return r;
   if (nsteps > 0 && (r = small_dt_pending (c, st0))) return r;
   const int step0 = st0[0].step;
-  const bool fixed_fused = c->fused_ok && !inloop (c);
+  const bool fixed_fused = c->fused_ok && !inloop (c) && c->photo_n == 0;
   if (fixed_fused) {
     // set_h_attempt and reset_dmax (slot 0) in one stream-ordered write
     c->st_stage = st0;
@@ -2594,8 +2712,10 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
   } else if ((r = set_h_attempt (c, h))) {
     return r;
   }
-  if (!c->fused_ok && !inloop (c) && !c->per_patch && nsteps > 0) {
-    // trees: one step (all its batched launches) captured once, replayed
+  // trees, and single grids with photoionization: the general step
+  const bool general = !c->fused_ok || c->photo_n > 0;
+  if (general && (!inloop (c) || c->pois) && !c->per_patch && nsteps > 0) {
+    // one step (all its batched launches) captured once, replayed
     const bool lean = lean_tree_ok (c);
     if (!c->graph_tree) {
       cudaGraph_t gr;
@@ -2609,7 +2729,7 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
     }
     for (int k = 0; k < nsteps; k++) CK (cudaGraphLaunch (c->graph_tree, c->stream));
     if (lean && (r = do_prepare (c, 0))) return r;      // cdr.c:1322, once
-  } else if (!c->fused_ok) {
+  } else if (general) {
     for (int k = 0; k < nsteps; k++)
       if ((r = rk2_general (c))) return r;
   } else if (inloop (c)) {

@@ -17,6 +17,7 @@
 #define ARCOS_MAXIN 4
 #define ARCOS_MAXOUT 6
 #define ARCOS_MAXPLANES 68   // ntheta <= 64
+#define ARCOS_MAX_PHOTO 8    // photoionization terms
 #define ARCOS_MAXLEVELS 16   // refinement levels
 
 namespace arcos {

@@ -174,29 +174,29 @@ k_pois_field (const PatchDesc *__restrict__ pd, int patch, int set, PoisArgs A, 
 // ---- theta transforms of one array, every element of the (nr+4) x (nz+4)
 // rows of planes 0 .. nt-1: r2hc (WHAT 0), hc2r (WHAT 1), or dft_diff then
 // hc2r (WHAT 2), each as the host restatement sums them ----
+// `a` is plane 0 of an array in the patch layout (rows of `pitch`, planes of
+// `pstride` doubles).
 template <int WHAT>
 __global__ void
-k_theta_dft (const PatchDesc *__restrict__ pd, int patch, int set, int kind, PoisArgs A)
+k_theta_dft (double *__restrict__ a, long long pitch, long long pstride, PoisArgs A)
 {
-  const PatchDesc &P = pd[patch];
   const int n = A.nt, w = A.nr + 4;
   const int cells = w * (A.nz + 4);
-  double *a = P.arr (set, kind) + (long long) (0 - P.theta0) * P.plane_stride;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
     const int row = c / w, col = c - row * w;
-    double *e = a + (long long) row * P.pitch + col;
+    double *e = a + (long long) row * pitch + col;
     double t[64];
-    for (int j = 0; j < n; j++) t[j] = e[(long long) j * P.plane_stride];
+    for (int j = 0; j < n; j++) t[j] = e[(long long) j * pstride];
     if (WHAT == 0) {
       for (int k = 0; k <= n / 2; k++) {
         double re = 0.0;
         for (int j = 0; j < n; j++) re += t[j] * A.tcos[(j * k) % n];
-        e[(long long) k * P.plane_stride] = re;
+        e[(long long) k * pstride] = re;
       }
       for (int k = 1; k < (n + 1) / 2; k++) {
         double im = 0.0;
         for (int j = 0; j < n; j++) im += t[j] * A.tsin[(j * k) % n];
-        e[(long long) (n - k) * P.plane_stride] = -im;
+        e[(long long) (n - k) * pstride] = -im;
       }
       continue;
     }
@@ -223,8 +223,56 @@ k_theta_dft (const PatchDesc *__restrict__ pd, int patch, int set, int kind, Poi
         acc += 2.0 * (t[k] * A.tcos[q] - t[n - k] * A.tsin[q]);
       }
       if (n % 2 == 0) acc += t[n / 2] * A.tcos[(j * (n / 2)) % n];
-      e[(long long) j * P.plane_stride] = acc;
+      e[(long long) j * pstride] = acc;
     }
+  }
+}
+
+// ---- photoionization (photo_calc, src/photo.c:313-345) ----
+// photo_copy_source (src/photo.c:247-264): charge = d_dens[src] / ntheta on
+// every element (iter_grid_3d_n with 2 covers the whole array).
+__global__ void
+k_photo_source (const PatchDesc *__restrict__ pd, int patch, int set, int src)
+{
+  const PatchDesc &P = pd[patch];
+  const double *d = P.arr (set, K_DDENS, src);
+  double *ch = P.arr (set, K_CHARGE);
+  for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < P.asz;
+       i += (long long) gridDim.x * blockDim.x)
+    ch[i] = d[i] / P.ntheta;
+}
+
+// phi of every theta mode into the photo array (photo_copy, src/photo.c:82-93):
+// the interior of planes 0 .. nt-1, zero on their other elements.
+__global__ void
+k_photo_field (const PatchDesc *__restrict__ pd, int patch, double *__restrict__ photo, PoisArgs A)
+{
+  const PatchDesc &P = pd[patch];
+  const int nr = A.nr, nz = A.nz;
+  const long long len = (long long) (nz + 4) * P.pitch;
+  for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < len * A.nt;
+       t += (long long) gridDim.x * blockDim.x) {
+    const int m = (int) (t / len);
+    const long long e = t - (long long) m * len;
+    const int row = (int) (e / P.pitch), col = (int) (e - (long long) row * P.pitch);
+    const int i = col - 2, j = row - 2;
+    const double v = (j >= 0 && j < nz && i >= 0 && i < nr) ? A.phi[(size_t) m * nr * nz + (size_t) i * nz + j] : 0.0;
+    photo[(long long) (m - P.theta0) * P.plane_stride + e] = v;
+  }
+}
+
+// photo_add_term (src/photo.c:268-291): d_dens of electrons and photo ions
+// += A photo on every element.
+__global__ void
+k_photo_add (const PatchDesc *__restrict__ pd, int patch, int set, const double *__restrict__ photo,
+             double a, int se, int spi)
+{
+  const PatchDesc &P = pd[patch];
+  double *de = P.arr (set, K_DDENS, se), *dp = P.arr (set, K_DDENS, spi);
+  for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < P.asz;
+       i += (long long) gridDim.x * blockDim.x) {
+    de[i] += a * photo[i];
+    dp[i] += a * photo[i];
   }
 }
 

@@ -146,6 +146,19 @@ int arcos_set_field_fn (void *ctx, arcos_field_fn fn, void *user);
  * trip (arcos_run replays the whole step from a CUDA graph).  Excludes
  * arcos_set_field_fn. */
 int arcos_set_field_poisson (void *ctx, int on);
+/* Photoionization (has_photoionization; photo_calc, src/photo.c:313-345, the
+ * entry that ends the reactions list as kinetic_init builds it,
+ * src/rt.c:38-47), on a context of one grid (at most 64 theta planes, every
+ * side external): n_terms (at most 8) terms (A, lambda) in the order of the
+ * photoionization file (photo_load_file, src/photo.c:373-400; photo_calc
+ * visits them last-first), the source species ("dummyplus": the Helmholtz
+ * source is its d_dens / ntheta) and the two species that receive A * photo
+ * ("electrons" and "xplus").  Each term is one Helmholtz solve per theta mode
+ * with es = lambda on the operator of arcos_set_field_poisson, on the device;
+ * every derivative (arcos_run, arcos_cdr_rk2, arcos_cdr_calc_d_dens,
+ * arcos_react_apply_all) then includes it.  n_terms = 0 switches it off. */
+int arcos_set_photo (void *ctx, int n_terms, const double *A, const double *lambda,
+                     int source, int electrons, int photo_ions);
 /* One device field solve of storage set `set` from its current charge, then
  * the external field, |E| and theta periodicity (as arcos_field_post). */
 int arcos_solve_field (void *ctx, int set);
