@@ -274,7 +274,11 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
   constexpr int VX = L::VX, VY = L::VY, NT = L::NT, NW = NT / 32;
   constexpr int SC = L::SC, SR = L::SR, WC = L::WC, WR = L::WR, EC = L::EC, ZR = L::ZR;
   constexpr int FR = L::FR, FZ = L::FZ;
-  constexpr int RP = (VY * FR + NT - 1) / NT;        // passes over the radial faces
+  // one list of face items per species: the radial faces (row, face) first,
+  // padded to whole warps, then the axial faces (face row, column = lane), so
+  // a warp never mixes the two kinds and the passes are spread evenly
+  constexpr int NRI = VY * FR, NRP = (NRI + 31) / 32 * 32, NAI = FZ * VX;
+  constexpr int RP = (NRP + NAI + NT - 1) / NT;      // passes over the face items
   constexpr int CPT = L::CPT;                        // cells (rows) per thread
   static_assert (VX == 32 && VY == CPT * NW, "tile: a warp per CPT rows of 32 columns");
   extern __shared__ __align__ (16) double vsm[];
@@ -378,10 +382,7 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
     static_for<0, NS> ([&] (auto S_) {
       constexpr int s = decltype (S_)::value;
       if (!M.mobile[s]) return;                 // block-uniform
-#pragma unroll
-      for (int m = 0; m < RP; m++) {            // radial face ar - 1/2 of row j
-        const int jj = rjj[m], fi = rfi[m];
-        if (jj >= VY) break;
+      auto radial_item = [&] (int jj, int fi) {     // radial face ar - 1/2 of row j
         const int ar = c0 - 1 + fi, j = j0 + jj;
         double pLL = 0.0, pL = 0.0, pR = 0.0, pRR = 0.0;
         if (ar >= 0 && ar <= nr && j < nz) {
@@ -402,11 +403,8 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         }
         double *pr = sPR + jj * FR + fi;
         pr[0] = pLL; pr[VY * FR] = pL; pr[2 * VY * FR] = pR; pr[3 * VY * FR] = pRR;
-      }
-#pragma unroll
-      for (int m = 0; m < (FZ + NW - 1) / NW; m++) {   // axial face a - 1/2 of column c
-        const int fa = wq + NW * m;
-        if (fa >= FZ) break;
+      };
+      auto axial_item = [&] (int fa) {              // axial face a - 1/2 of column c
         const int a = j0 - 1 + fa, c = c0 + lane;
         double pLL = 0.0, pL = 0.0, pR = 0.0, pRR = 0.0;
         if (a >= 0 && a <= nz && c < nr) {
@@ -425,6 +423,15 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         }
         double *pz = sPZ + fa * VX + lane;
         pz[0] = pLL; pz[FZ * VX] = pL; pz[2 * FZ * VX] = pR; pz[3 * FZ * VX] = pRR;
+      };
+#pragma unroll
+      for (int m = 0; m < RP; m++) {
+        const int i = t + NT * m;
+        if (i < NRP) {
+          if (i < NRI) radial_item (rjj[m], rfi[m]);
+        } else if (i < NRP + NAI) {
+          axial_item ((i - NRP) >> 5);
+        }
       }
       __syncthreads ();
       // face x - 1/2 touches cells x-2 (LL), x-1 (L), x (R), x+1 (RR): cell y
@@ -472,31 +479,55 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
     // d_dens[s] += coef[s] rate.  Every lane joins the warp-wide table-gradient
     // reductions ----
     if (M.nreact > 0) {
+      // the folded coefficients as doubles, once per tile, in the radial
+      // partial buffer (dead after the faces)
+      double *const sCf = sPR;
+      for (int i = t; i < M.nreact * NS; i += NT) sCf[i] = (double) M.r_coef[i / NS][i - (i / NS) * NS];
       double wc[CPT][NS];
-      bool on[CPT];
+      bool on[CPT], own[CPT];
+      const double *rp0[CPT];
 #pragma unroll
       for (int q = 0; q < CPT; q++) {
         const int jj = CPT * wq + q, j = j0 + jj, c = c0 + lane;
-        const bool own = c < nr && j < nz;
+        own[q] = c < nr && j < nz;
 #pragma unroll
-        for (int s = 0; s < NS; s++) wc[q][s] = own ? sW[(s * WR + jj + 2) * WC + lane + 2] : 0.0;
-        on[q] = own && ((double) (Pp->z0 + j) + 0.5) * Pp->dz < M.z_cutoff;
+        for (int s = 0; s < NS; s++) wc[q][s] = own[q] ? sW[(s * WR + jj + 2) * WC + lane + 2] : 0.0;
+        on[q] = own[q] && ((double) (Pp->z0 + j) + 0.5) * Pp->dz < M.z_cutoff;
+        rp0[q] = adj + (long long) A.rates_idx * asz + AO (c0 + lane, j0 + CPT * wq + q);
       }
+      // the lookups of k_adj_rates for this cell, one reaction ahead
+      double nk[CPT], ntt[CPT], ncd[CPT];
+#pragma unroll
+      for (int q = 0; q < CPT; q++) {
+        nk[q] = own[q] ? __ldg (rp0[q]) : 0.0;
+        ntt[q] = own[q] ? __ldg (rp0[q] + asz) : 0.0;
+        ncd[q] = own[q] ? __ldg (rp0[q] + 2 * asz) : 0.0;
+      }
+      __syncthreads ();
 #pragma unroll 1
       for (int r = 0; r < M.nreact; r++) {
         const int nin = M.r_nin[r];
         int i_lo[CPT], i_hi[CPT];
         double g_lo[CPT], g_hi[CPT];
+        double ck[CPT], ctt[CPT], ccd[CPT];
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+          ck[q] = nk[q]; ctt[q] = ntt[q]; ccd[q] = ncd[q];
+          if (r + 1 < M.nreact && own[q]) {
+            const double *rp = rp0[q] + (long long) (3 * (r + 1)) * asz;
+            nk[q] = __ldg (rp);
+            ntt[q] = __ldg (rp + asz);
+            ncd[q] = __ldg (rp + 2 * asz);
+          }
+        }
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
           i_lo[q] = -1; i_hi[q] = -1; g_lo[q] = 0.0; g_hi[q] = 0.0;
           double rho = 0.0;                     // w . coef
 #pragma unroll
-          for (int s = 0; s < NS; s++) rho = __fma_rn ((double) M.r_coef[r][s], wc[q][s], rho);
+          for (int s = 0; s < NS; s++) rho = __fma_rn (sCf[r * NS + s], wc[q][s], rho);
           if (on[q] && rho != 0.0) {
-            // the lookup of k_adj_rates for this cell
-            const double *rp = adj + (long long) (A.rates_idx + 3 * r) * asz + AO (c0 + lane, j0 + CPT * wq + q);
-            const double k = __ldg (rp), tt = __ldg (rp + asz), cd = __ldg (rp + 2 * asz);
+            const double k = ck[q], tt = ctt[q], cd = ccd[q];
             // inputs |n_in| from the staged state (clamped in mode 2)
             const double *stq = sST + (CPT * wq + q + 3) * SC + lane + 3;
             // d/dn_s of k prod |n_in|: per input, k sign(n) prod of the others

@@ -167,6 +167,7 @@ struct Ctx {
   int adj_tab_smem = 0;               // table gradients accumulate in shared memory
   int adj_lam = 0;                    // lam buffer holding the current cotangent
   bool adj_fwd = false;
+  bool adj_stored = false;            // single segment: the forward kept n0, n* of every step
   cudaGraphExec_t adj_graph = nullptr;   // the whole reverse sweep
   int occ_fused[2][2][N_TILE_CFG_MAX] = {};   // [stage_eabs][stage 2][tile]
 };
@@ -1254,11 +1255,13 @@ adj_enqueue_sweep (Ctx *c)
   int lam = 0;
   for (int seg = c->adj_nseg - 1; seg >= 0; seg--) {
     const int k0 = seg * c->adj_ck, k1 = std::min (c->adj_nsteps, k0 + c->adj_ck);
-    if ((r = adj_copy (c, false, 0, adj_ckpt (c, seg)))) return r;
-    for (int k = k0; k < k1; k++) {
-      if ((r = adj_frozen_step (c, k, false))) return r;
-      if ((r = adj_keep (c, adj_seg_n0 (c, k - k0), adj_seg_ns (c, k - k0)))) return r;
-      if (k + 1 < k1 && (r = run_fused (c, true, 0, 0, k))) return r;
+    if (!c->adj_stored) {                       // recompute the segment from its checkpoint
+      if ((r = adj_copy (c, false, 0, adj_ckpt (c, seg)))) return r;
+      for (int k = k0; k < k1; k++) {
+        if ((r = adj_frozen_step (c, k, false))) return r;
+        if ((r = adj_keep (c, adj_seg_n0 (c, k - k0), adj_seg_ns (c, k - k0)))) return r;
+        if (k + 1 < k1 && (r = run_fused (c, true, 0, 0, k))) return r;
+      }
     }
     for (int k = k1 - 1; k >= k0; k--) {
       if ((r = run_vjp (c, 1, adj_seg_ns (c, k - k0), adj_lam_idx (c, lam), 0, adj_lams_idx (c), k))) return r;
@@ -1270,6 +1273,52 @@ adj_enqueue_sweep (Ctx *c)
   if ((r = adj_copy (c, false, 0, adj_final (c)))) return r;
   if ((r = do_ext_bnd (c, 0))) return r;
   return do_periodic (c, 0, 1);
+}
+
+// The forward run of a single-segment adjoint (every state fits in the
+// segment buffer): the lean step's two stages with n0 and n* kept between
+// them, so the reverse sweep recomputes nothing.  The step sizes follow the
+// CFL rule from h_attempt as arcos_run takes them (recorded in the step log),
+// or the frozen record.
+int
+adj_forward_keep (Ctx *c, int nsteps, double h_attempt, bool frozen)
+{
+  int r;
+  std::vector<DevState> st0;
+  if ((r = read_states (c, st0))) return r;
+  if ((r = small_dt_pending (c, st0))) return r;
+  const int step0 = st0[0].step;
+  if (!frozen) {
+    // as arcos_run: h_attempt, the dmax slot and the clamp flags in one write
+    c->st_stage = st0;
+    for (auto &st : c->st_stage) {
+      st.h_attempt = h_attempt;
+      st.dmax_key[st.step & 1] = dkey (-1.0);
+      st.neg[st.step & 1] = 1;
+      st.neg[(st.step + 1) & 1] = 0;
+    }
+    CK (cudaMemcpyAsync (c->st_d, c->st_stage.data (), sizeof (DevState) * c->nfam, cudaMemcpyHostToDevice,
+                         c->stream));
+    if ((r = do_dmax (c, 0, 0))) return r;
+    k_cfl<<<(c->nfam + 127) / 128, 128, 0, c->stream>>> (c->M, c->st_d, c->nfam, 0);
+    CKL ();
+  }
+  for (int k = 0; k < nsteps; k++) {
+    if ((r = frozen ? run_fused (c, false, 0, 1, k) : run_fused (c, false, 0))) return r;
+    if ((r = adj_keep (c, adj_seg_n0 (c, k), adj_seg_ns (c, k)))) return r;
+    if ((r = frozen ? run_fused (c, true, 0, 0, k) : run_fused (c, true, 1))) return r;
+  }
+  if (!frozen) {
+    CK (cudaStreamSynchronize (c->stream));
+    std::vector<double> dts (nsteps);
+    for (int f = 0; f < c->nfam; f++) {
+      const int n = std::min (nsteps, std::max (0, c->dt_cap - step0));
+      CK (cudaMemcpy (dts.data (), c->dtlog_d + (size_t) f * c->dt_cap + step0, sizeof (double) * n,
+                      cudaMemcpyDeviceToHost));
+      for (int k = 0; k < n; k++) c->adj_hs[(size_t) f * nsteps + k] = dts[k];
+    }
+  }
+  return ARCOS_OK;
 }
 
 int
@@ -2874,7 +2923,12 @@ arcos_adj_forward (void *ctx, int nsteps, int ckpt_every, double h_attempt, cons
     CK (cudaMemcpyAsync (c->adj_hs_d, c->adj_hs.data (), sizeof (double) * c->adj_hs.size (), cudaMemcpyHostToDevice, c->stream));
   }
   std::vector<double> dts;
-  for (int seg = 0; seg < c->adj_nseg; seg++) {
+  c->adj_stored = c->adj_nseg == 1;
+  if (c->adj_stored) {
+    if ((r = adj_copy (c, true, 0, adj_ckpt (c, 0)))) return r;
+    if ((r = adj_forward_keep (c, nsteps, h_attempt, h_seq != nullptr))) return r;
+  }
+  for (int seg = 0; seg < c->adj_nseg && !c->adj_stored; seg++) {
     const int k0 = seg * c->adj_ck, k1 = std::min (nsteps, k0 + c->adj_ck);
     if ((r = adj_copy (c, true, 0, adj_ckpt (c, seg)))) return r;
     if (h_seq) {
@@ -2890,7 +2944,7 @@ arcos_adj_forward (void *ctx, int nsteps, int ckpt_every, double h_attempt, cons
   if ((r = adj_copy (c, true, 0, adj_final (c)))) return r;
   if (!h_seq)
     CK (cudaMemcpyAsync (c->adj_hs_d, c->adj_hs.data (), sizeof (double) * c->adj_hs.size (), cudaMemcpyHostToDevice, c->stream));
-  else {
+  if (h_seq || c->adj_stored) {
     if ((r = do_ext_bnd (c, 0))) return r;
     if ((r = do_periodic (c, 0, 1))) return r;
   }

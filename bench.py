@@ -354,12 +354,14 @@ def _time_sweep(tree, stream) -> float:
     return e0.elapsed_time(e1)
 
 
-def extra_adjoint(stream, K: int = 64, ck: int = 8, ndir: int = 32):
-    """Discrete adjoint: 256 x 512 grid, 64 RK2 steps, checkpoints every 8;
-    J = 1/2 sum (n_e(T) - n_target)^2 cell_volume; reverse sweep time over the
-    forward run's time, and central finite differences (step 1e-6 relative,
-    32 seeded smooth directions over densities, mobility, diffusion and the
-    256 table values) of the frozen-step forward."""
+def extra_adjoint(stream, K: int = 64, ck: int = 64, ndir: int = 32):
+    """Discrete adjoint: 256 x 512 grid, 64 RK2 steps, every state kept by the
+    forward run (one segment: no recomputation in the reverse sweep; the
+    sweep with checkpoints every 8 steps is timed beside it); J = 1/2 sum
+    (n_e(T) - n_target)^2 cell_volume; reverse sweep time over the forward
+    run's time, and central finite differences (step 1e-6 relative, 32 seeded
+    smooth directions over densities, mobility, diffusion and the 256 table
+    values) of the frozen-step forward."""
     import numpy as np
     from arcos_b200 import workloads
     from arcos_b200.adjoint import Adjoint, cell_volume, fd_objective_difference, smooth_direction
@@ -401,6 +403,8 @@ def extra_adjoint(stream, K: int = 64, ck: int = 8, ndir: int = 32):
     e1.synchronize()
     fwd_ms = e0.elapsed_time(e1)
     apply(d0, mu0, D0, base_vals)
+    adj.forward(K, ck, h=50.0)              # the first call allocates the state buffers
+    apply(d0, mu0, D0, base_vals)
     e0.record(stream)
     hs = adj.forward(K, ck, h=50.0)
     e1.record(stream)
@@ -416,6 +420,13 @@ def extra_adjoint(stream, K: int = 64, ck: int = 8, ndir: int = 32):
     adj.set_cotangent(0, 0, (ne - target) * vol)
     adj.set_cotangent(0, 1, np.zeros_like(ne))
     g = adj.backward()
+    # the same sweep with checkpoints every 8 steps (segments recomputed)
+    apply(d0, mu0, D0, base_vals)
+    adj.forward(K, 8, h=50.0)
+    for _ in range(2):                      # the first call captures the sweep's CUDA graph
+        adj.set_cotangent(0, 0, (ne - target) * vol)
+        adj.set_cotangent(0, 1, np.zeros_like(ne))
+        bwd8_ms = _time_sweep(tree, stream)
     # finite differences
     eps, worst = 1e-6, 0.0
     for _ in range(ndir):
@@ -435,12 +446,15 @@ def extra_adjoint(stream, K: int = 64, ck: int = 8, ndir: int = 32):
         fd = fd_objective_difference(outs[0], outs[1], target, vol, eps)
         worst = max(worst, abs(fd - pred) / abs(fd))
     tree.close()
-    return {"workload": "256x512 grid, 2 species (ions immobile), 64 RK2 steps, checkpoints every 8, "
+    return {"workload": "256x512 grid, 2 species (ions immobile), 64 RK2 steps, every state kept, "
                         "gradients wrt n_e(0), n_i(0), mobility, diffusion, 256 table values",
-            "forward_ms": fwd_ms, "forward_with_checkpoints_ms": fwd_ck_ms, "adjoint_ms": bwd_ms,
+            "forward_ms": fwd_ms, "forward_keeping_states_ms": fwd_ck_ms, "adjoint_ms": bwd_ms,
             "adjoint_timed": "one arcos_adj_backward call, CUDA events",
-            "adjoint_over_forward": bwd_ms / fwd_ms, "fd_directions": ndir, "fd_step": eps,
-            "fd_max_rel_err": worst}
+            "adjoint_over_forward": bwd_ms / fwd_ms,
+            "adjoint_with_forward_overhead_over_forward": (bwd_ms + fwd_ck_ms - fwd_ms) / fwd_ms,
+            "adjoint_ms_checkpoints_every_8": bwd8_ms,
+            "adjoint_over_forward_checkpoints_every_8": bwd8_ms / fwd_ms,
+            "fd_directions": ndir, "fd_step": eps, "fd_max_rel_err": worst}
 
 
 def extra_kinetic(stream, K: int = 20):
@@ -471,8 +485,14 @@ def extra_kinetic(stream, K: int = 20):
     ns = pb.model.no_species
     _load(tree, pb)
     adj = Adjoint(tree)
-    Ka, ck = 16, 8
+    Ka, ck = 16, 16                         # one segment: every state kept by the forward run
+    adj.forward(Ka, ck, h=50.0)             # the first call allocates the state buffers
+    _load(tree, pb)
+    e0.record(stream)
     adj.forward(Ka, ck, h=50.0)
+    e1.record(stream)
+    e1.synchronize()
+    fwd_keep_ms = e0.elapsed_time(e1)
     for g, sp in enumerate(pb.specs):
         vol = cell_volume(sp, pb.params.dr(0), pb.params.dz(0))
         adj.set_cotangent(g, 0, vol)
@@ -484,12 +504,25 @@ def extra_kinetic(stream, K: int = 20):
         for s in range(1, ns):
             adj.set_cotangent(g, s, np.zeros(sp.shape))
     bwd = _time_sweep(tree, stream)
+    # the same sweep with checkpoints every 8 steps (segments recomputed)
+    _load(tree, pb)
+    adj.forward(Ka, 8, h=50.0)
+    for _ in range(2):                      # the first call captures the sweep's CUDA graph
+        for g, sp in enumerate(pb.specs):
+            adj.set_cotangent(g, 0, cell_volume(sp, pb.params.dr(0), pb.params.dz(0)))
+            for s in range(1, ns):
+                adj.set_cotangent(g, s, np.zeros(sp.shape))
+        bwd8 = _time_sweep(tree, stream)
     tree.close()
     return {"workload": f"{len(pb.specs)} instances, {pb.cells} cells, {ns} species, "
                         f"{len(pb.model.reactions)} reactions (1000-entry tables)",
             "cells": pb.cells, "ms_per_step": ms, "value": pb.cells * ns / (ms / 1e3),
             "tile_autotune_ms_per_step": {str(k): v for k, v in tune.items()},
-            "adjoint_steps": Ka, "adjoint_ms": bwd, "adjoint_over_forward": bwd / (ms * Ka),
+            "adjoint_steps": Ka, "adjoint_states": "every state kept by the forward run (one segment)",
+            "adjoint_ms": bwd, "adjoint_over_forward": bwd / (ms * Ka),
+            "forward_keeping_states_ms": fwd_keep_ms,
+            "adjoint_with_forward_overhead_over_forward": (bwd + fwd_keep_ms - ms * Ka) / (ms * Ka),
+            "adjoint_ms_checkpoints_every_8": bwd8, "adjoint_over_forward_checkpoints_every_8": bwd8 / (ms * Ka),
             "adjoint_timed": "one arcos_adj_backward call, CUDA events",
             "table_grad_norm": float(sum(np.linalg.norm(t) for t in gr.tables))}
 

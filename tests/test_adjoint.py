@@ -139,12 +139,15 @@ def device_J(tree, adj, pb, q, hs, K, ck, target, vol):
     return objective(device_ne(tree, adj, pb, q, hs, K, ck), target, vol)
 
 
+@pytest.mark.parametrize("ck", [4, 16])
 @pytest.mark.parametrize("field", ["uniform", "wavy"])
 @pytest.mark.parametrize("which", [("dens",), ("mu",), ("D",), ("table",), ("dens", "mu", "D", "table")])
-def test_adjoint_matches_device_fd(cuda_device, which, field):
+def test_adjoint_matches_device_fd(cuda_device, which, field, ck):
     """Uniform applied field, and the non-uniform wavy field (radial drift,
-    sign changes of the velocity inside a warp, |E| over the whole table)."""
-    K, ck = 16, 4
+    sign changes of the velocity inside a warp, |E| over the whole table);
+    checkpoints every 4 steps (segments recomputed), or one segment (every
+    state kept by the forward run)."""
+    K = 16
     pb, tree, adj, base, hs, target, vol = device_setup(32, 64, K, ck, seed=1, field=field)
     grads, J0 = device_grads(tree, adj, target, vol)
     assert J0 > 0
@@ -192,8 +195,9 @@ def test_adjoint_matches_oracle_fd(cuda_device, field):
         assert abs(fd - pr) <= TOL * abs(fd), (fd, pr)
 
 
-def test_adjoint_keeps_forward_state(cuda_device):
-    K, ck = 6, 4
+@pytest.mark.parametrize("ck", [4, 6])
+def test_adjoint_keeps_forward_state(cuda_device, ck):
+    K = 6
     pb, tree, adj, base, hs, target, vol = device_setup(32, 64, K, ck, seed=3)
     before = [tree.download(0, "dens", s) for s in range(2)]
     device_grads(tree, adj, target, vol)
@@ -201,9 +205,10 @@ def test_adjoint_keeps_forward_state(cuda_device):
         assert np.array_equal(tree.download(0, "dens", s)[0, 2:-2, 2:-2], before[s][0, 2:-2, 2:-2])
 
 
-def test_frozen_forward_reproduces_cfl_run(cuda_device):
+@pytest.mark.parametrize("ck", [4, 10])
+def test_frozen_forward_reproduces_cfl_run(cuda_device, ck):
     """The frozen-step forward with the recorded sizes gives the CFL run's state."""
-    K, ck = 10, 4
+    K = 10
     pb, tree, adj, base, hs, target, vol = device_setup(32, 64, K, ck, seed=4)
     a = [tree.download(0, "dens", s) for s in range(2)]
     apply_device(tree, pb, base)
@@ -212,13 +217,36 @@ def test_frozen_forward_reproduces_cfl_run(cuda_device):
         assert np.array_equal(tree.download(0, "dens", s)[0, 2:-2, 2:-2], a[s][0, 2:-2, 2:-2])
 
 
-@pytest.mark.parametrize("field", ["uniform", "wavy"])
-def test_kinetic_batch_adjoint_matches_fd(cuda_device, field):
+def test_kept_states_give_the_checkpointed_gradients(cuda_device):
+    """One segment (states kept by the forward run) and checkpoints every 3
+    steps (segments recomputed with the recorded step sizes) give the same
+    gradients: the recomputed states are the forward's, bit for bit, so the
+    density, mobility and diffusion gradients are identical (the table
+    gradients to the order of their atomic sums)."""
+    K = 9
+    out = []
+    for ck in (3, 9):
+        pb, tree, adj, base, hs, target, vol = device_setup(32, 64, K, ck, seed=6, field="wavy")
+        g, _ = device_grads(tree, adj, target, vol)
+        out.append((g, hs))
+        tree.close()
+    (ga, ha), (gb, hb) = out
+    assert np.array_equal(ha, hb)
+    for s in range(2):
+        assert np.array_equal(ga.dens0[0][s], gb.dens0[0][s]), s
+    assert np.array_equal(ga.mobility, gb.mobility) and ga.diffusion == gb.diffusion
+    # the table gradients are sums of atomic additions, whose order varies
+    ta, tb = ga.tables[0], gb.tables[0]
+    assert np.max(np.abs(ta - tb)) <= 1e-12 * np.max(np.abs(tb))
+
+
+@pytest.mark.parametrize("field,ck", [("uniform", 3), ("wavy", 6)])
+def test_kinetic_batch_adjoint_matches_fd(cuda_device, field, ck):
     """Three families of different sizes, six species (ions mobile), nine
     reactions with one- and two-input terms: the adjoint of the total electron
     number at T with respect to the initial densities of every species and
     every table value, against central differences of the frozen-step
-    forward.  Two checkpoint segments."""
+    forward.  Two checkpoint segments, or one (every state kept)."""
     pb = workloads.kinetic_batch(n_inst=3, points=200, sizes_r=(24, 40), sizes_z=(32, 48), seed=1,
                                  field=field)
     ns = pb.model.no_species
@@ -235,7 +263,7 @@ def test_kinetic_batch_adjoint_matches_fd(cuda_device, field):
         for r, re in enumerate(pb.model.reactions):
             tree.set_table_values(r, vals[r], re.table.underflow, re.table.overflow)
 
-    K, ck = 6, 3
+    K = 6
     adj = Adjoint(tree)
     apply(pb.dens, tabs)
     hs = adj.forward(K, ck, h=50.0)
