@@ -78,7 +78,15 @@ class ClockSampler:
             self.mx = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
             self.th = threading.Thread(target=self._poll_nvml, daemon=True)
             self.th.start()
-            return
+            t0 = time.time()                 # the polling runs before the timed region starts
+            while len(self.lines) < 3 and self.th.is_alive() and time.time() - t0 < 5:
+                time.sleep(0.001)
+            if self.lines:
+                return
+            self.stop_flag = True            # NVML gave nothing: nvidia-smi instead
+            self.th.join(timeout=2)
+            self.th = None
+            self.nv = None
         except Exception:
             self.nv = None
         try:
@@ -547,6 +555,46 @@ def _refine_state(tree_like, pb, upload):
     upload(d0, d1, eabs)
 
 
+def extra_field(stream, K: int = 100):
+    """The field solved on the device at both stages of every step (c0:
+    128 x 256, immobile ions; the same with 16 theta planes, solved by theta
+    modes) and photoionization (two terms, 128 x 256 and 128 x 256 x 16,
+    fixed field): device time per RK2 step over K steps replayed from the
+    step graph, CUDA events."""
+    from arcos_b200 import workloads
+    from arcos_b200.cdr import CdrTree
+    out = {}
+
+    def timed(tree, name, cells, ns):
+        tree.run(3, 50.0)                       # warm-up (captures the step graph)
+        e0, e1 = _events(stream)
+        e0.record(stream)
+        tree.run(K, 50.0)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / K
+        out[name] = {"ms_per_step": ms, "cells": cells, "value": cells * ns / (ms / 1e3)}
+
+    for nt in (1, 16):
+        pb = workloads.plain(nr=128, nz=256, ntheta=nt, ion_mass=0.0, noise=0.3 if nt > 1 else 0.0, seed=0)
+        tree = CdrTree(pb.params, pb.model, pb.specs, stream=stream.cuda_stream)
+        for s in range(2):
+            tree.upload(0, "dens", pb.dens[0][s], s)
+        tree.cdr_calc_charge_r(0)
+        tree.set_field_poisson(True)
+        timed(tree, "field_in_loop_128x256" + ("" if nt == 1 else f"x{nt}"), 128 * 256 * nt, 2)
+        tree.close()
+    for nt in (1, 16):
+        pb = workloads.photo(nr=128, nz=256, ntheta=nt, noise=0.3 if nt > 1 else 0.0, seed=0)
+        tree = CdrTree(pb.params, pb.model, pb.specs, stream=stream.cuda_stream)
+        _load(tree, pb)
+        timed(tree, "photo_128x256" + ("" if nt == 1 else f"x{nt}"), 128 * 256 * nt, pb.model.no_species)
+        tree.close()
+    out["workload"] = ("field solve in the loop (sine transform in z, tridiagonal in r, theta modes in 3-D) "
+                       "and photoionization (2 terms, 5 species), device time per RK2 step")
+    return out
+
+
 def extra_refine(stream, calls: int = 5):
     """Refinement criteria (cdr_refine, src/cdr.c:1630-1682) of the
     512 x 1024 x 16 grid with the reference's default parameters: one
@@ -746,7 +794,8 @@ def run_device(args):
     if rank == 0 and not args.no_extras:
         wanted = set(args.extras.split(","))
         for name, fn in (("amr_batched", extra_amr), ("adjoint", extra_adjoint),
-                         ("kinetic_batch", extra_kinetic), ("refine", extra_refine)):
+                         ("kinetic_batch", extra_kinetic), ("refine", extra_refine),
+                         ("field", extra_field)):
             if name not in wanted:
                 continue
             try:
@@ -787,7 +836,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-AMR, adjoint and kinetic-batch measurements")
-    ap.add_argument("--extras", default="amr_batched,adjoint,kinetic_batch,refine",
+    ap.add_argument("--extras", default="amr_batched,adjoint,kinetic_batch,refine,field",
                     help="comma-separated subset of the extra measurements")
     ap.add_argument("--exact", action="store_true", help="bit-exact flux limiter")
     ap.add_argument("--tile", type=int, default=None,
