@@ -1326,6 +1326,7 @@ adj_check (Ctx *c)
 {
   if (!lean_ok (c))
     return fail (ARCOS_ERR_STATE, "adjoint: needs single-grid families, fixed field, the division-free limiter and TMA staging");
+  if (c->photo_n) return fail (ARCOS_ERR_STATE, "adjoint: photoionization is not differentiated");
   for (auto &P : c->pd_h)
     if (P.ntheta != 1) return fail (ARCOS_ERR_ARG, "adjoint: 2-D grids only");
   return ARCOS_OK;
@@ -2857,6 +2858,7 @@ arcos_run_prepare (void *ctx, double h)
   int r = chk_committed (c);
   if (r) return r;
   if (!c->fused_ok) return fail (ARCOS_ERR_STATE, "fused path needs single-grid families");
+  if (c->photo_n) return fail (ARCOS_ERR_STATE, "the fused path has no photoionization (arcos_run takes the general step)");
   if ((r = set_h_attempt (c, h))) return r;
   if ((r = reset_dmax (c, 0))) return r;
   if ((r = do_dmax (c, 0, 0))) return r;
@@ -2884,6 +2886,7 @@ arcos_run_enqueue (void *ctx, int nsteps)
   int r = chk_committed (c);
   if (r) return r;
   if (!c->graph2) return fail (ARCOS_ERR_STATE, "call arcos_run_prepare first");
+  if (c->photo_n) return fail (ARCOS_ERR_STATE, "the fused path has no photoionization (arcos_run takes the general step)");
   if ((nsteps & 1) && !lean_ok (c))
     return fail (ARCOS_ERR_STATE, "nsteps must be even on this path (the state alternates between sets)");
   for (int k = 0; k < nsteps / 2; k++) CK (cudaGraphLaunch (c->graph2, c->stream));

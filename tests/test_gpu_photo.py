@@ -88,3 +88,16 @@ def test_photo_refuses_trees(cuda_device):
     with pytest.raises(Exception):
         t.set_photo(workloads.photo_model())
     t.close()
+
+
+def test_photo_refuses_the_fused_entry_and_the_adjoint(cuda_device):
+    """The fused two-launch step and the discrete adjoint carry no
+    photoionization: with it on they refuse instead of dropping it."""
+    import ctypes as C
+    from arcos_b200.adjoint import Adjoint
+    pb = workloads.photo(nr=16, nz=24, seed=2)
+    dev = device_tree(pb, exact=False)
+    assert dev.L.arcos_run_prepare(dev.h, C.c_double(50.0)) != 0
+    with pytest.raises(Exception):
+        Adjoint(dev).forward(2, 2, h=50.0)
+    dev.close()
