@@ -2341,13 +2341,14 @@ pois_build (Ctx *c, double es, PoisArgs &A, double *&buf)
     tc[i] = rp / (ri * dr * dr);
   }
   const size_t nn = (size_t) nr * nz * nt;
-  const size_t total = St.size () + 3 * (size_t) nz + 2 * (size_t) nr + mk.size () + 4 * (size_t) nt + 5 * nn;
+  const size_t total = 2 * St.size () + 3 * (size_t) nz + 2 * (size_t) nr + mk.size () + 4 * (size_t) nt + 5 * nn;
   cudaFree (buf);
   buf = nullptr;
   CK (cudaMalloc (&buf, sizeof (double) * total));
   double *q = buf;
   A.nr = nr; A.nz = nz; A.nt = nt; A.r0 = P.r0; A.dr = dr; A.dz = dz;
   A.St = q; q += St.size ();
+  A.Sk = q; q += St.size ();
   A.norm = q; q += nz;
   A.lam = q; q += nz;
   A.ta = q; q += nr;
@@ -2363,6 +2364,12 @@ pois_build (Ctx *c, double es, PoisArgs &A, double *&buf)
   A.dp = q; q += nn;
   A.phi = q; q += nn;
   CK (cudaMemcpy ((void *) A.St, St.data (), sizeof (double) * St.size (), cudaMemcpyHostToDevice));
+  {
+    std::vector<double> Sk (St.size ());        // the same matrix, k-major
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < nz; j++) Sk[(size_t) k * nz + j] = St[(size_t) j * nz + k];
+    CK (cudaMemcpy ((void *) A.Sk, Sk.data (), sizeof (double) * Sk.size (), cudaMemcpyHostToDevice));
+  }
   CK (cudaMemcpy ((void *) A.norm, norm.data (), sizeof (double) * nz, cudaMemcpyHostToDevice));
   CK (cudaMemcpy ((void *) A.lam, lam.data (), sizeof (double) * nz, cudaMemcpyHostToDevice));
   CK (cudaMemcpy ((void *) A.ta, ta.data (), sizeof (double) * nr, cudaMemcpyHostToDevice));

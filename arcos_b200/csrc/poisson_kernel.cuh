@@ -45,6 +45,7 @@ struct PoisArgs {
   int r0;                // the grid's first column (r of column c: (c + r0 + 1/2) dr)
   double dr, dz;
   const double *St;      // [j][k] = sin(pi (k+1) (j+1/2) / nz)
+  const double *Sk;      // [k][j], the same values k-major (coalesced for the inverse)
   const double *norm;    // [k] = sum_j S[k][j]^2
   const double *lam;     // [k] = -4/dz^2 sin^2(pi (k+1) / (2 nz))
   const double *ta, *tc; // [i] = r_{i-1/2} / (r_i dr^2), r_{i+1/2} / (r_i dr^2)
@@ -55,23 +56,43 @@ struct PoisArgs {
   double *qh, *ph, *cp, *dp, *phi;   // [m][i][k] (phi: [m][i][j]) scratch, nt * nr * nz each
 };
 
+// The sums below run in the host solver's order (index ascending, one
+// addition per term); their operands are loaded PF terms ahead, so the
+// memory latency is paid once per PF terms instead of once per term.
+constexpr int POIS_PF = 8;
+
 // qh[m][i][k] = (sum_j -charge_m(i, j) S[k][j]) / norm[k]
 __global__ void
 k_pois_fwd (const PatchDesc *__restrict__ pd, int patch, int set, PoisArgs A)
 {
   const PatchDesc &P = pd[patch];
-  const int nn = A.nr * A.nz, n = nn * A.nt;
+  const int nn = A.nr * A.nz, n = nn * A.nt, nz = A.nz;
   const double *ch = P.arr (set, K_CHARGE);
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const int m = t / nn, u = t - m * nn;
-    const int i = u / A.nz, k = u - i * A.nz;
+    const int i = u / nz, k = u - i * nz;
+    const double *cp = ch + P.off (i, 0, m);          // + j pitch
+    const double *sp = A.St + k;                       // + j nz
     double s = 0.0;
-    for (int j = 0; j < A.nz; j++) s += -ch[P.off (i, j, m)] * A.St[(size_t) j * A.nz + k];
+    int j = 0;
+    for (; j + POIS_PF <= nz; j += POIS_PF) {
+      double cv[POIS_PF], sv[POIS_PF];
+#pragma unroll
+      for (int q = 0; q < POIS_PF; q++) {
+        cv[q] = cp[(long long) (j + q) * P.pitch];
+        sv[q] = sp[(size_t) (j + q) * nz];
+      }
+#pragma unroll
+      for (int q = 0; q < POIS_PF; q++) s += -cv[q] * sv[q];
+    }
+    for (; j < nz; j++) s += -cp[(long long) j * P.pitch] * sp[(size_t) j * nz];
     A.qh[t] = s / A.norm[k];
   }
 }
 
-// One (theta mode, z mode) per thread: the tridiagonal system in r (Thomas).
+// One (theta mode, z mode) per thread: the tridiagonal system in r (Thomas),
+// the coefficients and right-hand sides of PF rows loaded ahead of the
+// recurrence, cp and dp of PF rows ahead of the back substitution.
 __global__ void
 k_pois_tri (PoisArgs A)
 {
@@ -82,28 +103,52 @@ k_pois_tri (PoisArgs A)
   const size_t base = (size_t) m * nr * nz;
   const double lam = A.lam[k];
   const double *mk = A.mk + (size_t) m * nr;
-  auto bcoef = [&] (int i) {
-    double b = -(A.ta[i] + A.tc[i]) + lam + mk[i];
-    if (i == nr - 1) b -= A.tc[i];       // phi_{nr} = -phi_{nr-1} (Dirichlet at r = L_r)
+  auto bcoef = [&] (int i, double ta, double tc, double mki) {
+    double b = -(ta + tc) + lam + mki;
+    if (i == nr - 1) b -= tc;            // phi_{nr} = -phi_{nr-1} (Dirichlet at r = L_r)
     return b;
   };
-  const double b0 = bcoef (0);
+  const double b0 = bcoef (0, A.ta[0], A.tc[0], mk[0]);
   double cpv = (nr - 1 == 0 ? 0.0 : A.tc[0]) / b0;
   double dpv = A.qh[base + k] / b0;
   A.cp[base + k] = cpv;
   A.dp[base + k] = dpv;
-  for (int i = 1; i < nr; i++) {
-    const double mm = bcoef (i) - A.ta[i] * cpv;
-    cpv = (i == nr - 1 ? 0.0 : A.tc[i]) / mm;
-    dpv = (A.qh[base + (size_t) i * nz + k] - A.ta[i] * dpv) / mm;
-    A.cp[base + (size_t) i * nz + k] = cpv;
-    A.dp[base + (size_t) i * nz + k] = dpv;
+  for (int i0 = 1; i0 < nr; i0 += POIS_PF) {
+    double ta[POIS_PF], tc[POIS_PF], mm[POIS_PF], qq[POIS_PF];
+#pragma unroll
+    for (int q = 0; q < POIS_PF; q++) {
+      const int i = i0 + q < nr ? i0 + q : nr - 1;
+      ta[q] = A.ta[i]; tc[q] = A.tc[i]; mm[q] = mk[i];
+      qq[q] = A.qh[base + (size_t) i * nz + k];
+    }
+#pragma unroll
+    for (int q = 0; q < POIS_PF; q++) {
+      const int i = i0 + q;
+      if (i >= nr) break;
+      const double mq = bcoef (i, ta[q], tc[q], mm[q]) - ta[q] * cpv;
+      cpv = (i == nr - 1 ? 0.0 : tc[q]) / mq;
+      dpv = (qq[q] - ta[q] * dpv) / mq;
+      A.cp[base + (size_t) i * nz + k] = cpv;
+      A.dp[base + (size_t) i * nz + k] = dpv;
+    }
   }
   double p = dpv;
   A.ph[base + (size_t) (nr - 1) * nz + k] = p;
-  for (int i = nr - 2; i >= 0; i--) {
-    p = A.dp[base + (size_t) i * nz + k] - A.cp[base + (size_t) i * nz + k] * p;
-    A.ph[base + (size_t) i * nz + k] = p;
+  for (int i0 = nr - 2; i0 >= 0; i0 -= POIS_PF) {
+    double cc[POIS_PF], dd[POIS_PF];
+#pragma unroll
+    for (int q = 0; q < POIS_PF; q++) {
+      const int i = i0 - q >= 0 ? i0 - q : 0;
+      cc[q] = A.cp[base + (size_t) i * nz + k];
+      dd[q] = A.dp[base + (size_t) i * nz + k];
+    }
+#pragma unroll
+    for (int q = 0; q < POIS_PF; q++) {
+      const int i = i0 - q;
+      if (i < 0) break;
+      p = dd[q] - cc[q] * p;
+      A.ph[base + (size_t) i * nz + k] = p;
+    }
   }
 }
 
@@ -111,13 +156,25 @@ k_pois_tri (PoisArgs A)
 __global__ void
 k_pois_inv (PoisArgs A)
 {
-  const int nn = A.nr * A.nz, n = nn * A.nt;
+  const int nn = A.nr * A.nz, n = nn * A.nt, nz = A.nz;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const int m = t / nn, u = t - m * nn;
-    const int i = u / A.nz, j = u - i * A.nz;
-    const double *ph = A.ph + (size_t) m * nn + (size_t) i * A.nz;
+    const int i = u / nz, j = u - i * nz;
+    const double *ph = A.ph + (size_t) m * nn + (size_t) i * nz;
+    const double *sk = A.Sk + j;                       // + k nz
     double s = 0.0;
-    for (int k = 0; k < A.nz; k++) s += ph[k] * A.St[(size_t) j * A.nz + k];
+    int k = 0;
+    for (; k + POIS_PF <= nz; k += POIS_PF) {
+      double pv[POIS_PF], sv[POIS_PF];
+#pragma unroll
+      for (int q = 0; q < POIS_PF; q++) {
+        pv[q] = ph[k + q];
+        sv[q] = sk[(size_t) (k + q) * nz];
+      }
+#pragma unroll
+      for (int q = 0; q < POIS_PF; q++) s += pv[q] * sv[q];
+    }
+    for (; k < nz; k++) s += ph[k] * sk[(size_t) k * nz];
     A.phi[t] = s;
   }
 }
