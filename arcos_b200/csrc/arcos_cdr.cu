@@ -771,17 +771,16 @@ int
 device_poisson (Ctx *c, int set)
 {
   const PoisArgs &A = c->pois_args;
-  const int n = A.nr * A.nz * A.nt;
-  const int b = std::min ((n + 255) / 256, 8 * c->num_sms);
   const int cells = (A.nr + 4) * (A.nz + 4);
   const int bd = std::min ((cells + 127) / 128, 8 * c->num_sms);
   const PatchDesc &P = c->pd_h[0];
   auto plane0 = [&] (int kind) { return P.arr (set, kind) + (long long) (0 - P.theta0) * P.plane_stride; };
   if (A.nt > 1)                                 // cdr_dft_charge_r
     k_theta_dft<0><<<bd, 128, 0, c->stream>>> (plane0 (K_CHARGE), P.pitch, P.plane_stride, A);
-  k_pois_fwd<<<b, 256, 0, c->stream>>> (c->pd_d, 0, set, A);
+  const size_t rowb = sizeof (double) * A.nz;
+  k_pois_fwd<<<A.nr * A.nt, 256, rowb, c->stream>>> (c->pd_d, 0, set, A);
   k_pois_tri<<<(A.nz * A.nt + 127) / 128, 128, 0, c->stream>>> (A);
-  k_pois_inv<<<b, 256, 0, c->stream>>> (A);
+  k_pois_inv<<<A.nr * A.nt, 256, rowb, c->stream>>> (A);
   // set 1 is the RK2 intermediate grid, fresh every step in the reference
   const int fresh = set == 1;
   const long long len = (long long) (A.nz + 4) * P.pitch * (A.nt + (fresh && A.nt > 1 ? 4 : 0));
@@ -804,8 +803,6 @@ device_photo (Ctx *c, int set)
   const PatchDesc &P = c->pd_h[0];
   const PoisArgs &A0 = c->photo_args[0];
   const int nt = A0.nt;
-  const int n = A0.nr * A0.nz * nt;
-  const int b = std::min ((n + 255) / 256, 8 * c->num_sms);
   const int bd = std::min (((A0.nr + 4) * (A0.nz + 4) + 127) / 128, 8 * c->num_sms);
   const int be = (int) std::min<long long> ((P.asz + 255) / 256, 8 * c->num_sms);
   const long long p0 = (long long) (0 - P.theta0) * P.plane_stride;
@@ -815,9 +812,9 @@ device_photo (Ctx *c, int set)
   if (nt > 1) k_theta_dft<0><<<bd, 128, 0, c->stream>>> (P.arr (set, K_CHARGE) + p0, P.pitch, P.plane_stride, A0);
   for (int t = 0; t < c->photo_n; t++) {
     const PoisArgs &A = c->photo_args[t];
-    k_pois_fwd<<<b, 256, 0, c->stream>>> (c->pd_d, 0, set, A);
+    k_pois_fwd<<<A.nr * A.nt, 256, sizeof (double) * A.nz, c->stream>>> (c->pd_d, 0, set, A);
     k_pois_tri<<<(A.nz * A.nt + 127) / 128, 128, 0, c->stream>>> (A);
-    k_pois_inv<<<b, 256, 0, c->stream>>> (A);
+    k_pois_inv<<<A.nr * A.nt, 256, sizeof (double) * A.nz, c->stream>>> (A);
     k_photo_field<<<bf, 256, 0, c->stream>>> (c->pd_d, 0, c->photo_d, A);
     if (nt > 1) k_theta_dft<1><<<bd, 128, 0, c->stream>>> (c->photo_d + p0, P.pitch, P.plane_stride, A);
     k_photo_add<<<be, 256, 0, c->stream>>> (c->pd_d, 0, set, c->photo_d, c->photo_A[t], c->photo_e, c->photo_pi);

@@ -57,36 +57,37 @@ struct PoisArgs {
 };
 
 // The sums below run in the host solver's order (index ascending, one
-// addition per term); their operands are loaded PF terms ahead, so the
+// addition per term); their matrix operands are loaded PF terms ahead, so the
 // memory latency is paid once per PF terms instead of once per term.
 constexpr int POIS_PF = 8;
 
-// qh[m][i][k] = (sum_j -charge_m(i, j) S[k][j]) / norm[k]
+// qh[m][i][k] = (sum_j -charge_m(i, j) S[k][j]) / norm[k]: a block per
+// (mode, row i) with -charge of the row in shared memory, threads over k.
 __global__ void
 k_pois_fwd (const PatchDesc *__restrict__ pd, int patch, int set, PoisArgs A)
 {
+  extern __shared__ double prow[];
   const PatchDesc &P = pd[patch];
-  const int nn = A.nr * A.nz, n = nn * A.nt, nz = A.nz;
-  const double *ch = P.arr (set, K_CHARGE);
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int m = t / nn, u = t - m * nn;
-    const int i = u / nz, k = u - i * nz;
-    const double *cp = ch + P.off (i, 0, m);          // + j pitch
-    const double *sp = A.St + k;                       // + j nz
+  const int nz = A.nz;
+  const int m = blockIdx.x / A.nr, i = blockIdx.x - m * A.nr;
+  if (m >= A.nt) return;
+  const double *cp = P.arr (set, K_CHARGE) + P.off (i, 0, m);     // + j pitch
+  for (int j = threadIdx.x; j < nz; j += blockDim.x) prow[j] = -cp[(long long) j * P.pitch];
+  __syncthreads ();
+  double *qh = A.qh + ((size_t) m * A.nr + i) * nz;
+  for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+    const double *sp = A.St + k;                                    // + j nz
     double s = 0.0;
     int j = 0;
     for (; j + POIS_PF <= nz; j += POIS_PF) {
-      double cv[POIS_PF], sv[POIS_PF];
+      double sv[POIS_PF];
 #pragma unroll
-      for (int q = 0; q < POIS_PF; q++) {
-        cv[q] = cp[(long long) (j + q) * P.pitch];
-        sv[q] = sp[(size_t) (j + q) * nz];
-      }
+      for (int q = 0; q < POIS_PF; q++) sv[q] = sp[(size_t) (j + q) * nz];
 #pragma unroll
-      for (int q = 0; q < POIS_PF; q++) s += -cv[q] * sv[q];
+      for (int q = 0; q < POIS_PF; q++) s += prow[j + q] * sv[q];
     }
-    for (; j < nz; j++) s += -cp[(long long) j * P.pitch] * sp[(size_t) j * nz];
-    A.qh[t] = s / A.norm[k];
+    for (; j < nz; j++) s += prow[j] * sp[(size_t) j * nz];
+    qh[k] = s / A.norm[k];
   }
 }
 
@@ -152,30 +153,31 @@ k_pois_tri (PoisArgs A)
   }
 }
 
-// phi[m][i][j] = sum_k ph[m][i][k] S[k][j]
+// phi[m][i][j] = sum_k ph[m][i][k] S[k][j]: a block per (mode, row i) with
+// the row of ph in shared memory, threads over j.
 __global__ void
 k_pois_inv (PoisArgs A)
 {
-  const int nn = A.nr * A.nz, n = nn * A.nt, nz = A.nz;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int m = t / nn, u = t - m * nn;
-    const int i = u / nz, j = u - i * nz;
-    const double *ph = A.ph + (size_t) m * nn + (size_t) i * nz;
-    const double *sk = A.Sk + j;                       // + k nz
+  extern __shared__ double prow[];
+  const int nz = A.nz;
+  const int m = blockIdx.x / A.nr, i = blockIdx.x - m * A.nr;
+  if (m >= A.nt) return;
+  const size_t row = ((size_t) m * A.nr + i) * nz;
+  for (int k = threadIdx.x; k < nz; k += blockDim.x) prow[k] = A.ph[row + k];
+  __syncthreads ();
+  for (int j = threadIdx.x; j < nz; j += blockDim.x) {
+    const double *sk = A.Sk + j;                                    // + k nz
     double s = 0.0;
     int k = 0;
     for (; k + POIS_PF <= nz; k += POIS_PF) {
-      double pv[POIS_PF], sv[POIS_PF];
+      double sv[POIS_PF];
 #pragma unroll
-      for (int q = 0; q < POIS_PF; q++) {
-        pv[q] = ph[k + q];
-        sv[q] = sk[(size_t) (k + q) * nz];
-      }
+      for (int q = 0; q < POIS_PF; q++) sv[q] = sk[(size_t) (k + q) * nz];
 #pragma unroll
-      for (int q = 0; q < POIS_PF; q++) s += pv[q] * sv[q];
+      for (int q = 0; q < POIS_PF; q++) s += prow[k + q] * sv[q];
     }
-    for (; k < nz; k++) s += ph[k] * sk[(size_t) k * nz];
-    A.phi[t] = s;
+    for (; k < nz; k++) s += prow[k] * sk[(size_t) k * nz];
+    A.phi[row + j] = s;
   }
 }
 
