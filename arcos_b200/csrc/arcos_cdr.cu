@@ -2338,7 +2338,7 @@ pois_build (Ctx *c, double es, PoisArgs &A, double *&buf)
     tc[i] = rp / (ri * dr * dr);
   }
   const size_t nn = (size_t) nr * nz * nt;
-  const size_t total = 2 * St.size () + 3 * (size_t) nz + 2 * (size_t) nr + mk.size () + 4 * (size_t) nt + 5 * nn;
+  const size_t total = 2 * St.size () + 3 * (size_t) nz + 2 * (size_t) nr + mk.size () + 4 * (size_t) nt + 6 * nn;
   cudaFree (buf);
   buf = nullptr;
   CK (cudaMalloc (&buf, sizeof (double) * total));
@@ -2358,9 +2358,40 @@ pois_build (Ctx *c, double es, PoisArgs &A, double *&buf)
   A.qh = q; q += nn;
   A.ph = q; q += nn;
   A.cp = q; q += nn;
+  A.piv = q; q += nn;
   A.dp = q; q += nn;
   A.phi = q; q += nn;
   CK (cudaMemcpy ((void *) A.St, St.data (), sizeof (double) * St.size (), cudaMemcpyHostToDevice));
+  {
+    // The elimination of the tridiagonal systems does not depend on the
+    // charge: its pivot reciprocals rp_i = 1 / (b_i - a_i cp_{i-1}) and
+    // cp_i = c_i rp_i of every (theta mode, z mode) are evaluated here, in
+    // the host solver's expressions and order, so the device sweep only
+    // carries dp.
+    std::vector<double> cpt (nn), pvt (nn);
+    for (int m = 0; m < nt; m++)
+      for (int k = 0; k < nz; k++) {
+        const size_t base = (size_t) m * nr * nz;
+        auto bcoef = [&] (int i) {
+          double b = -(ta[i] + tc[i]) + lam[k] + mk[(size_t) m * nr + i];
+          if (i == nr - 1) b -= tc[i];
+          return b;
+        };
+        double rp = 1.0 / bcoef (0);
+        double cpv = (nr - 1 == 0 ? 0.0 : tc[0]) * rp;
+        pvt[base + k] = rp;
+        cpt[base + k] = cpv;
+        for (int i = 1; i < nr; i++) {
+          const double pv = bcoef (i) - ta[i] * cpv;
+          rp = 1.0 / pv;
+          cpv = (i == nr - 1 ? 0.0 : tc[i]) * rp;
+          pvt[base + (size_t) i * nz + k] = rp;
+          cpt[base + (size_t) i * nz + k] = cpv;
+        }
+      }
+    CK (cudaMemcpy ((void *) A.cp, cpt.data (), sizeof (double) * nn, cudaMemcpyHostToDevice));
+    CK (cudaMemcpy ((void *) A.piv, pvt.data (), sizeof (double) * nn, cudaMemcpyHostToDevice));
+  }
   {
     std::vector<double> Sk (St.size ());        // the same matrix, k-major
     for (int k = 0; k < nz; k++)

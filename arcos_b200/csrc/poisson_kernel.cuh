@@ -53,7 +53,8 @@ struct PoisArgs {
   const double *elm;     // [m] = elmbda_m
   const double *tcos, *tsin;   // [q] = cos, sin (2 pi q / nt): the theta twiddles
   const double *wk;      // [m]: the theta derivative factors (init_wk_a)
-  double *qh, *ph, *cp, *dp, *phi;   // [m][i][k] (phi: [m][i][j]) scratch, nt * nr * nz each
+  double *cp, *piv;      // [m][i][k]: the elimination's cp_i and pivot reciprocals (host-evaluated)
+  double *qh, *ph, *dp, *phi;   // [m][i][k] (phi: [m][i][j]) scratch, nt * nr * nz each
 };
 
 // The sums below run in the host solver's order (index ascending, one
@@ -91,9 +92,11 @@ k_pois_fwd (const PatchDesc *__restrict__ pd, int patch, int set, PoisArgs A)
   }
 }
 
-// One (theta mode, z mode) per thread: the tridiagonal system in r (Thomas),
-// the coefficients and right-hand sides of PF rows loaded ahead of the
-// recurrence, cp and dp of PF rows ahead of the back substitution.
+// One (theta mode, z mode) per thread: the tridiagonal system in r (Thomas)
+// with the host-evaluated pivot reciprocals rp_i and cp_i,
+// dp_i = (q_i - a_i dp_{i-1}) rp_i, and
+// the back substitution p_i = dp_i - cp_i p_{i+1}; the operands of PF rows
+// are loaded ahead of each recurrence.
 __global__ void
 k_pois_tri (PoisArgs A)
 {
@@ -101,54 +104,42 @@ k_pois_tri (PoisArgs A)
   if (t >= A.nz * A.nt) return;
   const int nr = A.nr, nz = A.nz;
   const int m = t / nz, k = t - m * nz;
-  const size_t base = (size_t) m * nr * nz;
-  const double lam = A.lam[k];
-  const double *mk = A.mk + (size_t) m * nr;
-  auto bcoef = [&] (int i, double ta, double tc, double mki) {
-    double b = -(ta + tc) + lam + mki;
-    if (i == nr - 1) b -= tc;            // phi_{nr} = -phi_{nr-1} (Dirichlet at r = L_r)
-    return b;
-  };
-  const double b0 = bcoef (0, A.ta[0], A.tc[0], mk[0]);
-  double cpv = (nr - 1 == 0 ? 0.0 : A.tc[0]) / b0;
-  double dpv = A.qh[base + k] / b0;
-  A.cp[base + k] = cpv;
-  A.dp[base + k] = dpv;
+  const size_t base = (size_t) m * nr * nz + k;
+  double dpv = A.qh[base] * A.piv[base];
+  A.dp[base] = dpv;
   for (int i0 = 1; i0 < nr; i0 += POIS_PF) {
-    double ta[POIS_PF], tc[POIS_PF], mm[POIS_PF], qq[POIS_PF];
+    double ta[POIS_PF], pv[POIS_PF], qq[POIS_PF];
 #pragma unroll
     for (int q = 0; q < POIS_PF; q++) {
       const int i = i0 + q < nr ? i0 + q : nr - 1;
-      ta[q] = A.ta[i]; tc[q] = A.tc[i]; mm[q] = mk[i];
-      qq[q] = A.qh[base + (size_t) i * nz + k];
+      ta[q] = A.ta[i];
+      pv[q] = A.piv[base + (size_t) i * nz];
+      qq[q] = A.qh[base + (size_t) i * nz];
     }
 #pragma unroll
     for (int q = 0; q < POIS_PF; q++) {
       const int i = i0 + q;
       if (i >= nr) break;
-      const double mq = bcoef (i, ta[q], tc[q], mm[q]) - ta[q] * cpv;
-      cpv = (i == nr - 1 ? 0.0 : tc[q]) / mq;
-      dpv = (qq[q] - ta[q] * dpv) / mq;
-      A.cp[base + (size_t) i * nz + k] = cpv;
-      A.dp[base + (size_t) i * nz + k] = dpv;
+      dpv = (qq[q] - ta[q] * dpv) * pv[q];
+      A.dp[base + (size_t) i * nz] = dpv;
     }
   }
   double p = dpv;
-  A.ph[base + (size_t) (nr - 1) * nz + k] = p;
+  A.ph[base + (size_t) (nr - 1) * nz] = p;
   for (int i0 = nr - 2; i0 >= 0; i0 -= POIS_PF) {
     double cc[POIS_PF], dd[POIS_PF];
 #pragma unroll
     for (int q = 0; q < POIS_PF; q++) {
       const int i = i0 - q >= 0 ? i0 - q : 0;
-      cc[q] = A.cp[base + (size_t) i * nz + k];
-      dd[q] = A.dp[base + (size_t) i * nz + k];
+      cc[q] = A.cp[base + (size_t) i * nz];
+      dd[q] = A.dp[base + (size_t) i * nz];
     }
 #pragma unroll
     for (int q = 0; q < POIS_PF; q++) {
       const int i = i0 - q;
       if (i < 0) break;
       p = dd[q] - cc[q] * p;
-      A.ph[base + (size_t) i * nz + k] = p;
+      A.ph[base + (size_t) i * nz] = p;
     }
   }
 }

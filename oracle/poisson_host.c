@@ -14,7 +14,8 @@
  * with a regular axis (r_{-1/2} = 0), and homogeneous Dirichlet conditions on
  * the faces r = L_r, z = 0, z = L_z (pois_bnd_* = -1, the arcos default,
  * src/cstream.c:136-138).  Solved by a sine transform in z (eigenvectors of the
- * antisymmetric-ghost second difference) and a tridiagonal solve in r per mode.
+ * antisymmetric-ghost second difference) and a tridiagonal solve in r per mode
+ * (Thomas elimination, multiplying by each pivot's reciprocal).
  * The field is E = -grad phi on the staggered faces of src/grid.h:40-44:
  * er(i) on the face between cells i and i+1 (i = -1..nr-1), ez(j) likewise.
  *
@@ -81,12 +82,17 @@ oracle_poisson_mode (int nr, int nz, double dr, double dz, double elmbda, double
     }
     b[nr - 1] -= c[nr - 1];
     c[nr - 1] = 0.0;
-    cp[0] = c[0] / b[0];
-    dp[0] = qh[0 * nz + k] / b[0];
-    for (i = 1; i < nr; i++) {
-      double m = b[i] - a[i] * cp[i - 1];
-      cp[i] = c[i] / m;
-      dp[i] = (qh[i * nz + k] - a[i] * dp[i - 1]) / m;
+    /* the elimination multiplies by the pivot's reciprocal */
+    {
+      double rp = 1.0 / b[0];
+      cp[0] = c[0] * rp;
+      dp[0] = qh[0 * nz + k] * rp;
+      for (i = 1; i < nr; i++) {
+        double m = b[i] - a[i] * cp[i - 1];
+        rp = 1.0 / m;
+        cp[i] = c[i] * rp;
+        dp[i] = (qh[i * nz + k] - a[i] * dp[i - 1]) * rp;
+      }
     }
     ph[(nr - 1) * nz + k] = dp[nr - 1];
     for (i = nr - 2; i >= 0; i--)
