@@ -16,11 +16,13 @@
 // norms, the mode eigenvalues and the tridiagonal coefficients come from the
 // host, so the field is bit-identical to the host solver's.
 //
-// Four launches per solve, each thread one output value: forward transform
-// (i, k), tridiagonal solve per mode k, inverse transform (i, j), field on
-// every element of er and ez (ghosts included: zero off the faces).  The
-// work is O(nr nz^2) fused multiply-adds; at the field-in-the-loop
-// configuration (128 x 256) a few microseconds.
+// Four launches per solve: forward transform (a block per row i, a thread
+// per output k), tridiagonal solve per mode k (a thread each), inverse
+// transform (a block per row i, a thread per output j), field on every
+// element of er and ez (ghosts included: zero off the faces).  The
+// transforms are O(nr nz^2) multiply-adds; the tridiagonal sweep's
+// elimination (pivot reciprocals and cp) comes from the host, the device
+// carries dp and the back substitution.
 //
 // On a 3-D grid (cdr_calc_field_r, src/cdr.c:532-580) the charge first goes
 // to theta modes in place (dft_transform r2hc, src/dft.c:37-88), every mode
