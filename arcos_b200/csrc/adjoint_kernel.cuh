@@ -154,6 +154,24 @@ k_adj_keep (const PatchDesc *__restrict__ pd, int i0, int is)
   }
 }
 
+// Every species' density of storage set `set` of patch blockIdx.y to (to_adj)
+// or from its adjoint arrays idx + s (whole arrays): a checkpoint, or its
+// restore, as one launch instead of one copy per patch and species.
+static __global__ void __launch_bounds__ (256)
+k_adj_copy (const PatchDesc *__restrict__ pd, int to_adj, int set, int idx)
+{
+  const PatchDesc &P = pd[blockIdx.y];
+  const long long n2 = P.asz / 2;           // asz is a multiple of 32
+  const long long stride = (long long) gridDim.x * blockDim.x;
+  for (int s = 0; s < P.ns; s++) {
+    double2 *a = reinterpret_cast<double2 *> (P.arr (set, K_DENS, s));
+    double2 *b = reinterpret_cast<double2 *> (P.adj + (long long) (idx + s) * P.asz);
+    const double2 *src = to_adj ? a : b;
+    double2 *dst = to_adj ? b : a;
+    for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride) dst[i] = src[i];
+  }
+}
+
 // Per cell and reaction, the table lookup of react_apply (reaction.c:127-142)
 // for the fixed field of the sweep, stored for every transposed stage in
 // adjoint arrays rates_idx + 3 r + {0, 1, 2}: the rate k(|E|); the

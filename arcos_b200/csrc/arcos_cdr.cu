@@ -1098,11 +1098,12 @@ inline int adj_arrays (Ctx *c) { return adj_rates (c) + 3 * c->M.nreact; }
 int
 adj_copy (Ctx *c, bool to_adj, int set, int idx)
 {
-  for (auto &P : c->pd_h)
-    for (int s = 0; s < P.ns; s++) {
-      double *a = P.arr (set, K_DENS, s), *b = P.adj + (size_t) (idx + s) * P.asz;
-      CK (cudaMemcpyAsync (to_adj ? b : a, to_adj ? a : b, sizeof (double) * P.asz, cudaMemcpyDeviceToDevice, c->stream));
-    }
+  long long amax = 0;
+  for (auto &P : c->pd_h) amax = std::max (amax, P.asz);
+  const int bx = (int) std::min<long long> ((amax / 2 + 255) / 256, 2LL * c->num_sms);
+  k_adj_copy<<<dim3 (bx, (unsigned) c->pd_h.size ()), 256, 0, c->stream>>> (c->pd_d, to_adj ? 1 : 0, set, idx);
+  cudaError_t e = cudaGetLastError ();
+  if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("copy launch: ") + cudaGetErrorString (e));
   return ARCOS_OK;
 }
 
