@@ -75,6 +75,7 @@ def lib():
     L.arcos_set_field_fn.argtypes = [VP, FIELD_FN, VP]
     L.arcos_set_field_poisson.argtypes = [VP, C.c_int]
     L.arcos_set_photo.argtypes = [VP, C.c_int, DP, DP, C.c_int, C.c_int, C.c_int]
+    L.arcos_set_vjp_form.argtypes = [VP, C.c_int]
     L.arcos_dump.argtypes = [VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int]
     L.arcos_solve_field.argtypes = [VP, C.c_int]
     for name in ("arcos_cdr_nonegative_r", "arcos_cdr_set_ext_bnd_r", "arcos_cdr_set_periodic_r",

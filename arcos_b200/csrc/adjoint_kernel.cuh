@@ -176,8 +176,9 @@ k_adj_copy (const PatchDesc *__restrict__ pd, int to_adj, int set, int idx)
 // for the fixed field of the sweep, stored for every transposed stage in
 // adjoint arrays rates_idx + 3 r + {0, 1, 2}: the rate k(|E|); the
 // interpolation weight tt = (|E| - e1) / (e2 - e1); and the table-gradient
-// entry: i_lo (|E| inside the table), i_lo + 0.5 (inside, on the last node,
-// where v2 = v1), or -(under/over entry) - 1 (outside).  |E| as the VJP's
+// entry as a 32-bit integer in the first half of the third array: 2 i_lo
+// (|E| inside the table), 2 i_lo + 1 (inside, on the last node, where
+// v2 = v1), or -(under/over entry) - 1 (outside).  |E| as the VJP's
 // reactions take it (cdr.c:681-692).
 static __global__ void
 k_adj_rates (const __grid_constant__ Model M, const PatchDesc *__restrict__ pd, const TableNode *__restrict__ nodes,
@@ -203,17 +204,18 @@ k_adj_rates (const __grid_constant__ Model M, const PatchDesc *__restrict__ pd, 
         double k = n.val + n.slope * (e - n.e1);                       // table_rate
         k = over ? M.r_over[r] : k;
         k = (e >= nd[0].thr) ? k : M.r_under[r];
-        double tt = 0.0, cd;
+        double tt = 0.0;
+        int cd;
         if (inr) {
           tt = (e - n.e1) * inv_de[off + kk];
-          cd = (double) (off + kk) + (kk == steps ? 0.5 : 0.0);
+          cd = 2 * (off + kk) + (kk == steps ? 1 : 0);
         } else {
-          cd = -(double) (n_nodes + 2 * r + (over ? 1 : 0)) - 1.0;
+          cd = -(n_nodes + 2 * r + (over ? 1 : 0)) - 1;
         }
         double *rp = adj + (long long) (rates_idx + 3 * r) * asz + o;
         rp[0] = k;
         rp[asz] = tt;
-        rp[2 * asz] = cd;
+        reinterpret_cast<int *> (adj + (long long) (rates_idx + 3 * r + 2) * asz)[o] = cd;
       }
     }
 }
@@ -504,6 +506,7 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
       double wc[CPT][NS];
       bool on[CPT], own[CPT];
       const double *rp0[CPT];
+      const int *ip0[CPT];                 // the entry codes: reaction r at + 6 r asz
 #pragma unroll
       for (int q = 0; q < CPT; q++) {
         const int jj = CPT * wq + q, j = j0 + jj, c = c0 + lane;
@@ -512,14 +515,16 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         for (int s = 0; s < NS; s++) wc[q][s] = own[q] ? sW[(s * WR + jj + 2) * WC + lane + 2] : 0.0;
         on[q] = own[q] && ((double) (Pp->z0 + j) + 0.5) * Pp->dz < M.z_cutoff;
         rp0[q] = adj + (long long) A.rates_idx * asz + AO (c0 + lane, j0 + CPT * wq + q);
+        ip0[q] = reinterpret_cast<const int *> (adj + (long long) (A.rates_idx + 2) * asz) + AO (c0 + lane, j0 + CPT * wq + q);
       }
       // the lookups of k_adj_rates for this cell, one reaction ahead
-      double nk[CPT], ntt[CPT], ncd[CPT];
+      double nk[CPT], ntt[CPT];
+      int ncd[CPT];
 #pragma unroll
       for (int q = 0; q < CPT; q++) {
         nk[q] = own[q] ? __ldg (rp0[q]) : 0.0;
         ntt[q] = own[q] ? __ldg (rp0[q] + asz) : 0.0;
-        ncd[q] = own[q] ? __ldg (rp0[q] + 2 * asz) : 0.0;
+        ncd[q] = own[q] ? __ldg (ip0[q]) : 0;
       }
       __syncthreads ();
 #pragma unroll 1
@@ -527,7 +532,8 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         const int nin = M.r_nin[r];
         int i_lo[CPT], i_hi[CPT];
         double g_lo[CPT], g_hi[CPT];
-        double ck[CPT], ctt[CPT], ccd[CPT];
+        double ck[CPT], ctt[CPT];
+        int ccd[CPT];
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
           ck[q] = nk[q]; ctt[q] = ntt[q]; ccd[q] = ncd[q];
@@ -535,7 +541,7 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
             const double *rp = rp0[q] + (long long) (3 * (r + 1)) * asz;
             nk[q] = __ldg (rp);
             ntt[q] = __ldg (rp + asz);
-            ncd[q] = __ldg (rp + 2 * asz);
+            ncd[q] = __ldg (ip0[q] + (long long) (6 * (r + 1)) * asz);
           }
         }
 #pragma unroll
@@ -545,7 +551,8 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
 #pragma unroll
           for (int s = 0; s < NS; s++) rho = __fma_rn (sCf[r * NS + s], wc[q][s], rho);
           if (on[q] && rho != 0.0) {
-            const double k = ck[q], tt = ctt[q], cd = ccd[q];
+            const double k = ck[q], tt = ctt[q];
+            const int cd = ccd[q];
             // inputs |n_in| from the staged state (clamped in mode 2)
             const double *stq = sST + (CPT * wq + q + 3) * SC + lane + 3;
             // d/dn_s of k prod |n_in|: per input, k sign(n) prod of the others
@@ -595,15 +602,15 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
             }
             // table entries: rate = v1 + (v2 - v1) (E - e1) / (e2 - e1) (reaction.c:142)
             const double gr = rho * prod;
-            if (cd >= 0.0) {                            // |E| inside the table
-              const int il = (int) cd;
+            if (cd >= 0) {                              // |E| inside the table
+              const int il = cd >> 1;
               i_lo[q] = il;
               g_lo[q] = gr * (1.0 - tt);
               g_hi[q] = gr * tt;
-              if (cd != (double) il) { g_lo[q] += g_hi[q]; g_hi[q] = 0.0; }   // last node: v2 = v1
+              if (cd & 1) { g_lo[q] += g_hi[q]; g_hi[q] = 0.0; }   // last node: v2 = v1
               else i_hi[q] = il + 1;
             } else {
-              i_lo[q] = (int) (-cd) - 1;
+              i_lo[q] = -cd - 1;
               g_lo[q] = gr;
             }
           }
@@ -656,6 +663,392 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
   if (A.tab_smem)
     for (int i = t; i < ntab; i += NT)
       if (sTab[i] != 0.0) atomicAdd (A.g_table + i, sTab[i]);
+}
+
+// ---- the split form for many species: faces and reactions in two kernels ----
+//
+// With six species the one-kernel form holds every species' state and
+// cotangent in shared memory (72 KB a block, three blocks per SM) and the
+// reactions' registers beside the faces'.  The split form stages one species
+// at a time for its faces (k_vjp_faces: 33 KB a block, no per-species
+// registers: each species' gathered faces go straight to the output array,
+// the mobility sums to shared memory) and applies the reactions and the
+// mode-2 terms in a second, streaming kernel (k_vjp_react, one thread per
+// cell).  Every value is computed with the one-kernel form's operations in
+// its order, so both forms give the same bits.
+struct VjpTileF {
+  static constexpr int VX = 32, VY = 8, NT = 256;
+  static constexpr int SC = VX + 6, SR = VY + 6, WC = VX + 4, WR = VY + 4;
+  static constexpr int EC = VX + 3, ZR = VY + 3, FR = VX + 3, FZ = VY + 3;
+  static constexpr int O_ST = 0;
+  static constexpr int O_W = O_ST + SR * SC;
+  static constexpr int O_ER = O_W + WR * WC;
+  static constexpr int O_EZ = O_ER + VY * EC;
+  static constexpr int O_PR = O_EZ + ZR * VX;
+  static constexpr int O_PZ = O_PR + 4 * VY * FR;
+  static constexpr int END = O_PZ + 4 * FZ * VX;
+};
+
+// out_s = (J_faces^T w)_s for every species of every tile (zero for
+// immobile species); the mobility and diffusion partial sums as k_vjp.
+template <int NS>
+__global__ void __launch_bounds__ (256, 4)
+k_vjp_faces (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
+{
+  using L = VjpTileF;
+  constexpr int VX = L::VX, VY = L::VY, NT = L::NT, NW = NT / 32;
+  constexpr int SC = L::SC, SR = L::SR, WC = L::WC, WR = L::WR, EC = L::EC, ZR = L::ZR;
+  constexpr int FR = L::FR, FZ = L::FZ;
+  constexpr int NRI = VY * FR, NRP = (NRI + 31) / 32 * 32, NAI = FZ * VX;
+  constexpr int RP = (NRP + NAI + NT - 1) / NT;
+  extern __shared__ __align__ (16) double vsm[];
+  double *const sST = vsm + L::O_ST, *const sW = vsm + L::O_W;
+  double *const sER = vsm + L::O_ER, *const sEZ = vsm + L::O_EZ;
+  double *const sPR = vsm + L::O_PR, *const sPZ = vsm + L::O_PZ;
+  __shared__ double sGmu[NW][NS];
+  __shared__ double red[NW][NS + 1];
+  const int t = threadIdx.x, lane = t & 31, wq = t >> 5;
+  if (lane < NS) sGmu[wq][lane] = 0.0;
+  double gD = 0.0;
+  int rjj[RP], rfi[RP];
+  {
+    int jj = t / FR, fi = t - (t / FR) * FR;
+#pragma unroll
+    for (int m = 0; m < RP; m++) {
+      rjj[m] = jj; rfi[m] = fi;
+      fi += NT % FR; jj += NT / FR;
+      if (fi >= FR) { fi -= FR; jj++; }
+    }
+  }
+
+  for (int ti = blockIdx.x; ti < A.n_tiles; ti += gridDim.x) {
+    const AdjTile T = A.tiles[ti];
+    const PatchDesc *Pp = A.patches + T.patch;
+    const int nr = Pp->nr, nz = Pp->nz, pitch = Pp->pitch;
+    const long long asz = Pp->asz;
+    double *adj = Pp->adj;
+    const int c0 = T.c0, j0 = T.zb;
+    const double h = A.hs[Pp->fam * A.hs_stride + A.k];
+    const double a1 = 0.5 * h, b1 = (A.mode == 2) ? h : 0.0;
+    const bool clampst = A.mode == 2;
+    const double *er = Pp->arr (0, K_ER), *ez = Pp->arr (0, K_EZ);
+    const double sg_r = (double) M.bnd_sign[1], sg_b = (double) M.bnd_sign[2], sg_t = (double) M.bnd_sign[3];
+    auto AO = [&] (int col, int row) -> long long { return (long long) (col + 2) + (long long) (row + 2) * pitch; };
+    const int c = c0 + lane, j = j0 + wq;
+    const bool own = c < nr && j < nz;
+
+    __syncthreads ();                           // the previous tile is done with the shared arrays
+    tile_for<EC, VY, NT> (t, [&] (int yy, int xx) {
+      const int col = c0 - 2 + xx, row = j0 + yy;
+      sER[yy * EC + xx] = (col >= -2 && col <= nr + 1 && row <= nz + 1) ? __ldg (er + AO (col, row)) : 0.0;
+    });
+#pragma unroll
+    for (int y8 = 0; y8 < (ZR + NW - 1) / NW; y8++) {
+      const int yy = wq + NW * y8;
+      if (yy >= ZR) break;
+      const int row = j0 - 2 + yy, col = c0 + lane;
+      sEZ[yy * VX + lane] = (col <= nr + 1 && row >= -2 && row <= nz + 1) ? __ldg (ez + AO (col, row)) : 0.0;
+    }
+
+    static_for<0, NS> ([&] (auto S_) {
+      constexpr int s = decltype (S_)::value;
+      double *outp = adj + (long long) (A.out_idx + s) * asz;
+      if (!M.mobile[s]) {                       // block-uniform
+        if (own) outp[AO (c, j)] = 0.0;
+        return;
+      }
+      __syncthreads ();                         // the previous species is done with the buffers
+      const double *src = adj + (long long) (A.st_idx + s) * asz;
+      tile_for<SC, SR, NT> (t, [&] (int yy, int xx) {
+        int col = c0 - 3 + xx, row = j0 - 3 + yy;
+        double sg = 1.0;
+        if (col < 0) { col = -1 - col; }
+        else if (col >= nr) { col = 2 * nr - 1 - col; sg = sg_r; }
+        if (row < 0) { row = -1 - row; sg = sg_b; }
+        else if (row >= nz) { row = 2 * nz - 1 - row; sg = sg_t; }
+        double v = 0.0;
+        if (col >= 0 && col < nr && row >= 0 && row < nz) {
+          v = __ldg (src + AO (col, row));
+          if (clampst) v = clamp0 (v);
+          v = sg * v;
+        }
+        sST[yy * SC + xx] = v;
+      });
+      const double *lp = adj + (long long) (A.lam_idx + s) * asz;
+      const double *lsp = adj + (long long) (A.lams_idx + s) * asz;
+      tile_for<WC, WR, NT> (t, [&] (int yy, int xx) {
+        const int col = c0 - 2 + xx, row = j0 - 2 + yy;
+        double w = 0.0;
+        if (col >= 0 && col < nr && row >= 0 && row < nz) {
+          const long long o = AO (col, row);
+          w = a1 * __ldg (lp + o);
+          if (A.mode == 2) w = __fma_rn (b1, __ldg (lsp + o), w);
+        }
+        sW[yy * WC + xx] = w;
+      });
+      __syncthreads ();
+      double gmu = 0.0;
+      auto radial_item = [&] (int jj, int fi) {
+        const int ar = c0 - 1 + fi, jr = j0 + jj;
+        double pLL = 0.0, pL = 0.0, pR = 0.0, pRR = 0.0;
+        if (ar >= 0 && ar <= nr && jr < nz) {
+          const double fm = ar < nr ? A.colfac[2 * ar] : 0.0;
+          const double fp = ar >= 1 ? A.colfac[2 * (ar - 1) + 1] : 0.0;
+          const double *w = sW + (jj + 2) * WC + fi;
+          const double g = fm * w[1] - fp * w[0];
+          if (g != 0.0) {
+            const double *st = sST + (jj + 3) * SC + fi;
+            const double e = sER[jj * EC + fi];
+            const FaceGrad fg = face_grad (true, st[0], st[1], st[2], st[3], A.cm[s] * e, A.ddr[s]);
+            pLL = g * fg.pLL; pL = g * fg.pL; pR = g * fg.pR; pRR = g * fg.pRR;
+            if ((ar >= c0 && ar < c0 + VX && ar < nr) || (ar == nr && nr - 1 >= c0 && nr - 1 < c0 + VX)) {
+              gmu += g * (fg.dv * M.charge[s] * e + fg.ddd * A.Ddr);
+              gD += g * fg.ddd * A.mudr[s];
+            }
+          }
+        }
+        double *pr = sPR + jj * FR + fi;
+        pr[0] = pLL; pr[VY * FR] = pL; pr[2 * VY * FR] = pR; pr[3 * VY * FR] = pRR;
+      };
+      auto axial_item = [&] (int fa) {
+        const int a = j0 - 1 + fa, ca = c0 + lane;
+        double pLL = 0.0, pL = 0.0, pR = 0.0, pRR = 0.0;
+        if (a >= 0 && a <= nz && ca < nr) {
+          const double *w = sW + fa * WC + lane + 2;
+          const double g = A.gdz * (w[WC] - w[0]);
+          if (g != 0.0) {
+            const double *st = sST + fa * SC + lane + 3;
+            const double e = sEZ[fa * VX + lane];
+            const FaceGrad fg = face_grad (false, st[0], st[SC], st[2 * SC], st[3 * SC], A.cm[s] * e, A.ddz[s]);
+            pLL = g * fg.pLL; pL = g * fg.pL; pR = g * fg.pR; pRR = g * fg.pRR;
+            if ((a >= j0 && a < j0 + VY && a < nz) || (a == nz && nz - 1 >= j0 && nz - 1 < j0 + VY)) {
+              gmu += g * (fg.dv * M.charge[s] * e + fg.ddd * A.Ddz);
+              gD += g * fg.ddd * A.mudz[s];
+            }
+          }
+        }
+        double *pz = sPZ + fa * VX + lane;
+        pz[0] = pLL; pz[FZ * VX] = pL; pz[2 * FZ * VX] = pR; pz[3 * FZ * VX] = pRR;
+      };
+#pragma unroll
+      for (int m = 0; m < RP; m++) {
+        const int i = t + NT * m;
+        if (i < NRP) {
+          if (i < NRI) radial_item (rjj[m], rfi[m]);
+        } else if (i < NRP + NAI) {
+          axial_item ((i - NRP) >> 5);
+        }
+      }
+      // this species' mobility sum: per warp into shared memory
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) gmu += __shfl_xor_sync (0xffffffffu, gmu, o);
+      if (lane == 0) sGmu[wq][s] += gmu;
+      __syncthreads ();
+      auto RAD = [&] (int jj, int x) -> double {
+        const int f = x - c0 + 1;
+        const double *pr = sPR + jj * FR;
+        double v = 0.0;
+        if (f - 1 >= 0 && f - 1 < FR) v += pr[3 * VY * FR + f - 1];
+        if (f >= 0 && f < FR) v += pr[2 * VY * FR + f];
+        if (f + 1 >= 0 && f + 1 < FR) v += pr[VY * FR + f + 1];
+        if (f + 2 >= 0 && f + 2 < FR) v += pr[f + 2];
+        return v;
+      };
+      auto AXI = [&] (int y) -> double {
+        const int f = y - j0 + 1;
+        const double *pz = sPZ + lane;
+        double v = 0.0;
+        if (f - 1 >= 0 && f - 1 < FZ) v += pz[(3 * FZ + f - 1) * VX];
+        if (f >= 0 && f < FZ) v += pz[(2 * FZ + f) * VX];
+        if (f + 1 >= 0 && f + 1 < FZ) v += pz[(FZ + f + 1) * VX];
+        if (f + 2 >= 0 && f + 2 < FZ) v += pz[(f + 2) * VX];
+        return v;
+      };
+      if (own) {
+        double z = AXI (j);
+        if (j == 0) z = __fma_rn (sg_b, AXI (-1), z);
+        if (j == 1) z = __fma_rn (sg_b, AXI (-2), z);
+        if (j == nz - 1) z = __fma_rn (sg_t, AXI (nz), z);
+        if (j == nz - 2) z = __fma_rn (sg_t, AXI (nz + 1), z);
+        double rr = RAD (wq, c);
+        if (c == 0) rr += RAD (wq, -1);
+        if (c == 1) rr += RAD (wq, -2);
+        if (c == nr - 1) rr = __fma_rn (sg_r, RAD (wq, nr), rr);
+        if (c == nr - 2) rr = __fma_rn (sg_r, RAD (wq, nr + 1), rr);
+        outp[AO (c, j)] = z + rr;
+      }
+    });
+  }
+
+  // ---- block partial sums of the mobility and diffusion gradients ----
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) gD += __shfl_xor_sync (0xffffffffu, gD, o);
+  __syncthreads ();
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s < NS; s++) red[wq][s] = sGmu[wq][s];
+    red[wq][NS] = gD;
+  }
+  __syncthreads ();
+  if (t <= NS) {
+    double v = 0.0;
+    for (int w = 0; w < NW; w++) v += red[w][t];
+    A.g_part[(size_t) blockIdx.x * (NS + 1) + t] += v;
+  }
+}
+
+// The reactions of every cell (react_apply, folded form) added to the faces
+// that k_vjp_faces left in the output array, then the mode-2 terms: the
+// reaction and output code of k_vjp with the cell's state and cotangent
+// read from global memory.  One thread per cell of a 32 x 8 tile.
+// GENERIC: some reaction has more than two inputs (the product rule over up
+// to four); without it the kernel keeps to the one- and two-input forms.
+template <int NS, bool GENERIC>
+__global__ void __launch_bounds__ (256, 4)
+k_vjp_react (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
+{
+  extern __shared__ __align__ (16) double sTab[];
+  const int t = threadIdx.x, lane = t & 31, wq = t >> 5;
+  const int ntab = A.n_nodes + 2 * M.nreact;
+  double *const gtab = A.tab_smem ? sTab : A.g_table;
+  if (A.tab_smem) {
+    for (int i = t; i < ntab; i += blockDim.x) sTab[i] = 0.0;
+    __syncthreads ();
+  }
+  __shared__ double sCf[ARCOS_MAXR * NS];
+  for (int i = t; i < M.nreact * NS; i += blockDim.x) sCf[i] = (double) M.r_coef[i / NS][i - (i / NS) * NS];
+  __syncthreads ();
+  for (int ti = blockIdx.x; ti < A.n_tiles; ti += gridDim.x) {
+    const AdjTile T = A.tiles[ti];
+    const PatchDesc *Pp = A.patches + T.patch;
+    const int nr = Pp->nr, nz = Pp->nz, pitch = Pp->pitch;
+    const long long asz = Pp->asz;
+    double *adj = Pp->adj;
+    const int c = T.c0 + lane, j = T.zb + wq;
+    const bool own = c < nr && j < nz;
+    const double h = A.hs[Pp->fam * A.hs_stride + A.k];
+    const double a1 = 0.5 * h, b1 = (A.mode == 2) ? h : 0.0;
+    const long long o = (long long) (c + 2) + (long long) (j + 2) * pitch;
+    double out[NS], nv[NS], wc[NS], lm[NS], ls[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      out[s] = own ? adj[(long long) (A.out_idx + s) * asz + o] : 0.0;
+      double v = own ? __ldg (adj + (long long) (A.st_idx + s) * asz + o) : 0.0;
+      if (A.mode == 2) v = clamp0 (v);
+      nv[s] = v;
+      lm[s] = own ? __ldg (adj + (long long) (A.lam_idx + s) * asz + o) : 0.0;
+      ls[s] = (own && A.mode == 2) ? __ldg (adj + (long long) (A.lams_idx + s) * asz + o) : 0.0;
+      double w = 0.0;
+      if (own) {
+        w = a1 * lm[s];
+        if (A.mode == 2) w = __fma_rn (b1, ls[s], w);
+      }
+      wc[s] = w;
+    }
+    if (M.nreact > 0) {
+      const bool on = own && ((double) (Pp->z0 + j) + 0.5) * Pp->dz < M.z_cutoff;
+      const double *rp0 = adj + (long long) A.rates_idx * asz + o;
+      const int *ip0 = reinterpret_cast<const int *> (adj + (long long) (A.rates_idx + 2) * asz) + o;
+      double nk = own ? __ldg (rp0) : 0.0, ntt = own ? __ldg (rp0 + asz) : 0.0;
+      int ncd = own ? __ldg (ip0) : 0;
+#pragma unroll 1
+      for (int r = 0; r < M.nreact; r++) {
+        const int nin = M.r_nin[r];
+        const double k = nk, tt = ntt;
+        const int cd = ncd;
+        if (r + 1 < M.nreact && own) {
+          const double *rp = rp0 + (long long) (3 * (r + 1)) * asz;
+          nk = __ldg (rp); ntt = __ldg (rp + asz); ncd = __ldg (ip0 + (long long) (6 * (r + 1)) * asz);
+        }
+        int i_lo = -1, i_hi = -1;
+        double g_lo = 0.0, g_hi = 0.0;
+        double rho = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; s++) rho = __fma_rn (sCf[r * NS + s], wc[s], rho);
+        if (on && rho != 0.0) {
+          const double rk = rho * k;
+          auto sgn = [] (double v) -> double { return v > 0.0 ? 1.0 : (v < 0.0 ? -1.0 : 0.0); };
+          auto pick = [&] (int sp) -> double {
+            double v = 0.0;
+#pragma unroll
+            for (int s = 0; s < NS; s++) if (s == sp) v = nv[s];
+            return v;
+          };
+          double prod;
+          if (!GENERIC || nin == 1 || nin == 2) {
+            const int s0 = M.r_in[r][0], s1 = nin == 2 ? M.r_in[r][1] : s0;
+            const double v0 = pick (s0);
+            const double v1 = nin == 2 ? pick (s1) : 1.0;
+            const double a0 = fabs (v0), av1 = fabs (v1);
+            prod = a0 * av1;
+            const double d0 = rk * sgn (v0) * av1;
+#pragma unroll
+            for (int s = 0; s < NS; s++)
+              if (s == s0) out[s] += d0;
+            if (nin == 2) {
+              const double d1 = rk * sgn (v1) * a0;
+#pragma unroll
+              for (int s = 0; s < NS; s++)
+                if (s == s1) out[s] += d1;
+            }
+          } else if constexpr (GENERIC) {
+            double av[ARCOS_MAXIN], sv[ARCOS_MAXIN];
+            int sp[ARCOS_MAXIN];
+            prod = 1.0;
+#pragma unroll
+            for (int i = 0; i < ARCOS_MAXIN; i++) {
+              const int si = i < nin ? M.r_in[r][i] : 0;
+              sp[i] = i < nin ? si : -1;
+              const double v = i < nin ? pick (si) : 1.0;
+              sv[i] = v;
+              av[i] = fabs (v);
+              prod *= av[i];
+            }
+#pragma unroll
+            for (int i = 0; i < ARCOS_MAXIN; i++) {
+              double others = 1.0;
+#pragma unroll
+              for (int q = 0; q < ARCOS_MAXIN; q++)
+                if (q != i) others *= av[q];
+              const double d = rk * sgn (sv[i]) * others;
+#pragma unroll
+              for (int s = 0; s < NS; s++)
+                if (s == sp[i]) out[s] += d;
+            }
+          }
+          const double gr = rho * prod;
+          if (cd >= 0) {
+            const int il = cd >> 1;
+            i_lo = il;
+            g_lo = gr * (1.0 - tt);
+            g_hi = gr * tt;
+            if (cd & 1) { g_lo += g_hi; g_hi = 0.0; }
+            else i_hi = il + 1;
+          } else {
+            i_lo = -cd - 1;
+            g_lo = gr;
+          }
+        }
+        warp_add2 (gtab, i_lo, g_lo, i_hi, g_hi);
+      }
+    }
+    if (own) {
+#pragma unroll
+      for (int s = 0; s < NS; s++) {
+        double v = out[s];
+        if (A.mode == 2) {
+          v += lm[s] + ls[s];
+          if (!(nv[s] > 0.0)) v = 0.0;      // d max(0, n0)
+        }
+        adj[(long long) (A.out_idx + s) * asz + o] = v;
+      }
+    }
+  }
+  if (A.tab_smem) {
+    __syncthreads ();
+    for (int i = t; i < ntab; i += blockDim.x)
+      if (sTab[i] != 0.0) atomicAdd (A.g_table + i, sTab[i]);
+  }
 }
 
 }  // namespace arcos

@@ -164,6 +164,10 @@ struct Ctx {
   AdjTile *adj_tiles_d = nullptr;
   int adj_ntiles = 0, adj_blocks = 0;
   size_t adj_smem = 0;                // dynamic shared memory of a VJP block
+  int vjp_form = -1;                  // -1 automatic, 0 one kernel, 1 faces + reactions
+  bool adj_split = false;             // the VJP runs as k_vjp_faces + k_vjp_react
+  int adj_blocks_r = 0;               // blocks of k_vjp_react
+  size_t adj_smem_r = 0;
   int adj_tab_smem = 0;               // table gradients accumulate in shared memory
   int adj_lam = 0;                    // lam buffer holding the current cotangent
   bool adj_fwd = false;
@@ -1057,6 +1061,21 @@ vjp_launch_m (int ns, const Model &M, const VjpArgs &A, int blocks, size_t smem,
   }
 }
 
+cudaError_t
+vjp_split_launch_m (int ns, const Model &M, const VjpArgs &A, int blocks_f, int blocks_r, size_t smem_r,
+                    cudaStream_t st, int *occ)
+{
+  switch (ns) {
+  case 1: return launch_vjp_split_ns<1> (M, A, blocks_f, blocks_r, smem_r, st, occ);
+  case 2: return launch_vjp_split_ns<2> (M, A, blocks_f, blocks_r, smem_r, st, occ);
+  case 3: return launch_vjp_split_ns<3> (M, A, blocks_f, blocks_r, smem_r, st, occ);
+  case 4: return launch_vjp_split_ns<4> (M, A, blocks_f, blocks_r, smem_r, st, occ);
+  case 5: return launch_vjp_split_ns<5> (M, A, blocks_f, blocks_r, smem_r, st, occ);
+  case 6: return launch_vjp_split_ns<6> (M, A, blocks_f, blocks_r, smem_r, st, occ);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
 // Rows of a VJP tile.
 int
 vjp_tile_rows (int ns)
@@ -1155,12 +1174,25 @@ adj_alloc (Ctx *c, int nsteps, int ck)
     // memory; larger ones take warp-aggregated atomics in global memory, so
     // that the table does not cost the kernel its resident blocks
     const size_t base = sizeof (double) * vjp_base_doubles (ns), limit = 227 * 1024;
-    c->adj_tab_smem = (ng <= 4096 && base + sizeof (double) * ng <= limit) ? 1 : 0;
-    c->adj_smem = base + (c->adj_tab_smem ? sizeof (double) * ng : 0);
-    int occ = 0;
-    cudaError_t e = vjp_launch_m (ns, c->M, VjpArgs{}, 0, c->adj_smem, 0, &occ);
-    if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("vjp occupancy: ") + cudaGetErrorString (e));
-    c->adj_blocks = std::min (c->adj_ntiles, c->num_sms * std::max (occ, 1));
+    // four or more species: faces and reactions in two kernels (the one
+    // kernel holds every species in shared memory, three blocks per SM)
+    c->adj_split = c->vjp_form == 1 || (c->vjp_form < 0 && ns >= 4);
+    if (c->adj_split) {
+      c->adj_tab_smem = ng <= 4096 ? 1 : 0;
+      c->adj_smem_r = c->adj_tab_smem ? sizeof (double) * ng : 0;
+      int occ2[2] = {0, 0};
+      cudaError_t e = vjp_split_launch_m (ns, c->M, VjpArgs{}, 0, 0, c->adj_smem_r, 0, occ2);
+      if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("vjp occupancy: ") + cudaGetErrorString (e));
+      c->adj_blocks = std::min (c->adj_ntiles, c->num_sms * std::max (occ2[0], 1));
+      c->adj_blocks_r = std::min (c->adj_ntiles, c->num_sms * std::max (occ2[1], 1));
+    } else {
+      c->adj_tab_smem = (ng <= 4096 && base + sizeof (double) * ng <= limit) ? 1 : 0;
+      c->adj_smem = base + (c->adj_tab_smem ? sizeof (double) * ng : 0);
+      int occ = 0;
+      cudaError_t e = vjp_launch_m (ns, c->M, VjpArgs{}, 0, c->adj_smem, 0, &occ);
+      if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("vjp occupancy: ") + cudaGetErrorString (e));
+      c->adj_blocks = std::min (c->adj_ntiles, c->num_sms * std::max (occ, 1));
+    }
     CK (cudaMalloc (&c->adj_gpart_d, sizeof (double) * (size_t) c->adj_blocks * (ns + 1)));
     CK (cudaMalloc (&c->adj_gtab_d, sizeof (double) * std::max<size_t> (ng, 1)));
   }
@@ -1226,7 +1258,9 @@ run_vjp (Ctx *c, int mode, int st_idx, int lam_idx, int lams_idx, int out_idx, i
   A.tab_smem = c->adj_tab_smem;
   A.rates_idx = adj_rates (c);
   if (c->M.ns < 1 || c->M.ns > 6) return fail (ARCOS_ERR_ARG, "adjoint: 1..6 species");
-  cudaError_t e = vjp_launch_m (c->M.ns, c->M, A, c->adj_blocks, c->adj_smem, c->stream, nullptr);
+  cudaError_t e = c->adj_split
+                    ? vjp_split_launch_m (c->M.ns, c->M, A, c->adj_blocks, c->adj_blocks_r, c->adj_smem_r, c->stream, nullptr)
+                    : vjp_launch_m (c->M.ns, c->M, A, c->adj_blocks, c->adj_smem, c->stream, nullptr);
   if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("vjp launch: ") + cudaGetErrorString (e));
   return ARCOS_OK;
 }
@@ -2429,6 +2463,29 @@ arcos_set_field_poisson (void *ctx, int on)
   // a 3-D solve gives E_theta != 0: the stage kernels read |E| from memory
   if (nt > 1) c->stage_eabs = 1;
   c->pois = true;
+  return ARCOS_OK;
+}
+
+// The form of the adjoint's transposed-step kernel: -1 automatic (faces and
+// reactions in two kernels from four species on), 0 one kernel, 1 two.  Both
+// give the same values; a change drops the adjoint's buffers (run
+// arcos_adj_forward again).
+int
+arcos_set_vjp_form (void *ctx, int form)
+{
+  Ctx *c = (Ctx *) ctx;
+  int r = chk_committed (c);
+  if (r) return r;
+  if (form < -1 || form > 1) return fail (ARCOS_ERR_ARG, "arcos_set_vjp_form: -1, 0 or 1");
+  if (form == c->vjp_form) return ARCOS_OK;
+  c->vjp_form = form;
+  if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
+  cudaFree (c->adj_tiles_d); c->adj_tiles_d = nullptr;
+  cudaFree (c->adj_gpart_d); c->adj_gpart_d = nullptr;
+  cudaFree (c->adj_gtab_d); c->adj_gtab_d = nullptr;
+  cudaFree (c->adj_pool); c->adj_pool = nullptr;
+  c->adj_nsteps = c->adj_ck = 0;
+  c->adj_fwd = false;
   return ARCOS_OK;
 }
 

@@ -40,6 +40,9 @@ cudaError_t launch_march_ns (bool s2, bool tree, const Model &M, const FusedArgs
 template <int NS>
 cudaError_t launch_vjp_ns (const Model &M, const VjpArgs &A, int blocks, size_t smem, cudaStream_t st,
                            int *occ);
+template <int NS>
+cudaError_t launch_vjp_split_ns (const Model &M, const VjpArgs &A, int blocks_f, int blocks_r, size_t smem_r,
+                                 cudaStream_t st, int *occ);
 
 #define ARCOS_DECLARE_NS(N)                                                                          \
   extern template cudaError_t launch_stage_ns<N> (int, int, const Model &, const StageArgs &, int,   \
@@ -48,6 +51,8 @@ cudaError_t launch_vjp_ns (const Model &M, const VjpArgs &A, int blocks, size_t 
                                                   int, cudaStream_t, int *);                         \
   extern template cudaError_t launch_vjp_ns<N> (const Model &, const VjpArgs &, int, size_t,         \
                                                 cudaStream_t, int *);                                \
+  extern template cudaError_t launch_vjp_split_ns<N> (const Model &, const VjpArgs &, int, int,      \
+                                                      size_t, cudaStream_t, int *);                  \
   extern template cudaError_t launch_march_ns<N> (bool, bool, const Model &, const FusedArgs &, int, \
                                                   cudaStream_t);
 ARCOS_DECLARE_NS (1)

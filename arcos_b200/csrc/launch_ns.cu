@@ -110,6 +110,40 @@ launch_vjp_ns (const Model &M, const VjpArgs &A, int blocks, size_t smem, cudaSt
   return cudaGetLastError ();
 }
 
+// The split form of the VJP (faces, then reactions); with occ the two
+// kernels' resident blocks per SM (occ[0] faces, occ[1] reactions).
+template <int NS>
+cudaError_t
+launch_vjp_split_ns (const Model &M, const VjpArgs &A, int blocks_f, int blocks_r, size_t smem_r,
+                     cudaStream_t st, int *occ)
+{
+  const size_t smem_f = sizeof (double) * VjpTileF::END;
+  if (occ) {
+    cudaError_t e = cudaFuncSetAttribute (k_vjp_faces<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_f);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor (&occ[0], k_vjp_faces<NS>, VjpTileF::NT, smem_f);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute (k_vjp_react<NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_r);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute (k_vjp_react<NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_r);
+    if (e != cudaSuccess) return e;
+    int o1 = 0, o2 = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor (&o1, k_vjp_react<NS, false>, 256, smem_r);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor (&o2, k_vjp_react<NS, true>, 256, smem_r);
+    occ[1] = o1 < o2 ? o1 : o2;
+    return e;
+  }
+  bool generic = false;
+  for (int r = 0; r < M.nreact; r++) generic = generic || M.r_nin[r] > 2;
+  k_vjp_faces<NS><<<blocks_f, VjpTileF::NT, smem_f, st>>> (M, A);
+  cudaError_t e = cudaGetLastError ();
+  if (e != cudaSuccess) return e;
+  if (generic) k_vjp_react<NS, true><<<blocks_r, 256, smem_r, st>>> (M, A);
+  else k_vjp_react<NS, false><<<blocks_r, 256, smem_r, st>>> (M, A);
+  return cudaGetLastError ();
+}
+
 template <int NS, bool S2, bool TREE>
 cudaError_t
 launch_march_t (const Model &M, const FusedArgs &A, int blocks, cudaStream_t s)
@@ -132,5 +166,6 @@ template cudaError_t launch_march_ns<ARCOS_NS> (bool, bool, const Model &, const
 template cudaError_t launch_stage_ns<ARCOS_NS> (int, int, const Model &, const StageArgs &, int, cudaStream_t, int *);
 template cudaError_t launch_fused_ns<ARCOS_NS> (bool, bool, int, const Model &, const FusedArgs &, int, cudaStream_t, int *);
 template cudaError_t launch_vjp_ns<ARCOS_NS> (const Model &, const VjpArgs &, int, size_t, cudaStream_t, int *);
+template cudaError_t launch_vjp_split_ns<ARCOS_NS> (const Model &, const VjpArgs &, int, int, size_t, cudaStream_t, int *);
 
 }  // namespace arcos

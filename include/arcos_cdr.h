@@ -306,6 +306,12 @@ int arcos_adj_set_cotangent (void *ctx, int grid, int species, const double *hos
 int arcos_adj_get_cotangent (void *ctx, int grid, int species, double *host);
 int arcos_adj_backward (void *ctx, double *grad_mobility, double *grad_diffusion,
                         double *grad_tables);
+/* The form of the transposed-step kernel: -1 automatic (faces and reactions
+ * in two kernels from four species on), 0 one kernel, 1 two kernels.  Both
+ * forms give the same values (the table gradients to the order of their
+ * atomic sums); a change drops the adjoint's buffers, so arcos_adj_forward
+ * runs again. */
+int arcos_set_vjp_form (void *ctx, int form);
 int arcos_adj_table_entries (void *ctx);
 int arcos_adj_table_offset (void *ctx, int reaction);
 

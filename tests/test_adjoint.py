@@ -302,3 +302,40 @@ def test_kinetic_batch_adjoint_matches_fd(cuda_device, field, ck):
         fd = sum(float(np.sum(vols[g] * (outs[0][g] - outs[1][g]))) for g in range(len(pb.specs))) / (2 * eps)
         assert abs(fd - pred) <= TOL * abs(fd), (which, fd, pred)
     tree.close()
+
+
+def test_vjp_forms_give_the_same_gradients(cuda_device):
+    """The transposed step as one kernel and as faces + reactions (the
+    automatic choice from four species on): the density gradients bit for
+    bit (every value computed with the same operations in the same order),
+    the mobility, diffusion and table sums to the order of their partial
+    sums."""
+    pb = workloads.kinetic_batch(n_inst=3, points=200, sizes_r=(24, 40), sizes_z=(32, 48), seed=4,
+                                 field="wavy")
+    ns = pb.model.no_species
+    out = []
+    for form in (0, 1):
+        tree = CdrTree(pb.params, pb.model, pb.specs)
+        for f, E in enumerate(pb.family_E):
+            tree.set_family_field(f, *E)
+        tree.set_fixed_field(pb.fields)
+        for g, per in enumerate(pb.dens):
+            for s, a in enumerate(per):
+                tree.upload(g, "dens", a, s)
+        assert tree.L.arcos_set_vjp_form(tree.h, form) == 0
+        adj = Adjoint(tree)
+        adj.forward(5, 5, h=50.0)
+        for g, sp in enumerate(pb.specs):
+            for s in range(ns):
+                adj.set_cotangent(g, s, cell_volume(sp, pb.params.dr(0), pb.params.dz(0)) * (1.0 + 0.1 * s))
+        out.append(adj.backward())
+        tree.close()
+    a, b = out
+    for g in range(len(pb.specs)):
+        for s in range(ns):
+            assert np.array_equal(a.dens0[g][s], b.dens0[g][s]), (g, s)
+    assert np.allclose(a.mobility, b.mobility, rtol=1e-12, atol=0)
+    assert abs(a.diffusion - b.diffusion) <= 1e-12 * abs(b.diffusion)
+    for r in range(len(a.tables)):
+        ta, tb = a.tables[r], b.tables[r]
+        assert np.max(np.abs(ta - tb)) <= 1e-12 * max(np.max(np.abs(tb)), 1e-300), r
