@@ -89,6 +89,8 @@ struct VjpArgs {
   const PatchDesc *patches;
   const AdjTile *tiles;
   int n_tiles;
+  const AdjTile *tiles_f;   // the split form's face tiles (VjpTileF::VY rows)
+  int n_tiles_f;
   int mode;             // 1: out = J^T (h/2 lam);  2: out = [n0>0](lam + lams + J^T (h/2 lam + h lams))
   int st_idx;           // adjoint-block array of the state, species s at st_idx + s
   int lam_idx, lams_idx, out_idx;
@@ -670,14 +672,16 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
 // With six species the one-kernel form holds every species' state and
 // cotangent in shared memory (72 KB a block, three blocks per SM) and the
 // reactions' registers beside the faces'.  The split form stages one species
-// at a time for its faces (k_vjp_faces: 33 KB a block, no per-species
-// registers: each species' gathered faces go straight to the output array,
-// the mobility sums to shared memory) and applies the reactions and the
+// at a time for its faces (k_vjp_faces: 32 x 8 tiles, a warp per row,
+// 33 KB a block, four blocks per SM — 32 x 16 tiles at two blocks per SM ran
+// no faster — and no per-species registers: each species' gathered faces go
+// straight to the output array, the mobility sums to shared memory) and
+// applies the reactions and the
 // mode-2 terms in a second, streaming kernel (k_vjp_react, one thread per
 // cell).  Every value is computed with the one-kernel form's operations in
 // its order, so both forms give the same bits.
 struct VjpTileF {
-  static constexpr int VX = 32, VY = 8, NT = 256;
+  static constexpr int VX = 32, VY = 8, NT = 32 * VY;    // a warp per row
   static constexpr int SC = VX + 6, SR = VY + 6, WC = VX + 4, WR = VY + 4;
   static constexpr int EC = VX + 3, ZR = VY + 3, FR = VX + 3, FZ = VY + 3;
   static constexpr int O_ST = 0;
@@ -692,7 +696,7 @@ struct VjpTileF {
 // out_s = (J_faces^T w)_s for every species of every tile (zero for
 // immobile species); the mobility and diffusion partial sums as k_vjp.
 template <int NS>
-__global__ void __launch_bounds__ (256, 4)
+__global__ void __launch_bounds__ (VjpTileF::NT, 4)
 k_vjp_faces (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
 {
   using L = VjpTileF;
@@ -721,8 +725,8 @@ k_vjp_faces (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
     }
   }
 
-  for (int ti = blockIdx.x; ti < A.n_tiles; ti += gridDim.x) {
-    const AdjTile T = A.tiles[ti];
+  for (int ti = blockIdx.x; ti < A.n_tiles_f; ti += gridDim.x) {
+    const AdjTile T = A.tiles_f[ti];
     const PatchDesc *Pp = A.patches + T.patch;
     const int nr = Pp->nr, nz = Pp->nz, pitch = Pp->pitch;
     const long long asz = Pp->asz;

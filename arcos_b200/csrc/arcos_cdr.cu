@@ -168,6 +168,8 @@ struct Ctx {
   bool adj_split = false;             // the VJP runs as k_vjp_faces + k_vjp_react
   int adj_blocks_r = 0;               // blocks of k_vjp_react
   size_t adj_smem_r = 0;
+  AdjTile *adj_tiles_f_d = nullptr;   // the split form's face tiles
+  int adj_ntiles_f = 0;
   int adj_tab_smem = 0;               // table gradients accumulate in shared memory
   int adj_lam = 0;                    // lam buffer holding the current cotangent
   bool adj_fwd = false;
@@ -1178,12 +1180,22 @@ adj_alloc (Ctx *c, int nsteps, int ck)
     // kernel holds every species in shared memory, three blocks per SM)
     c->adj_split = c->vjp_form == 1 || (c->vjp_form < 0 && ns >= 4);
     if (c->adj_split) {
+      std::vector<AdjTile> tf;
+      for (int p = 0; p < (int) c->pd_h.size (); p++) {
+        const PatchDesc &P = c->pd_h[p];
+        for (int zb = 0; zb < P.nz; zb += VjpTileF::VY)
+          for (int c0 = 0; c0 < P.nr; c0 += VjpTileF::VX) tf.push_back (AdjTile{p, c0, zb, 0});
+      }
+      c->adj_ntiles_f = (int) tf.size ();
+      cudaFree (c->adj_tiles_f_d);
+      CK (cudaMalloc (&c->adj_tiles_f_d, sizeof (AdjTile) * tf.size ()));
+      CK (cudaMemcpy (c->adj_tiles_f_d, tf.data (), sizeof (AdjTile) * tf.size (), cudaMemcpyHostToDevice));
       c->adj_tab_smem = ng <= 4096 ? 1 : 0;
       c->adj_smem_r = c->adj_tab_smem ? sizeof (double) * ng : 0;
       int occ2[2] = {0, 0};
       cudaError_t e = vjp_split_launch_m (ns, c->M, VjpArgs{}, 0, 0, c->adj_smem_r, 0, occ2);
       if (e != cudaSuccess) return fail (ARCOS_ERR_CUDA, std::string ("vjp occupancy: ") + cudaGetErrorString (e));
-      c->adj_blocks = std::min (c->adj_ntiles, c->num_sms * std::max (occ2[0], 1));
+      c->adj_blocks = std::min (c->adj_ntiles_f, c->num_sms * std::max (occ2[0], 1));
       c->adj_blocks_r = std::min (c->adj_ntiles, c->num_sms * std::max (occ2[1], 1));
     } else {
       c->adj_tab_smem = (ng <= 4096 && base + sizeof (double) * ng <= limit) ? 1 : 0;
@@ -1229,6 +1241,8 @@ run_vjp (Ctx *c, int mode, int st_idx, int lam_idx, int lams_idx, int out_idx, i
   A.patches = c->pd_d;
   A.tiles = c->adj_tiles_d;
   A.n_tiles = c->adj_ntiles;
+  A.tiles_f = c->adj_tiles_f_d;
+  A.n_tiles_f = c->adj_ntiles_f;
   A.mode = mode;
   A.st_idx = st_idx; A.lam_idx = lam_idx; A.lams_idx = lams_idx; A.out_idx = out_idx;
   A.hs = c->adj_hs_d;
@@ -1528,7 +1542,7 @@ arcos_destroy (void *ctx)
   cudaFree (c->photo_d);
   cudaFree (c->lean_nodes_d);
   cudaFree (c->adj_pool); cudaFree (c->adj_hs_d); cudaFree (c->adj_gtab_d);
-  cudaFree (c->adj_gpart_d); cudaFree (c->adj_invde_d); cudaFree (c->adj_tiles_d);
+  cudaFree (c->adj_gpart_d); cudaFree (c->adj_invde_d); cudaFree (c->adj_tiles_d); cudaFree (c->adj_tiles_f_d);
   cudaFree (c->pool); cudaFree (c->pd_d); cudaFree (c->nodes_d); cudaFree (c->st_d);
   cudaFree (c->dtlog_d); cudaFree (c->etz_d); cudaFree (c->done_d); cudaFree (c->items_d);
   cudaFree (c->plist_d); cudaFree (c->roots_d); cudaFree (c->chunks_d); cudaFree (c->kids_d); cudaFree (c->strips_d); cudaFree (c->ext_d);
@@ -2481,6 +2495,8 @@ arcos_set_vjp_form (void *ctx, int form)
   c->vjp_form = form;
   if (c->adj_graph) { cudaGraphExecDestroy (c->adj_graph); c->adj_graph = nullptr; }
   cudaFree (c->adj_tiles_d); c->adj_tiles_d = nullptr;
+  cudaFree (c->adj_tiles_f_d); c->adj_tiles_f_d = nullptr;
+  c->adj_ntiles_f = 0;
   cudaFree (c->adj_gpart_d); c->adj_gpart_d = nullptr;
   cudaFree (c->adj_gtab_d); c->adj_gtab_d = nullptr;
   cudaFree (c->adj_pool); c->adj_pool = nullptr;
