@@ -88,3 +88,28 @@ def test_device_3d_field_step_by_step_and_tree_entry(cuda_device):
     for s in range(2):
         assert max_ulp(dev.download(0, "dens", s), port.dens(0, s)) == 0
     dev.close()
+
+
+def test_device_3d_field_in_loop_division_free_within_tolerance(cuda_device):
+    """The default (division-free) stage kernels with the 3-D field solved
+    on the device: within 1e-12 of the oracle per step (resynchronised to
+    the oracle after every step; the field solve itself is exact)."""
+    nt = 4
+    pb = workloads.plain(nr=24, nz=40, ntheta=nt, ion_mass=0.0, noise=0.3, seed=13)
+    port = port_tree(pb, field_mode=bind.FIELD_POISSON, per_plane=True)
+    port.call("port_calc_charge")
+    dev = CdrTree(pb.params, pb.model, pb.specs, exact=False)
+    for s in range(2):
+        dev.upload(0, "dens", pb.dens[0][s], s)
+    dev.cdr_calc_charge_r(0)
+    dev.set_field_poisson(True)
+    for _ in range(4):
+        hp = port.rk2(50.0)[0]
+        hd = dev.run(1, 50.0)[0][0]
+        assert abs(hd - hp) <= 1e-12 * hp
+        for s in range(2):
+            a, b = dev.download(0, "dens", s), port.dens(0, s)
+            assert rel_err(a, b) <= 1e-12, (s, rel_err(a, b))
+            dev.upload(0, "dens", b, s)
+        dev.cdr_calc_charge_r(0)
+    dev.close()
