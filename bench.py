@@ -15,8 +15,8 @@ own replica (independent runs; the path has no exchange step).
 
 --impl reference times the reference's own CPU implementation of the same
 step (the reference C sources with the restated Fortran kernel, built under
-oracle/_ref, OpenMP build on all host cores) on a bounded slab of the same
-grid per step.
+oracle/_ref, serial build as shipped) with one process per host core, each on
+its own slab of the grid's rows.
 """
 from __future__ import annotations
 
@@ -224,23 +224,15 @@ def run_reference(args):
     return 0
 
 
-def _reference_line(args):
-    """The reference's own CPU step on this workload: the serial build as
-    shipped (oracle/_ref/libarcos_ref.so, the reference's C with its Fortran
-    flux kernel restated), drift/diffusion on every theta plane.  Each timed
-    step is one RK2 step of the whole 512 x 1024 x 16 grid when the run is
-    short enough (K + W <= 40 steps, about 3 s per step on one core);
-    otherwise a slab of the grid's rows sized so the run stays within a few
-    minutes.  The reference's OpenMP build is not used: the parallel region
-    of react_apply (src/reaction.c:95-160) shares its per-cell temporaries
-    (eabs, log_e, pos, e1, e2, rate, r_mod, ...) between threads, a data race
-    that makes it both slower than the serial build and wrong."""
+def _ref_slab(nz: int, seed: int, steps: int, warmup: int, barrier=None):
+    """One share of the reference arm: the reference's serial step (the
+    oracle/_ref build as shipped, else the CPU restatement) on a slab of nz
+    rows of the grid; W untimed steps, then (after the barrier, when several
+    processes share the work) K timed steps.  Returns (cell-species updates,
+    seconds, kind)."""
     from oracle import bind
     from arcos_b200 import workloads
-    total_steps = args.steps + args.warmup
-    nz = NZ if total_steps <= 40 else max(16, min(NZ, (NZ * 40 // max(1, total_steps)) // 16 * 16))
-    pb = workloads.plain(nr=NR, nz=nz, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=0)
-    threads = 1
+    pb = workloads.plain(nr=NR, nz=nz, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=seed)
     if bind.ref_available(False):
         t = bind.RefTree(pb.params, pb.model, pb.specs, field_mode=bind.FIELD_FIXED, omp=False)
         kind = "reference"
@@ -253,14 +245,74 @@ def _reference_line(args):
         t.dens(0, s)[...] = pb.dens[0][s]
     er, ez, _ = pb.fields[0]
     t.set_fixed_field(0, er, ez, pb.specs[0].zeros())
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
+    if barrier is not None:
+        barrier.wait(timeout=900)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         step()
-    el = time.perf_counter() - t0
-    value = NR * nz * NTHETA * NS * args.steps / el
-    what = "the whole grid" if nz == NZ else f"a {NR}x{nz}x{NTHETA} slab of the grid"
+    return NR * nz * NTHETA * NS * steps, time.perf_counter() - t0, kind
+
+
+def _ref_slab_proc(nz, seed, steps, warmup, barrier, queue):
+    with _CStdoutToStderr():
+        try:
+            queue.put(_ref_slab(nz, seed, steps, warmup, barrier))
+        except BaseException as exc:          # the parent reports it
+            barrier.abort()
+            queue.put(("error", f"{type(exc).__name__}: {exc}", None))
+
+
+def _reference_line(args):
+    """The reference's own CPU step on this workload, on all host cores.
+
+    The reference's OpenMP build is not used: the parallel region of
+    react_apply (src/reaction.c:95-160) shares its per-cell temporaries
+    (eabs, log_e, pos, e1, e2, rate, r_mod, ...) between threads, a data race
+    that makes it both slower than the serial build and wrong.  The host
+    cores are used instead by one process per core, each running the serial
+    build as shipped (oracle/_ref/libarcos_ref.so: the reference's C with its
+    Fortran flux kernel restated) on its own slab of the grid's rows, the
+    slabs' edges taken as domain boundaries; all processes start their timed
+    steps together and the arm's time is the slowest process's.  The slabs
+    cover the whole 512 x 1024 x 16 grid when the run is short enough (about
+    3 s per whole-grid step on one core, at most ~2 minutes per process);
+    otherwise they are thinner and the arm times a sample of the grid."""
+    import multiprocessing as mp
+    total = args.steps + args.warmup
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    procs = max(1, min(cores, NZ // 16))
+    budget_rows = max(16, (NZ * 40 // max(1, total)) // 16 * 16)     # ~2 min of steps per process
+    nz = max(16, min(NZ, budget_rows, -(-NZ // procs)))
+    results = []
+    if procs > 1:
+        ctx = mp.get_context("spawn")
+        barrier = ctx.Barrier(procs)
+        queue = ctx.Queue()
+        ps = [ctx.Process(target=_ref_slab_proc, args=(nz, i, args.steps, args.warmup, barrier, queue))
+              for i in range(procs)]
+        for p in ps:
+            p.start()
+        for _ in ps:
+            results.append(queue.get(timeout=1800))
+        for p in ps:
+            p.join(timeout=60)
+        bad = [r for r in results if r[0] == "error"]
+        if bad:
+            raise RuntimeError(f"reference slab process failed: {bad[0][1]}")
+    else:
+        results.append(_ref_slab(nz, 0, args.steps, args.warmup))
+    work = sum(r[0] for r in results)
+    el = max(r[1] for r in results)
+    kind = results[0][2]
+    value = work / el
+    rows = procs * nz
+    what = ("the whole grid" if rows >= NZ else f"{rows} of the grid's {NZ} rows") + \
+        f" as {procs} slab(s) of {NR}x{nz}x{NTHETA}, one process per core"
     sample = (f"each step: one RK2 step of {what} (serial build as shipped; "
               f"{'the reference C' if kind == 'reference' else 'the CPU restatement'})")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
@@ -268,7 +320,7 @@ def _reference_line(args):
             "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": workload_config({"replicas": args.gpus}),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return line
@@ -595,6 +647,52 @@ def extra_field(stream, K: int = 100):
     return out
 
 
+def extra_plain_wavy(stream, K: int = 20, W: int = 5):
+    """The headline grid (512 x 1024 x 16, 2 species, per-plane mode) on the
+    seeded non-uniform field (both components change sign inside a tile,
+    |E| sweeps the reaction table from underflow to overflow): the same
+    timing as the main line (K steps replayed from the step graph after W
+    warm-up steps, CUDA events) and the stage-2 kernel's roofline, so the
+    headline is not only measured on the uniform field."""
+    from arcos_b200 import workloads
+    from arcos_b200._lib import check
+    from arcos_b200.autotune import autotune_tiles
+    from arcos_b200.cdr import CdrTree
+    pb = workloads.plain(nr=NR, nz=NZ, ntheta=NTHETA, ion_mass=1.0, noise=1e-6, seed=0, field="wavy")
+    tree = CdrTree(pb.params, pb.model, pb.specs, stream=stream.cuda_stream)
+    _load(tree, pb)
+    L, h = tree.L, tree.h
+    tune = autotune_tiles(tree, steps=6, stream=stream)
+    check(L.arcos_run_prepare(h, 50.0))
+    check(L.arcos_run_enqueue(h, W))
+    e0, e1 = _events(stream)
+    e0.record(stream)
+    check(L.arcos_run_enqueue(h, K))
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    _, hlast, err = tree.family_state(0)
+    ev = _events(stream) + _events(stream)[:1]
+    s2 = 0.0
+    for k in range(10):
+        check(L.arcos_enqueue_stage(h, 1, k & 1))
+        ev[0].record(stream)
+        check(L.arcos_enqueue_stage(h, 2, k & 1))
+        ev[1].record(stream)
+        ev[1].synchronize()
+        s2 += ev[0].elapsed_time(ev[1]) / 10
+    tree.close()
+    cells = NR * NZ * NTHETA
+    peak, src = _peak_hbm()
+    bytes_s2 = 8 * (3 * NS + 2) * cells
+    return {"workload": f"{NR}x{NZ}x{NTHETA} grid, 2 species, wavy fixed field (er, ez change sign "
+                        "inside a tile; |E| from 0.02 to 30)",
+            "ms_per_step": ms, "value": cells * NS / (ms / 1e3), "steps": K, "warmup": W,
+            "stage2_ms": s2, "stage2_frac": bytes_s2 / (s2 / 1e3) / 1e9 / peak, "peak_source": src,
+            "tile_autotune_ms_per_step": {str(k): v for k, v in tune.items()},
+            "dt_last": hlast, "device_error_bits": err}
+
+
 def extra_refine(stream, calls: int = 5):
     """Refinement criteria (cdr_refine, src/cdr.c:1630-1682) of the
     512 x 1024 x 16 grid with the reference's default parameters: one
@@ -795,7 +893,7 @@ def run_device(args):
         wanted = set(args.extras.split(","))
         for name, fn in (("amr_batched", extra_amr), ("adjoint", extra_adjoint),
                          ("kinetic_batch", extra_kinetic), ("refine", extra_refine),
-                         ("field", extra_field)):
+                         ("field", extra_field), ("plain_wavy", extra_plain_wavy)):
             if name not in wanted:
                 continue
             try:
@@ -836,7 +934,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-AMR, adjoint and kinetic-batch measurements")
-    ap.add_argument("--extras", default="amr_batched,adjoint,kinetic_batch,refine,field",
+    ap.add_argument("--extras", default="amr_batched,adjoint,kinetic_batch,refine,field,plain_wavy",
                     help="comma-separated subset of the extra measurements")
     ap.add_argument("--exact", action="store_true", help="bit-exact flux limiter")
     ap.add_argument("--tile", type=int, default=None,
