@@ -101,7 +101,7 @@ struct VjpArgs {
   double *g_table;      // [nodes] then [under, over] per reaction
   int n_nodes;
   int tab_smem;         // accumulate the table gradients in shared memory (VjpTile::O_TAB)
-  int rates_idx;        // adjoint arrays of the per-cell reaction lookups (k_adj_rates), 3 per reaction
+  int rates_idx;        // adjoint arrays of the per-cell reaction lookups (k_adj_rates): 3 per reaction, then |E|
   double *g_part;       // [gridDim.x][ns + 1]: mobility gradients, then diffusion
   const double *colfac;
   double cm[ARCOS_MAXS], ddr[ARCOS_MAXS], ddz[ARCOS_MAXS];
@@ -181,7 +181,9 @@ k_adj_copy (const PatchDesc *__restrict__ pd, int to_adj, int set, int idx)
 // entry as a 32-bit integer in the first half of the third array: 2 i_lo
 // (|E| inside the table), 2 i_lo + 1 (inside, on the last node, where
 // v2 = v1), or -(under/over entry) - 1 (outside).  |E| as the VJP's
-// reactions take it (cdr.c:681-692).
+// reactions take it (cdr.c:681-692), in array rates_idx + 3 nreact: the
+// split form rebuilds k and tt from it and the entry code (same operations,
+// same values) instead of reading them.
 static __global__ void
 k_adj_rates (const __grid_constant__ Model M, const PatchDesc *__restrict__ pd, const TableNode *__restrict__ nodes,
              const double *__restrict__ inv_de, int n_nodes, int rates_idx)
@@ -219,6 +221,7 @@ k_adj_rates (const __grid_constant__ Model M, const PatchDesc *__restrict__ pd, 
         rp[asz] = tt;
         reinterpret_cast<int *> (adj + (long long) (rates_idx + 3 * r + 2) * asz)[o] = cd;
       }
+      adj[(long long) (rates_idx + 3 * M.nreact) * asz + o] = e;
     }
 }
 
@@ -709,10 +712,11 @@ k_vjp_faces (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
   double *const sST = vsm + L::O_ST, *const sW = vsm + L::O_W;
   double *const sER = vsm + L::O_ER, *const sEZ = vsm + L::O_EZ;
   double *const sPR = vsm + L::O_PR, *const sPZ = vsm + L::O_PZ;
-  __shared__ double sGmu[NW][NS];
-  __shared__ double red[NW][NS + 1];
+  __shared__ double sGt[NS][NT];              // per thread: its mobility sums, per species
+  __shared__ double red[NS + NW];
   const int t = threadIdx.x, lane = t & 31, wq = t >> 5;
-  if (lane < NS) sGmu[wq][lane] = 0.0;
+#pragma unroll
+  for (int s = 0; s < NS; s++) sGt[s][t] = 0.0;
   double gD = 0.0;
   int rjj[RP], rfi[RP];
   {
@@ -843,10 +847,7 @@ k_vjp_faces (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
           axial_item ((i - NRP) >> 5);
         }
       }
-      // this species' mobility sum: per warp into shared memory
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) gmu += __shfl_xor_sync (0xffffffffu, gmu, o);
-      if (lane == 0) sGmu[wq][s] += gmu;
+      sGt[s][t] += gmu;                         // this thread's slot: no other thread writes it
       __syncthreads ();
       auto RAD = [&] (int jj, int x) -> double {
         const int f = x - c0 + 1;
@@ -888,18 +889,25 @@ k_vjp_faces (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) gD += __shfl_xor_sync (0xffffffffu, gD, o);
   __syncthreads ();
-  if (lane == 0) {
-#pragma unroll
-    for (int s = 0; s < NS; s++) red[wq][s] = sGmu[wq][s];
-    red[wq][NS] = gD;
-  }
-  __syncthreads ();
-  if (t <= NS) {
+  for (int s = wq; s < NS; s += NW) {
     double v = 0.0;
-    for (int w = 0; w < NW; w++) v += red[w][t];
-    A.g_part[(size_t) blockIdx.x * (NS + 1) + t] += v;
+    for (int i = lane; i < NT; i += 32) v += sGt[s][i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync (0xffffffffu, v, o);
+    if (lane == 0) red[s] = v;
+  }
+  if (lane == 0) red[NS + wq] = gD;
+  __syncthreads ();
+  if (t < NS) {
+    A.g_part[(size_t) blockIdx.x * (NS + 1) + t] += red[t];
+  } else if (t == NS) {
+    double v = 0.0;
+    for (int w = 0; w < NW; w++) v += red[NS + w];
+    A.g_part[(size_t) blockIdx.x * (NS + 1) + NS] += v;
   }
 }
+
+
 
 // The reactions of every cell (react_apply, folded form) added to the faces
 // that k_vjp_faces left in the output array, then the mode-2 terms: the
@@ -951,25 +959,32 @@ k_vjp_react (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
     }
     if (M.nreact > 0) {
       const bool on = own && ((double) (Pp->z0 + j) + 0.5) * Pp->dz < M.z_cutoff;
-      const double *rp0 = adj + (long long) A.rates_idx * asz + o;
       const int *ip0 = reinterpret_cast<const int *> (adj + (long long) (A.rates_idx + 2) * asz) + o;
-      double nk = own ? __ldg (rp0) : 0.0, ntt = own ? __ldg (rp0 + asz) : 0.0;
+      const double ee = own ? __ldg (adj + (long long) (A.rates_idx + 3 * M.nreact) * asz + o) : 0.0;
       int ncd = own ? __ldg (ip0) : 0;
 #pragma unroll 1
       for (int r = 0; r < M.nreact; r++) {
         const int nin = M.r_nin[r];
-        const double k = nk, tt = ntt;
         const int cd = ncd;
-        if (r + 1 < M.nreact && own) {
-          const double *rp = rp0 + (long long) (3 * (r + 1)) * asz;
-          nk = __ldg (rp); ntt = __ldg (rp + asz); ncd = __ldg (ip0 + (long long) (6 * (r + 1)) * asz);
-        }
+        if (r + 1 < M.nreact && own) ncd = __ldg (ip0 + (long long) (6 * (r + 1)) * asz);
         int i_lo = -1, i_hi = -1;
         double g_lo = 0.0, g_hi = 0.0;
         double rho = 0.0;
 #pragma unroll
         for (int s = 0; s < NS; s++) rho = __fma_rn (sCf[r * NS + s], wc[s], rho);
         if (on && rho != 0.0) {
+          // k(|E|) and tt of k_adj_rates from the entry code: the same
+          // operations on the same node, so the same values
+          double k, tt = 0.0;
+          if (cd >= 0) {
+            const int il = cd >> 1;
+            const TableNode n = A.nodes[il];
+            const double de = ee - n.e1;
+            k = n.val + n.slope * de;
+            tt = de * __ldg (A.inv_de + il);
+          } else {
+            k = (-cd - 1 - A.n_nodes - 2 * r) ? M.r_over[r] : M.r_under[r];
+          }
           const double rk = rho * k;
           auto sgn = [] (double v) -> double { return v > 0.0 ? 1.0 : (v < 0.0 ? -1.0 : 0.0); };
           auto pick = [&] (int sp) -> double {

@@ -1112,8 +1112,8 @@ inline int adj_seg_n0 (Ctx *c, int j) { return 3 * c->M.ns + j * c->M.ns; }
 inline int adj_seg_ns (Ctx *c, int j) { return 3 * c->M.ns + (c->adj_ck + j) * c->M.ns; }
 inline int adj_ckpt (Ctx *c, int seg) { return 3 * c->M.ns + (2 * c->adj_ck + seg) * c->M.ns; }
 inline int adj_final (Ctx *c) { return 3 * c->M.ns + (2 * c->adj_ck + c->adj_nseg) * c->M.ns; }
-inline int adj_rates (Ctx *c) { return adj_final (c) + c->M.ns; }          // 3 per reaction
-inline int adj_arrays (Ctx *c) { return adj_rates (c) + 3 * c->M.nreact; }
+inline int adj_rates (Ctx *c) { return adj_final (c) + c->M.ns; }          // 3 per reaction, then |E|
+inline int adj_arrays (Ctx *c) { return adj_rates (c) + 3 * c->M.nreact + (c->M.nreact > 0 ? 1 : 0); }
 
 // copies the densities of `set` to (to_adj) or from adjoint arrays idx .. idx+ns-1
 int
