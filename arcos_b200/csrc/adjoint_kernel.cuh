@@ -714,6 +714,7 @@ k_vjp_faces (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
   double *const sPR = vsm + L::O_PR, *const sPZ = vsm + L::O_PZ;
   __shared__ double sGt[NS][NT];              // per thread: its mobility sums, per species
   __shared__ double red[NS + NW];
+  __shared__ double sFM[FR], sFP[FR];         // radial factors of the tile's radial faces
   const int t = threadIdx.x, lane = t & 31, wq = t >> 5;
 #pragma unroll
   for (int s = 0; s < NS; s++) sGt[s][t] = 0.0;
@@ -750,6 +751,11 @@ k_vjp_faces (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
       const int col = c0 - 2 + xx, row = j0 + yy;
       sER[yy * EC + xx] = (col >= -2 && col <= nr + 1 && row <= nz + 1) ? __ldg (er + AO (col, row)) : 0.0;
     });
+    for (int i = t; i < FR; i += NT) {          // face ar = c0 - 1 + i (.f90:408-412)
+      const int ar = c0 - 1 + i;
+      sFM[i] = (ar >= 0 && ar < nr) ? A.colfac[2 * ar] : 0.0;
+      sFP[i] = (ar >= 1 && ar <= nr) ? A.colfac[2 * (ar - 1) + 1] : 0.0;
+    }
 #pragma unroll
     for (int y8 = 0; y8 < (ZR + NW - 1) / NW; y8++) {
       const int yy = wq + NW * y8;
@@ -800,10 +806,8 @@ k_vjp_faces (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         const int ar = c0 - 1 + fi, jr = j0 + jj;
         double pLL = 0.0, pL = 0.0, pR = 0.0, pRR = 0.0;
         if (ar >= 0 && ar <= nr && jr < nz) {
-          const double fm = ar < nr ? A.colfac[2 * ar] : 0.0;
-          const double fp = ar >= 1 ? A.colfac[2 * (ar - 1) + 1] : 0.0;
           const double *w = sW + (jj + 2) * WC + fi;
-          const double g = fm * w[1] - fp * w[0];
+          const double g = sFM[fi] * w[1] - sFP[fi] * w[0];
           if (g != 0.0) {
             const double *st = sST + (jj + 3) * SC + fi;
             const double e = sER[jj * EC + fi];

@@ -307,7 +307,7 @@ __global__ void __launch_bounds__ (32 * WY)
 k_stage (const __grid_constant__ Model M, const StageArgs A)
 {
   using LY = TileLayout<NS, MODE, WY, RPW>;
-  constexpr int TY = LY::TY, ROWS = LY::ROWS, PL = LY::PLANE, NA = LY::NA;
+  constexpr int ROWS = LY::ROWS, PL = LY::PLANE, NA = LY::NA;
   constexpr int A_D = LY::A_D, A_F = LY::A_F;
   constexpr bool OTF = (MODE == M_S1 || MODE == M_S2);
   constexpr int NT = 32 * WY;
