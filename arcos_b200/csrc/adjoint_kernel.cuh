@@ -764,12 +764,12 @@ k_vjp_faces (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
       sEZ[yy * VX + lane] = (col <= nr + 1 && row >= -2 && row <= nz + 1) ? __ldg (ez + AO (col, row)) : 0.0;
     }
 
-    static_for<0, NS> ([&] (auto S_) {
-      constexpr int s = decltype (S_)::value;
+#pragma unroll 1
+    for (int s = 0; s < NS; s++) {             // one copy of the body: the kernel fits the instruction cache
       double *outp = adj + (long long) (A.out_idx + s) * asz;
       if (!M.mobile[s]) {                       // block-uniform
         if (own) outp[AO (c, j)] = 0.0;
-        return;
+        continue;
       }
       __syncthreads ();                         // the previous species is done with the buffers
       const double *src = adj + (long long) (A.st_idx + s) * asz;
@@ -886,7 +886,7 @@ k_vjp_faces (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
         if (c == nr - 2) rr = __fma_rn (sg_r, RAD (wq, nr + 1), rr);
         outp[AO (c, j)] = z + rr;
       }
-    });
+    }
   }
 
   // ---- block partial sums of the mobility and diffusion gradients ----
