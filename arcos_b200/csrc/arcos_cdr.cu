@@ -2868,8 +2868,12 @@ arcos_run (void *ctx, int nsteps, double h, double *dt_out)
     }
     CK (cudaMemcpyAsync (c->st_d, c->st_stage.data (), sizeof (DevState) * c->nfam, cudaMemcpyHostToDevice,
                          c->stream));
-  } else if ((r = set_h_attempt (c, h))) {
-    return r;
+  } else {
+    // set_h_attempt on the states just read: one write, no second read
+    c->st_stage = st0;
+    for (auto &s : c->st_stage) s.h_attempt = h;
+    CK (cudaMemcpyAsync (c->st_d, c->st_stage.data (), sizeof (DevState) * c->nfam, cudaMemcpyHostToDevice,
+                         c->stream));
   }
   // trees, and single grids with photoionization: the general step
   const bool general = !c->fused_ok || c->photo_n > 0;
