@@ -297,8 +297,20 @@ def _reference_line(args):
               for i in range(procs)]
         for p in ps:
             p.start()
-        for _ in ps:
-            results.append(queue.get(timeout=1800))
+        import queue as _queue
+        t_end = time.time() + 1800
+        while len(results) < procs:
+            try:
+                results.append(queue.get(timeout=5))
+            except _queue.Empty:
+                # a process that ended without reporting (a crash in the C code)
+                dead = [p.exitcode for p in ps if p.exitcode not in (None, 0)]
+                if dead or time.time() > t_end:
+                    for p in ps:
+                        if p.is_alive():
+                            p.terminate()
+                    raise RuntimeError(f"reference slab processes failed (exit codes {dead})"
+                                       if dead else "reference slab processes timed out")
         for p in ps:
             p.join(timeout=60)
         bad = [r for r in results if r[0] == "error"]
