@@ -273,7 +273,7 @@ mbar_expect_tx (unsigned long long *bar, unsigned bytes)
   asm volatile ("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32 (bar)), "r"(bytes) : "memory");
 }
 
-// 3-D tile copy global -> shared, completion counted on the mbarrier (no multicast)
+// 3-D tile copy global -> shared for this CTA alone, completion counted on the mbarrier
 __device__ __forceinline__ void
 tma_load_3d (void *dst, const void *tmap, int x, int y, int z, unsigned long long *bar)
 {
