@@ -264,6 +264,16 @@ def _ref_slab_proc(nz, seed, steps, warmup, barrier, queue):
             queue.put(("error", f"{type(exc).__name__}: {exc}", None))
 
 
+def ref_slab_plan(total_steps: int, cores: int):
+    """(processes, rows per slab) of the reference arm: one process per core
+    (at most one per 16 rows), slabs that together cover the grid's NZ rows,
+    thinned (multiples of 16 rows) so that one process's total_steps stay
+    within about two minutes at ~3 s per whole-grid step on one core."""
+    procs = max(1, min(cores, NZ // 16))
+    budget_rows = max(16, (NZ * 40 // max(1, total_steps)) // 16 * 16)
+    return procs, max(16, min(NZ, budget_rows, -(-NZ // procs)))
+
+
 def _reference_line(args):
     """The reference's own CPU step on this workload, on all host cores.
 
@@ -280,14 +290,11 @@ def _reference_line(args):
     3 s per whole-grid step on one core, at most ~2 minutes per process);
     otherwise they are thinner and the arm times a sample of the grid."""
     import multiprocessing as mp
-    total = args.steps + args.warmup
     try:
         cores = len(os.sched_getaffinity(0))
     except AttributeError:
         cores = os.cpu_count() or 1
-    procs = max(1, min(cores, NZ // 16))
-    budget_rows = max(16, (NZ * 40 // max(1, total)) // 16 * 16)     # ~2 min of steps per process
-    nz = max(16, min(NZ, budget_rows, -(-NZ // procs)))
+    procs, nz = ref_slab_plan(args.steps + args.warmup, cores)
     results = []
     if procs > 1:
         ctx = mp.get_context("spawn")

@@ -34,3 +34,19 @@ def test_reference_arm_line():
 def test_reference_arm_other_ranks_exit_quietly():
     p = _run({"RANK": "1"})
     assert p.returncode == 0 and p.stdout.strip() == ""
+
+
+def test_reference_slab_plan():
+    sys.path.insert(0, ROOT)
+    import bench
+    # the driver's 20 + 5 steps: the whole grid, one slab per core
+    assert bench.ref_slab_plan(25, 16) == (16, 64)
+    assert bench.ref_slab_plan(25, 8) == (8, 128)
+    assert bench.ref_slab_plan(25, 1) == (1, 1024)
+    # long runs: thinner slabs, a sample of the grid (multiples of 16 rows)
+    procs, nz = bench.ref_slab_plan(2010, 16)
+    assert procs == 16 and nz == 16 and procs * nz < bench.NZ
+    assert bench.ref_slab_plan(100, 4) == (4, 256)         # the per-core share binds
+    assert bench.ref_slab_plan(100, 1) == (1, 400)         # the time budget binds
+    # never more processes than 16-row slabs
+    assert bench.ref_slab_plan(25, 200)[0] == bench.NZ // 16
