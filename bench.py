@@ -691,7 +691,7 @@ def extra_plain_wavy(stream, K: int = 20, W: int = 5):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / K
     _, hlast, err = tree.family_state(0)
-    ev = _events(stream) + _events(stream)[:1]
+    ev = _events(stream)
     s2 = 0.0
     for k in range(10):
         check(L.arcos_enqueue_stage(h, 1, k & 1))
