@@ -74,7 +74,7 @@ def uniform_field(spec: GridSpec):
 
 def wavy_field(spec: GridSpec, params: Params, seed: int = 0, e_lo: float = 0.02,
                e_hi: float = 30.0, wavelength: Tuple[float, float] = (14.0, 40.0),
-               cancel_applied: bool = True):
+               cancel_applied: bool = True, span: Optional[float] = None):
     """A smooth, non-uniform fixed field: the field solve's part (er, ez,
     None) in rz layout on the staggered points (er at r faces (ir + 1) dr and
     cell-centre z, ez at cell-centre r and z faces (iz + 1) dz; grid.h:40,43).
@@ -82,9 +82,9 @@ def wavy_field(spec: GridSpec, params: Params, seed: int = 0, e_lo: float = 0.02
     Each component is a product of sines with seeded phases and wavelengths
     drawn from ``wavelength`` (in cells of the grid's level), so both
     components change sign inside 32-column and 16-row tiles, and an envelope
-    that grows log-uniformly from ``e_lo`` at z = 0 to ``e_hi`` at z = L_z, so
-    |E| sweeps a whole reaction table: underflow near z = 0, overflow near
-    z = L_z.  With ``cancel_applied`` the applied E0 is subtracted, so the
+    that grows log-uniformly from ``e_lo`` at z = 0 to ``e_hi`` at z = ``span``
+    (default L_z), so |E| sweeps a whole reaction table: underflow near
+    z = 0, overflow near z = span.  With ``cancel_applied`` the applied E0 is subtracted, so the
     total field (after cdr_add_ext_field adds E0 back) is the wave itself.
     In 3-D each plane is scaled by 1 + 0.3 cos(theta)."""
     rng = np.random.default_rng(seed)
@@ -95,8 +95,10 @@ def wavy_field(spec: GridSpec, params: Params, seed: int = 0, e_lo: float = 0.02
     k = [2 * math.pi / (float(rng.uniform(lo, hi))) for _ in range(6)]
     ph = [float(rng.uniform(0, 2 * math.pi)) for _ in range(6)]
 
+    top = params.L_z if span is None else span
+
     def env(zc):
-        return e_lo * (e_hi / e_lo) ** np.clip(zc / params.L_z, 0.0, 1.0)
+        return e_lo * (e_hi / e_lo) ** np.clip(zc / top, 0.0, 1.0)
 
     # er: r faces, z centres; ez: r centres, z faces (positions in cells of this level)
     rf, zc = np.meshgrid(ir + 1.0, iz + 0.5)
@@ -307,8 +309,13 @@ def kinetic_batch(n_inst: int = 32, seed: int = 0, points: int = 1000,
     """A batch of independent single-grid instances of uneven sizes, each its
     own family with its own applied field Ez ~ U[-2, -0.5].  With
     ``field="wavy"`` each instance also gets a ``wavy_field`` (added to its
-    applied field) whose |E| sweeps [0.005, 80], beyond both ends of the
-    rate tables."""
+    applied field) whose envelope grows from 0.005 at z = 0 to 80 at z = L_z:
+    over the default 32 instances |E| reaches both ends of the rate tables
+    ([0.01, 50]), while an instance much shorter than L_z stays near its
+    applied field.  ``field="wavy_full"`` grows the same envelope over each
+    instance's own height, with the instance's applied field subtracted (the
+    total field is the wave itself), so every instance, however short,
+    sweeps from below the tables' first node to above their last."""
     rng = np.random.default_rng(seed)
     model = kinetic_model(points=points, seed=seed + 1)
     params = Params(L_r=2.0, L_z=4.0, gridpoints_r=128, gridpoints_z=256, E0_z=-1.0,
@@ -327,12 +334,15 @@ def kinetic_batch(n_inst: int = 32, seed: int = 0, points: int = 1000,
             per.append(seed_dens(sp, params, rng, amp=amp, noise=1e-6,
                                  center_z=0.9 * nz * params.dz(0)))
         dens.append(per)
-        if field == "wavy":
+        if field in ("wavy", "wavy_full"):
             fields.append(wavy_field(sp, params, seed=seed * 1000 + i, e_lo=0.005, e_hi=80.0,
-                                     cancel_applied=False))
+                                     cancel_applied=False,
+                                     span=nz * params.dz(0) if field == "wavy_full" else None))
         elif field == "uniform":
             fields.append(uniform_field(sp))
         else:
             raise ValueError(f"unknown field {field!r}")
         famE.append((0.0, 0.0, float(rng.uniform(-2.0, -0.5))))
+        if field == "wavy_full":
+            fields[-1][1][...] -= famE[-1][2]     # the total field is the wave itself
     return Problem(params, model, specs, dens, fields, famE)

@@ -155,9 +155,13 @@ def test_theta_ref_exact_wavy_field():
 
 
 @needs_ref
-def test_kinetic_model_wavy_field():
+@pytest.mark.parametrize("field", ["wavy", "wavy_full"])
+def test_kinetic_model_wavy_field(field):
+    """Nine reactions on a non-uniform field: "wavy" keeps |E| near each
+    instance's applied field (a few table nodes), "wavy_full" sweeps it from
+    below the tables' first node to above their last."""
     pb = workloads.kinetic_batch(n_inst=2, points=300, sizes_r=(24,), sizes_z=(40,), seed=8,
-                                 field="wavy")
+                                 field=field)
     for i in range(2):
         sub = single_family(pb, i)
         port = port_tree(sub, E=pb.family_E[i])
@@ -168,11 +172,12 @@ def test_kinetic_model_wavy_field():
 
 
 @pytest.mark.skipif(not bind.ref_available("bigtab"), reason="reference build absent")
-@pytest.mark.parametrize("field", ["uniform", "wavy"])
+@pytest.mark.parametrize("field", ["uniform", "wavy", "wavy_full"])
 def test_kinetic_model_1000_point_tables(field):
     """The kinetic batch's 1000-point tables, against the reference built
     with a 1024-entry MAX_TABLE_SIZE (oracle/react_table_1024.h): 9
-    reactions, 6 species, |E| over the whole table (and beyond it)."""
+    reactions, 6 species; with "wavy_full" |E| runs over the whole table
+    and beyond both of its ends."""
     pb = workloads.kinetic_batch(n_inst=2, points=1000, sizes_r=(24,), sizes_z=(40,), seed=8,
                                  field=field)
     for i in range(2):

@@ -45,3 +45,18 @@ def test_workloads_are_deterministic():
         assert np.array_equal(x, y)
     assert np.array_equal(a.dens[0][0], b.dens[0][0])
     assert not np.array_equal(a.fields[0][0], c.fields[0][0])
+
+
+def test_kinetic_wavy_full_sweeps_every_instance():
+    pb = workloads.kinetic_batch(n_inst=3, points=300, sizes_r=(24, 40), sizes_z=(32, 48), seed=4,
+                                 field="wavy_full")
+    t = pb.model.reactions[0].table
+    lo, hi = 10.0 ** t.e_min, 10.0 ** (t.e_min + t.steps * t.e_step)
+    for f, E in zip(pb.fields, pb.family_E):
+        er, ez, _ = f
+        e = np.hypot(er[0, 2:-2, 2:-2] + E[0], ez[0, 2:-2, 2:-2] + E[2])
+        assert (e < lo).any() and (e > hi).any(), (e.min(), e.max(), lo, hi)
+    # the other field choices are unchanged by the option
+    u = workloads.kinetic_batch(n_inst=3, points=300, sizes_r=(24, 40), sizes_z=(32, 48), seed=4,
+                                field="wavy")
+    assert u.family_E == pb.family_E and np.array_equal(u.dens[2][1], pb.dens[2][1])
