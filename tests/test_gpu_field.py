@@ -101,10 +101,33 @@ def test_fast_limiter_long_run_on_wavy_field(cuda_device):
 
 @pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5])
 def test_kinetic_batch_on_wavy_field(cuda_device, tile):
-    """Six species, nine reactions, |E| beyond both ends of the 200-node
-    tables, three families with their own applied fields, each tile shape."""
+    """Six species, nine reactions, three families with their own applied
+    fields, each tile shape; on these short instances |E| stays near each
+    family's applied field (a few adjacent nodes of the 200-node tables)."""
     pb = workloads.kinetic_batch(n_inst=3, points=200, sizes_r=(24, 40), sizes_z=(32, 48), seed=1,
                                  field="wavy")
+    dev = device_tree(pb, exact=False)
+    dev.set_tile(tile)
+    ports = [port_tree(single_family(pb, i), E=pb.family_E[i]) for i in range(3)]
+    for _ in range(3):
+        hd = dev.run(1, 50.0)
+        for i, port in enumerate(ports):
+            hp = port.rk2(50.0)[0]
+            assert abs(hd[i][0] - hp) <= TOL * hp
+            for s in range(6):
+                a, b = dev.download(i, "dens", s), port.dens(0, s)
+                assert rel_err(a, b) <= TOL, (tile, i, s, rel_err(a, b))
+                dev.upload(i, "dens", b, s)
+
+
+@pytest.mark.parametrize("tile", [0, 2, 3])
+def test_kinetic_batch_on_full_sweep_field(cuda_device, tile):
+    """The same on ``field="wavy_full"``: every instance's |E| runs from below
+    the tables' first node to above their last, so the division-free
+    kernel's lookups of all nine reactions are compared at both sentinel
+    nodes and across the table."""
+    pb = workloads.kinetic_batch(n_inst=3, points=200, sizes_r=(24, 40), sizes_z=(32, 48), seed=1,
+                                 field="wavy_full")
     dev = device_tree(pb, exact=False)
     dev.set_tile(tile)
     ports = [port_tree(single_family(pb, i), E=pb.family_E[i]) for i in range(3)]
