@@ -676,13 +676,15 @@ k_vjp (const __grid_constant__ Model M, const __grid_constant__ VjpArgs A)
 // cotangent in shared memory (72 KB a block, three blocks per SM) and the
 // reactions' registers beside the faces'.  The split form stages one species
 // at a time for its faces (k_vjp_faces: 32 x 8 tiles, a warp per row,
-// 33 KB a block, four blocks per SM — 32 x 16 tiles at two blocks per SM ran
-// no faster — and no per-species registers: each species' gathered faces go
-// straight to the output array, the mobility sums to shared memory) and
-// applies the reactions and the
-// mode-2 terms in a second, streaming kernel (k_vjp_react, one thread per
-// cell).  Every value is computed with the one-kernel form's operations in
-// its order, so both forms give the same bits.
+// 33 KB of dynamic and 13 KB of static shared memory a block, four blocks
+// per SM, the species loop a run-time loop so the kernel keeps to the
+// instruction cache; 32 x 16 tiles at two blocks per SM ran slower) with no
+// per-species registers: each species' gathered faces go straight to the
+// output array, each thread's mobility sums to its own shared-memory slot.
+// It applies the reactions and the mode-2 terms in a second, streaming
+// kernel (k_vjp_react, one thread per cell).  Every value is computed with
+// the one-kernel form's operations in its order, so both forms give the
+// same bits.
 struct VjpTileF {
   static constexpr int VX = 32, VY = 8, NT = 32 * VY;    // a warp per row
   static constexpr int SC = VX + 6, SR = VY + 6, WC = VX + 4, WR = VY + 4;
